@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark: edges/s of run! + build_edges on the SPH time-stepping workload.
+
+Workload (one GPU): 1,000,000 Float32 points on a 100^3 cubic lattice,
+spacing h = 0.01, uniform jitter +-0.1h, radius 2h; every step adds a
+Gaussian displacement sigma = 0.005h, then update_point_set! -> run! (refit
+mode) -> build_edges (count, allocate, fill).  A step is one such time step;
+`value` is total edges / device time of K steps with the coordinates already
+resident in HBM; `e2e` is the same through host buffers (H2D of the step's
+coordinates from pinned memory, D2H of the full COO).
+
+Under torchrun (N>1) every rank runs an independent replica of the workload
+(the path has no cross-GPU exchange); the time is the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+H = 0.01
+PER = 100
+RADIUS = 2 * H
+JITTER = 0.1 * H
+SIGMA = 0.005 * H
+METRIC = "edges/s build+query+COO @1M pts; batched & fwd+bwd vs plain, exact edges"
+WORKLOAD = "sph_lattice_timestep_1M"
+
+
+def config_dict(extra=None):
+    c = {
+        "workload": WORKLOAD,
+        "n_points": PER ** 3,
+        "ndims": 3,
+        "lattice": f"{PER}^3, h={H}, jitter=+-0.1h",
+        "radius": RADIUS,
+        "displacement_sigma": SIGMA,
+        "refit_mode": True,
+        "l2": "inputs+outputs per step exceed L2: ~680 MB of COO written per step (126 MB L2)",
+        "seed": 12345,
+    }
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------- inputs -----
+def lattice_np(per, seed):
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(*[np.arange(per)] * 3, indexing="ij"), -1).reshape(-1, 3).astype(np.float64)
+    return (g * H + rng.uniform(-JITTER, JITTER, g.shape)).astype(np.float32)
+
+
+def snapshots_np(per, nsteps, seed):
+    """Coordinates of steps 0..nsteps-1 (float32, (N,3)) on the host."""
+    rng = np.random.default_rng(seed + 1)
+    x = lattice_np(per, seed)
+    out = [x]
+    for _ in range(nsteps - 1):
+        x = (x + rng.normal(0.0, SIGMA, x.shape)).astype(np.float32)
+        out.append(x)
+    return out
+
+
+# ------------------------------------------------------------- clocks -----
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in out.strip().splitlines():
+            p = [v.strip() for v in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                smax.append(float(p[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- ranks ------
+def dist_setup(gpus):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value: float, world: int, device=None) -> float:
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------ our arm -----
+def run_ours(args, rank, world, local):
+    import torch
+    import __graft_entry__
+    ob = __graft_entry__.load_package()
+    lib = ob._lib.load()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    W, K = args.warmup, args.steps
+    host = snapshots_np(PER, W + K, 12345 + rank)
+    snaps = [torch.from_numpy(x).to(dev).t() for x in host]  # (3, N) column-major views
+    N = host[0].shape[0]
+
+    tns = ob.TNS(torch.float32, ndims=3)
+    ob.set_search_radius_(tns, RADIUS)
+    ob.set_refit_mode_(tns, True)
+    sid = ob.add_point_set_(tns, snaps[0])
+    ob.set_active_search_(tns, sid, sid)
+    ctx = tns._ctx
+
+    def step(x):
+        ob.update_point_set_(tns, sid, x)
+        ob.run_(tns)
+        e = ob.build_edges(tns, sid, sid)
+        return e.senders.numel()
+
+    for w in range(W):
+        step(snaps[w])
+    torch.cuda.synchronize()
+    barrier(world)
+
+    nph = len(ob._lib.PHASES)
+    ms_buf = (C.c_double * nph)()
+    cnt_buf = (C.c_int64 * nph)()
+    lib.oct_profile_read(ctx.handle, ms_buf, cnt_buf, nph)  # clear
+    lib.oct_profile_enable(ctx.handle, 1)
+    launches0 = lib.oct_profile_kernel_launches(ctx.handle)
+    clocks = ClockSampler(local)
+    clocks.start()
+    stream = torch.cuda.current_stream(dev)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    edges = 0
+    for k in range(K):
+        edges += step(snaps[W + k])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    launches = lib.oct_profile_kernel_launches(ctx.handle) - launches0
+    lib.oct_profile_read(ctx.handle, ms_buf, cnt_buf, nph)
+    lib.oct_profile_enable(ctx.handle, 0)
+    phases = {ob._lib.PHASES[i]: round(ms_buf[i] / K, 5) for i in range(nph) if cnt_buf[i]}
+    phase_calls = {ob._lib.PHASES[i]: int(cnt_buf[i]) for i in range(nph) if cnt_buf[i]}
+
+    # --- end to end through host buffers (pinned), same steps
+    hpin = [torch.from_numpy(x).pin_memory() for x in host]
+    dcoords = torch.empty((N, 3), dtype=torch.float32, device=dev)
+    e_last = edges // K
+    cap = int(e_last * 1.2) + 1024
+    h_snd = torch.empty(cap, dtype=torch.int32).pin_memory()
+    h_rcv = torch.empty(cap, dtype=torch.int32).pin_memory()
+    h_disp = torch.empty((cap, 3), dtype=torch.float32).pin_memory()
+    h_dist = torch.empty(cap, dtype=torch.float32).pin_memory()
+
+    def e2e_step(k):
+        dcoords.copy_(hpin[k], non_blocking=True)
+        ob.update_point_set_(tns, sid, dcoords.t())
+        ob.run_(tns)
+        e = ob.build_edges(tns, sid, sid)
+        m = e.senders.numel()
+        if m > cap:
+            raise RuntimeError("e2e host buffer too small")
+        h_snd[:m].copy_(e.senders, non_blocking=True)
+        h_rcv[:m].copy_(e.receivers, non_blocking=True)
+        h_disp[:m].copy_(e.rel_displacement.t(), non_blocking=True)
+        h_dist[:m].copy_(e.rel_dist_norm.reshape(-1), non_blocking=True)
+        return m
+
+    for w in range(W):
+        e2e_step(w)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0.record(stream)
+    e2e_edges = 0
+    for k in range(K):
+        e2e_edges += e2e_step(W + k)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = t0.elapsed_time(t1)
+
+    ms_max = max_over_ranks(ms, world, dev)
+    e2e_ms_max = max_over_ranks(e2e_ms, world, dev)
+    tot_edges = sum_over_ranks(float(edges), world, dev)
+    tot_e2e = sum_over_ranks(float(e2e_edges), world, dev)
+    value = tot_edges / (ms_max / 1e3)
+
+    # --- roofline of the dominant HBM kernel (edge write = fill), live timing
+    from_peaks = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            from_peaks = json.load(f)
+    except Exception:
+        pass
+    peak = float(from_peaks["hbm_gbs"]) if from_peaks else 6650.0
+    peak_src = "measured" if from_peaks else "fallback"
+    e_per_step = edges / K
+    fill_ms = phases.get("fill", float("nan"))
+    fill_bytes = (12 + 4 * 3) * e_per_step + 8 * N  # (12 + 4D) E + 8N
+    achieved = fill_bytes / (fill_ms / 1e3) / 1e9
+    dominant = max(phases, key=phases.get) if phases else None
+
+    result = None
+    if rank == 0:
+        cpu = cpu_baseline(args)
+        result = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "edges/s",
+            "n_gpus": world,
+            "steps": K,
+            "warmup": W,
+            "ms_per_step": ms_max / K,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded jittered lattice + Gaussian steps)",
+            "config": config_dict({"edges_per_step": e_per_step, "parallelism": f"replicas x{world}"}),
+            "e2e": {"value": tot_e2e / (e2e_ms_max / 1e3), "unit": "edges/s",
+                    "h2d_bytes_per_step": N * 12, "d2h_bytes_per_step": int(24 * e2e_edges / K),
+                    "ms_per_step": e2e_ms_max / K},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_src, "kernel": "fill (k_edges<FILL>)",
+                         "traffic": args.fill_traffic, "algorithmic_bytes_per_launch": fill_bytes},
+            "phases_ms_per_step": phases,
+            "phase_records": phase_calls,
+            "dominant_phase": dominant,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+    return result
+
+
+def cpu_baseline(args, budget_s=None):
+    """The oracle (C++ restatement of the reference CPU path) on the host's
+    cores, on full-size time steps, stopping after ~10 s of work."""
+    import oracle
+    budget_s = budget_s if budget_s is not None else args.cpu_budget
+    nthreads = oracle.max_threads()
+    snaps = snapshots_np(PER, 4, 999)
+    edges, secs, steps = 0, 0.0, 0
+    for x in snaps[1:]:
+        t0 = time.perf_counter()
+        t = oracle.build_tree(x, np.float32(RADIUS), nthreads=nthreads)
+        e = oracle.build_edges(t, x, exclude_self=True, nthreads=nthreads)
+        secs += time.perf_counter() - t0
+        edges += len(e["senders"])
+        steps += 1
+        if secs >= budget_s:
+            break
+    return {"value": edges / secs, "unit": "edges/s", "cores": nthreads, "kind": "port",
+            "sample": f"{steps} full 1M-point time steps (build + count + scan + fill), "
+                      f"{secs:.1f} s of CPU work"}
+
+
+# ------------------------------------------------------ reference arm -----
+REF_PER = 40  # sample: a 40^3 sub-lattice per step
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU path (the oracle port: the Julia original cannot
+    run here) on all host threads; each step one time step of a 40^3
+    sub-lattice of the workload (same spacing, radius and displacement)."""
+    if rank != 0:
+        return None
+    import oracle
+    nthreads = oracle.max_threads()
+    snaps = snapshots_np(REF_PER, args.warmup + args.steps, 4242)
+    r = np.float32(RADIUS)
+    for x in snaps[:args.warmup]:
+        oracle.build_edges(oracle.build_tree(x, r, nthreads=nthreads), x, exclude_self=True, nthreads=nthreads)
+    edges, secs = 0, 0.0
+    for x in snaps[args.warmup:]:
+        t0 = time.perf_counter()
+        t = oracle.build_tree(x, r, nthreads=nthreads)
+        e = oracle.build_edges(t, x, exclude_self=True, nthreads=nthreads)
+        secs += time.perf_counter() - t0
+        edges += len(e["senders"])
+    v = edges / secs
+    sample = f"{args.steps} time steps of a {REF_PER}^3-point sub-lattice (same h, radius, displacement)"
+    return {
+        "impl": "reference",
+        "metric": METRIC, "value": v, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded jittered lattice + Gaussian steps)",
+        "config": config_dict({"reference_sample": sample}),
+        "cpu_baseline": {"value": v, "unit": "edges/s", "cores": nthreads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--fill-traffic", type=float, default=None,
+                    help="dram bytes per fill launch from an ncu capture (reported as roofline.traffic)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res))
+        return
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        res = run_ours(args, rank, world, local)
+        if res is not None:
+            print(json.dumps(res))
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

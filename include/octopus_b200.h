@@ -1,0 +1,169 @@
+/*
+ * octopus_b200.h -- C ABI of the B200 (sm_100a) fixed-radius octree
+ * neighbor search.
+ *
+ * The entry points fill the backend hooks that Octopus.jl's CUDA extension
+ * fills today (src/Octopus.jl:46-54): a Julia extension (or any FFI host)
+ * binds these symbols with plain pointers and sizes.  Every pointer argument
+ * named *coords*, *senders*, *receivers*, *rel_*, *d_rel_* or *grad* is a
+ * device pointer on the context's device; sizes are element counts.
+ *
+ * Conventions (same as the reference, src/types.jl):
+ *   - coordinates are (ndims, n) column-major: x1 y1 z1 x2 y2 z2 ...
+ *   - dtype 0 = Float32, 1 = Float64
+ *   - indices (senders, receivers, perm, node ids) are 1-based Int32
+ *   - rel_displacement is (ndims, n_edges) column-major, rel_dist_norm (1, n_edges)
+ *
+ * Every function returns an oct_status; on failure oct_ctx_last_error()
+ * describes it.  Calls on one context are not re-entrant.
+ */
+#ifndef OCTOPUS_B200_H
+#define OCTOPUS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OCT_API __attribute__((visibility("default")))
+
+/* Status codes.  The host binding maps them to the exception types the
+ * reference raises (src/api.jl, test/api.jl, test/backend_errors_cpu.jl). */
+typedef enum {
+    OCT_OK = 0,
+    OCT_ERR_ARGUMENT = 1,   /* ArgumentError */
+    OCT_ERR_DIMENSION = 2,  /* DimensionMismatch */
+    OCT_ERR_INEXACT = 3,    /* InexactError: floor(Int32, ...) in bin_point, src/morton.jl:84 */
+    OCT_ERR_CUDA = 4,       /* CUDA runtime failure */
+    OCT_ERR_OVERFLOW = 5,   /* internal capacity retry did not converge */
+    OCT_ERR_CAPACITY = 6,   /* caller buffer smaller than required */
+    OCT_ERR_TIMEOUT = 7,    /* a bounded device wait ran out */
+    OCT_ERR_STATE = 8       /* ErrorException: call order / missing build */
+} oct_status;
+
+typedef struct oct_ctx oct_ctx;   /* one device + one stream */
+typedef struct oct_tree oct_tree; /* one point set's search structure */
+
+/* Device views of a built tree: the DeviceView contract of
+ * ext/OctopusCUDAExt.jl:23-35 (node_first/last, node_children, bounds,
+ * perm), valid until the next oct_tree_build on the same tree. */
+typedef struct {
+    int64_t n_points;
+    int64_t n_nodes;
+    int32_t ndims;
+    int32_t dtype;
+    double radius;
+    const int32_t* node_first;    /* (n_nodes,) 1-based inclusive range into perm */
+    const int32_t* node_last;     /* (n_nodes,) */
+    const int32_t* node_children; /* (2^ndims, n_nodes) column-major, -1 = empty slot */
+    const void* bounds_min;       /* (ndims, n_nodes) column-major */
+    const void* bounds_max;       /* (ndims, n_nodes) column-major */
+    const int32_t* perm;          /* (n_points,) 1-based Morton order */
+    const uint64_t* morton;       /* (n_points,) per original point, or NULL unless keep_morton */
+} oct_tree_view;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+OCT_API int oct_version(void);
+
+/* Human-readable name of a status code. */
+OCT_API const char* oct_status_string(int status);
+
+/* Create a context on `device` using the legacy default stream.  Replaces the
+ * implicit CUDA.jl device/stream state the reference's extension uses
+ * (ext/OctopusCUDAExt.jl:6-17). */
+OCT_API int oct_ctx_create(int device, oct_ctx** out);
+OCT_API int oct_ctx_destroy(oct_ctx* ctx);
+
+/* Order all later work after the caller's stream (a cudaStream_t). */
+OCT_API int oct_ctx_set_stream(oct_ctx* ctx, void* stream);
+
+/* Message of the last failure on this context ("" when none). */
+OCT_API const char* oct_ctx_last_error(const oct_ctx* ctx);
+
+/* Block until all work issued on the context's stream has finished; also
+ * reports OCT_ERR_STATE if a kernel's bounds guard fired since the last
+ * oct_edges_count. */
+OCT_API int oct_synchronize(oct_ctx* ctx);
+
+/* A tree for one point set (the Octree of src/types.jl:23-42). */
+OCT_API int oct_tree_create(oct_ctx* ctx, int ndims, int dtype, oct_tree** out);
+OCT_API int oct_tree_destroy(oct_tree* tree);
+
+/* run! for one dirty point set: origin, Morton binning, stable key sort,
+ * BFS topology and bounds.  Replaces _build_gpu_tree!
+ * (ext/cuda_build.jl:227-288) called from _run_cuda!
+ * (ext/OctopusCUDAExt.jl:214-248) and reproduces the CPU build
+ * (src/api.jl:194-250) exactly.  `coords` is read during the call only.
+ * keep_morton != 0 retains the per-point Morton codes (set_refit_mode!,
+ * src/api.jl:43-47).  Returns OCT_ERR_INEXACT where the reference's
+ * floor(Int32, ...) throws InexactError (non-finite or out-of-range cell). */
+OCT_API int oct_tree_build(oct_ctx* ctx, oct_tree* tree, const void* coords, int64_t n,
+                           double radius, int keep_morton);
+
+/* Number of nodes of the last build (synchronizes). */
+OCT_API int oct_tree_n_nodes(oct_ctx* ctx, const oct_tree* tree, int64_t* n_nodes);
+
+/* Materialize the reference-layout arrays of a built tree.  Replaces
+ * _device_view (ext/OctopusCUDAExt.jl:37-56); the pointers are owned by the
+ * tree. */
+OCT_API int oct_tree_view_get(oct_ctx* ctx, oct_tree* tree, oct_tree_view* out);
+
+/* Pass A of build_edges for the pair (query, target): count neighbors per
+ * query point (self pair excluded when exclude_self != 0), scan, and
+ * return the edge total.  Replaces _count_edges_kernel! + cumsum! + the
+ * host read of n_edges (ext/OctopusCUDAExt.jl:262-288, 369-387). */
+OCT_API int oct_edges_count(oct_ctx* ctx, const oct_tree* query, const oct_tree* target,
+                            int exclude_self, int64_t* n_edges);
+
+/* Pass B of build_edges: write the flat COO of the last oct_edges_count on
+ * the same pair into caller-owned device buffers of at least `capacity`
+ * edges: senders (target j), receivers (query i), rel_displacement =
+ * (x_i - x_j) / r and rel_dist_norm = |x_i - x_j| / r, in the CPU path's
+ * order.  Replaces _fill_edges_kernel_{3d,2d}! (ext/OctopusCUDAExt.jl:290-343,
+ * 401-411). */
+OCT_API int oct_edges_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* target,
+                           int exclude_self, int32_t* senders, int32_t* receivers,
+                           void* rel_displacement, void* rel_dist_norm, int64_t capacity);
+
+/* Neighbors of n_queries points (device coords, (ndims, n_queries)) in the
+ * target tree, in the reference's traversal order and without the self
+ * filter: the host for_each_neighbor / get_neighborlist accessors
+ * (src/cpu/iterator_cpu.jl:245-263, src/api.jl:282-292).  Writes
+ * out_counts[q] and up to cap_per_query 1-based indices per query at
+ * out_indices[q * cap_per_query ...]. */
+OCT_API int oct_neighbors(oct_ctx* ctx, const oct_tree* target, const void* query_coords,
+                          int64_t n_queries, int32_t* out_counts, int32_t* out_indices,
+                          int64_t cap_per_query);
+
+/* Pullback of build_edges_diff for a self pair: grad_coords (ndims, n_points)
+ * = sum over edges of (+c on the receiver, -c on the sender) with
+ * c = d_rel_displacement / r + rel_displacement * d_rel_dist_norm /
+ * (rel_dist_norm * r) (distance term skipped when rel_dist_norm <= 1e-8).
+ * Either cotangent may be NULL (zero).  Deterministic (no float atomics).
+ * Replaces _build_edges_diff_pullback_kernel!
+ * (ext/OctopusCUDAChainRulesCoreExt.jl:56-99) and matches the CPU rrule
+ * (ext/OctopusChainRulesCoreExt.jl:137-192). */
+OCT_API int oct_edges_diff_backward(oct_ctx* ctx, int ndims, int dtype, int64_t n_points,
+                                    int64_t n_edges, const int32_t* senders,
+                                    const int32_t* receivers, const void* rel_displacement,
+                                    const void* rel_dist_norm, const void* d_rel_displacement,
+                                    const void* d_rel_dist_norm, double radius, void* grad_coords);
+
+/* Per-phase device timing with CUDA events on the context's stream (the
+ * phase timers of benchmarks/profile_phases.jl:29-46, taken on the device).
+ * While enabled, every library call records its phases; oct_profile_read
+ * synchronizes, returns the summed milliseconds and record counts per phase
+ * (indices 0..n_phases-1, named by oct_profile_phase_name) and clears them. */
+OCT_API int oct_profile_enable(oct_ctx* ctx, int on);
+OCT_API const char* oct_profile_phase_name(int phase);
+OCT_API int oct_profile_read(oct_ctx* ctx, double* ms, int64_t* launches, int n_phases);
+
+/* Number of kernels this context has launched since it was created. */
+OCT_API int64_t oct_profile_kernel_launches(const oct_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OCTOPUS_B200_H */

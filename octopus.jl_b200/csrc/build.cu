@@ -1,0 +1,601 @@
+// Device-resident tree build: bounds reduce -> Morton encode -> stable LSD
+// radix sort -> sorted point gather -> BFS topology -> bottom-up bounds.
+//
+// Replaces _build_gpu_tree! (ext/cuda_build.jl:227-288) and reproduces the
+// CPU build exactly (src/cpu/bin_cpu.jl, src/sort.jl, src/cpu/build_cpu.jl,
+// src/cpu/refit_cpu.jl): the same keys, the same stable order, the same
+// leaves and BFS node numbering, and bit-identical bounds.
+//
+// Topology without per-level launches: a node at level L starts at sorted
+// position k iff the level-L key prefix changes at k and the level-(L-1)
+// group containing k holds more than 32 points (or k is the root).  A group
+// holds more than 32 points iff some window of 33 consecutive positions
+// around k shares its prefix, which one pass over the sorted keys detects.
+// Each position therefore owns a contiguous range of levels [lo, hi], with
+// hi the level of the leaf that contains it.  BFS ids are level-major,
+// position-minor, so they come from one exclusive scan of per-block,
+// per-level node counts; children of a node are consecutive ids.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "internal.h"
+#include "scan.cuh"
+#include "sort.cuh"
+
+namespace oct {
+
+constexpr int kThreads = 256;
+
+// ------------------------------------------------------------ 1. bounds --
+// Per-axis min/max (Julia min/max order) and a non-finite flag.  The last
+// block to finish folds the per-block partials into the header.
+template <class T, int D>
+__global__ void __launch_bounds__(kThreads) k_bounds(const T* __restrict__ coords, int64_t n,
+                                                     double* __restrict__ partials, OctHeader* hdr) {
+    __shared__ T smin[kThreads / 32][D], smax[kThreads / 32][D];
+    __shared__ int snan;
+    __shared__ bool is_last;
+    if (threadIdx.x == 0) snan = 0;
+    __syncthreads();
+    T lo[D], hi[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) { lo[d] = T(INFINITY); hi[d] = T(-INFINITY); }
+    int bad = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const T x = coords[D * i + d];
+            if (!isfinite(x)) bad = 1;
+            lo[d] = jl_min(lo[d], x);
+            hi[d] = jl_max(hi[d], x);
+        }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        lo[d] = warp_min(lo[d]);
+        hi[d] = warp_max(hi[d]);
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&snan, 1);
+    if (lane == 0) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) { smin[w][d] = lo[d]; smax[w][d] = hi[d]; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w2 = 1; w2 < kThreads / 32; ++w2)
+            for (int d = 0; d < D; ++d) {
+                smin[0][d] = jl_min(smin[0][d], smin[w2][d]);
+                smax[0][d] = jl_max(smax[0][d], smax[w2][d]);
+            }
+        double* p = partials + (size_t)blockIdx.x * 8;
+        for (int d = 0; d < D; ++d) { p[d] = (double)smin[0][d]; p[3 + d] = (double)smax[0][d]; }
+        p[6] = snan ? 1.0 : 0.0;
+        __threadfence();
+        const int ticket = atomicAdd(&hdr->n_blocks_done, 1);
+        is_last = (ticket == (int)gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        __threadfence();
+        T glo[D], ghi[D];
+        for (int d = 0; d < D; ++d) { glo[d] = T(INFINITY); ghi[d] = T(-INFINITY); }
+        int anynan = 0;
+        for (unsigned b = 0; b < gridDim.x; ++b) {
+            const volatile double* p = partials + (size_t)b * 8;
+            for (int d = 0; d < D; ++d) {
+                glo[d] = jl_min(glo[d], (T)p[d]);
+                ghi[d] = jl_max(ghi[d], (T)p[3 + d]);
+            }
+            if (p[6] != 0.0) anynan = 1;
+        }
+        for (int d = 0; d < D; ++d) { hdr->gmin[d] = (double)glo[d]; hdr->gmax[d] = (double)ghi[d]; }
+        hdr->nan_flag = anynan;
+        hdr->n_blocks_done = 0;
+    }
+}
+
+// ------------------------------------------------------------ 2. encode --
+// bin_point + clamp + morton_encode (src/cpu/bin_cpu.jl:52-95).  The host has
+// already proven every cell index fits Int32 (the max coordinate bins last).
+template <class T, int D, class K>
+__global__ void __launch_bounds__(kThreads) k_encode(const T* __restrict__ coords, int64_t n, T o0, T o1, T o2,
+                                                     T inv_cs, K* __restrict__ keys,
+                                                     uint64_t* __restrict__ morton_out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T o[3] = {o0, o1, o2};
+    constexpr int64_t cmax = (1LL << Dims<D>::bits) - 1;
+    uint64_t c[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const T v = mul_rn(sub_rn(coords[D * i + d], o[d]), inv_cs);
+        int64_t ci = (int64_t)floor(v);
+        ci = ci < 0 ? 0 : (ci > cmax ? cmax : ci);
+        c[d] = (uint64_t)ci;
+    }
+    const uint64_t key = (D == 3) ? ((split_by_3(c[2]) << 2) | (split_by_3(c[1]) << 1) | split_by_3(c[0]))
+                                  : ((split_by_2(c[1]) << 1) | split_by_2(c[0]));
+    keys[i] = (K)key;
+    if (morton_out) morton_out[i] = key;
+}
+
+// ------------------------------------------------------------ 4. gather --
+template <class T, int D>
+__global__ void __launch_bounds__(kThreads) k_gather(const T* __restrict__ coords, const int32_t* __restrict__ perm,
+                                                     int64_t n, SPt<T, D>* __restrict__ spts) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int32_t j = perm ? perm[k] : (int32_t)k;
+    SPt<T, D> p;
+#pragma unroll
+    for (int d = 0; d < D; ++d) p.x[d] = coords[(int64_t)D * j + d];
+    p.idx = j;
+    spts[k] = p;
+}
+
+// ---------------------------------------------------------- 5. topology --
+// Number of leading D-bit digits (of Dims<D>::bits) two keys share.
+template <int D, class K> __device__ __forceinline__ int common_levels(K a, K b) {
+    const uint64_t x = (uint64_t)(a ^ b);
+    if (x == 0) return Dims<D>::bits;
+    const int hb = 63 - __clzll((long long)x);
+    return Dims<D>::bits - 1 - hb / D;
+}
+
+constexpr int kMarkTile = kThreads;  // positions per block in mark / emit
+
+// lohi[k] = lo | hi << 8: the levels whose node starts at position k are
+// lo..hi (empty when lo > hi); hi is the level of the leaf containing k
+// (src/cpu/build_cpu.jl:146: leaf iff count <= 32 or level >= max_levels).
+template <int D, class K>
+__global__ void __launch_bounds__(kThreads) k_mark(const K* __restrict__ skeys, int64_t n,
+                                                   uint16_t* __restrict__ lohi, int32_t* __restrict__ blockcnt,
+                                                   int nblocks) {
+    constexpr int MAXLEV = Dims<D>::bits;
+    constexpr int NLEV = MAXLEV + 1;
+    __shared__ K sk[kMarkTile + 64];
+    __shared__ int8_t sc[kMarkTile + 32];
+    __shared__ int32_t wcnt[NLEV][kThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kMarkTile;
+    for (int i = threadIdx.x; i < kMarkTile + 64; i += kThreads) {
+        const int64_t p = base - 32 + i;
+        sk[i] = (p >= 0 && p < n) ? skeys[p] : K(0);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kMarkTile + 32; i += kThreads) {
+        const int64_t j = base - 32 + i;
+        sc[i] = (j >= 0 && j + 32 <= n - 1) ? (int8_t)common_levels<D, K>(sk[i], sk[i + 32]) : (int8_t)-1;
+    }
+    __syncthreads();
+    const int64_t k = base + threadIdx.x;
+    int lo = 1, hi = 0;
+    if (k < n) {
+        lo = (k == 0) ? 0 : common_levels<D, K>(sk[threadIdx.x + 31], sk[threadIdx.x + 32]) + 1;
+        int m = -1;
+#pragma unroll 11
+        for (int t = 0; t <= 32; ++t) m = max(m, (int)sc[threadIdx.x + t]);
+        hi = min(m + 1, MAXLEV);
+        lohi[k] = (uint16_t)(lo | (hi << 8));
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int L = 0; L < NLEV; ++L) {
+        const unsigned b = __ballot_sync(0xffffffffu, lo <= L && L <= hi);
+        if (lane == 0) wcnt[L][w] = __popc(b);
+    }
+    __syncthreads();
+    if (threadIdx.x < NLEV) {
+        int s = 0;
+#pragma unroll
+        for (int j = 0; j < kThreads / 32; ++j) s += wcnt[threadIdx.x][j];
+        blockcnt[(int64_t)threadIdx.x * nblocks + blockIdx.x] = s;
+    }
+}
+
+// Writes node (L, k) with BFS id `id`.  first_child < 0 marks a leaf.
+template <class T, int D, class K>
+__device__ void emit_node(const K* __restrict__ skeys, int64_t n, int L, int64_t k, int32_t id,
+                          int32_t first_child, TNode<T, D>* __restrict__ tnode, int2* __restrict__ nrange,
+                          int32_t* __restrict__ parent, int32_t* __restrict__ arrive, const OctHeader* hdr) {
+    constexpr int BITS = Dims<D>::bits;
+    constexpr int NCH = Dims<D>::nch;
+    int64_t e = n;
+    if (L > 0) {
+        const int sh = D * (BITS - L);
+        const uint64_t pk = (uint64_t)skeys[k] >> sh;
+        int64_t good = k, bad = n, step = 1;
+        while (true) {
+            const int64_t p = k + step;
+            if (p >= n) break;
+            if (((uint64_t)skeys[p] >> sh) != pk) { bad = p; break; }
+            good = p;
+            step <<= 1;
+        }
+        int64_t a = good + 1, b = bad;
+        while (a < b) {
+            const int64_t mid = (a + b) >> 1;
+            if (((uint64_t)skeys[mid] >> sh) != pk) b = mid; else a = mid + 1;
+        }
+        e = a;
+    }
+    TNode<T, D> nd;
+    if (first_child < 0) {
+        nd.a = (int32_t)k;
+        nd.b = (int32_t)(e - k);
+    } else {
+        const int shd = D * BITS - D * (L + 1);
+        const uint64_t msk = (uint64_t)(NCH - 1);
+        const int d0 = (int)(((uint64_t)skeys[k] >> shd) & msk);
+        const int d1 = (int)(((uint64_t)skeys[e - 1] >> shd) & msk);
+        unsigned slots = 1u << d0;
+        if (d1 != d0) {
+            // Boundaries bnd[v] = first position in [k, e) whose digit >= v.
+            int64_t prev = k;
+            for (int v = d0 + 1; v <= d1; ++v) {
+                int64_t a = prev, b = e;
+                while (a < b) {
+                    const int64_t mid = (a + b) >> 1;
+                    if ((int)(((uint64_t)skeys[mid] >> shd) & msk) >= v) b = mid; else a = mid + 1;
+                }
+                // Digit v is present iff the next boundary is beyond this one.
+                int64_t a2 = a, b2 = e;
+                while (a2 < b2) {
+                    const int64_t mid = (a2 + b2) >> 1;
+                    if ((int)(((uint64_t)skeys[mid] >> shd) & msk) >= v + 1) b2 = mid; else a2 = mid + 1;
+                }
+                if (a2 > a) slots |= 1u << v;
+                prev = a;
+            }
+        }
+        nd.a = first_child;
+        nd.b = -(int32_t)slots;
+        const int nc = __popc(slots);
+        for (int j = 0; j < nc; ++j) parent[first_child + j] = id;
+    }
+    if (k == 0 && e == n) {
+        // A node covering every point has the global bounds.
+#pragma unroll
+        for (int d = 0; d < D; ++d) { nd.lo[d] = (T)hdr->gmin[d]; nd.hi[d] = (T)hdr->gmax[d]; }
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) { nd.lo[d] = T(0); nd.hi[d] = T(0); }
+    }
+    tnode[id] = nd;
+    nrange[id] = make_int2((int)k, (int)(e - 1));
+    arrive[id] = 0;
+    if (id == 0) parent[0] = -1;
+}
+
+template <class T, int D, class K>
+__global__ void __launch_bounds__(kThreads) k_emit(const K* __restrict__ skeys, int64_t n,
+                                                   const uint16_t* __restrict__ lohi,
+                                                   const int64_t* __restrict__ blockoff, int nblocks,
+                                                   int64_t capacity, TNode<T, D>* __restrict__ tnode,
+                                                   int2* __restrict__ nrange, int32_t* __restrict__ parent,
+                                                   int32_t* __restrict__ arrive, OctHeader* hdr) {
+    constexpr int NLEV = Dims<D>::bits + 1;
+    __shared__ int32_t wpre[NLEV][kThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t k = (int64_t)blockIdx.x * kMarkTile + threadIdx.x;
+    int lo = 1, hi = 0;
+    if (k < n) {
+        const uint16_t v = lohi[k];
+        lo = v & 0xff;
+        hi = v >> 8;
+    }
+    for (int L = 0; L < NLEV; ++L) {
+        const unsigned b = __ballot_sync(0xffffffffu, lo <= L && L <= hi);
+        if (lane == 0) wpre[L][w] = __popc(b);
+    }
+    __syncthreads();
+    if (threadIdx.x < NLEV) {
+        int run = 0;
+#pragma unroll
+        for (int j = 0; j < kThreads / 32; ++j) {
+            const int c = wpre[threadIdx.x][j];
+            wpre[threadIdx.x][j] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    if (hdr->n_nodes > capacity) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&hdr->status, (int)DF_NODE_OVERFLOW);
+        return;
+    }
+    int32_t prev = -1;
+    for (int L = NLEV - 1; L >= 0; --L) {
+        const bool in = lo <= L && L <= hi;
+        const unsigned b = __ballot_sync(0xffffffffu, in);
+        if (in) {
+            const int32_t id = (int32_t)(blockoff[(int64_t)L * nblocks + blockIdx.x] + wpre[L][w] +
+                                         __popc(b & lanemask_lt()));
+            emit_node<T, D, K>(skeys, n, L, k, id, L < hi ? prev : -1, tnode, nrange, parent, arrive, hdr);
+            prev = id;
+        }
+    }
+}
+
+// ------------------------------------------------------------- 6. refit --
+// Leaves fold their points (src/cpu/refit_cpu.jl:39-48); the last child to
+// arrive at a parent folds the children (src/cpu/refit_cpu.jl:50-60).  No
+// thread waits: a thread that is not last simply stops.
+template <class T, int D>
+__global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n, TNode<T, D>* tnode,
+                                                    const int2* __restrict__ nrange, const int32_t* __restrict__ parent,
+                                                    int32_t* arrive, const SPt<T, D>* __restrict__ spts,
+                                                    const OctHeader* hdr) {
+    const int64_t nn = hdr->n_nodes;
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (nn > capacity || id >= nn) return;
+    const int32_t a = tnode[id].a, b = tnode[id].b;
+    if (b <= 0) return;
+    T lo[D], hi[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) { lo[d] = T(INFINITY); hi[d] = T(-INFINITY); }
+    for (int32_t m = a; m < a + b; ++m) {
+        const SPt<T, D> p = spts[m];
+#pragma unroll
+        for (int d = 0; d < D; ++d) { lo[d] = jl_min(lo[d], p.x[d]); hi[d] = jl_max(hi[d], p.x[d]); }
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) { tnode[id].lo[d] = lo[d]; tnode[id].hi[d] = hi[d]; }
+    int32_t node = (int32_t)id;
+    while (true) {
+        const int32_t p = parent[node];
+        if (p < 0) break;
+        const int2 rg = nrange[p];
+        if (rg.x == 0 && (int64_t)rg.y == n - 1) break;  // bounds preset from the global reduce
+        const int32_t pa = tnode[p].a, pb = tnode[p].b;
+        const int nc = __popc((unsigned)(-pb));
+        __threadfence();
+        const int old = atomicAdd(&arrive[p], 1);
+        if (old != nc - 1) break;
+        __threadfence();
+#pragma unroll
+        for (int d = 0; d < D; ++d) { lo[d] = T(INFINITY); hi[d] = T(-INFINITY); }
+        for (int c = 0; c < nc; ++c) {
+            const TNode<T, D>* cn = tnode + pa + c;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                lo[d] = jl_min(lo[d], __ldcg(&cn->lo[d]));
+                hi[d] = jl_max(hi[d], __ldcg(&cn->hi[d]));
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) { tnode[p].lo[d] = lo[d]; tnode[p].hi[d] = hi[d]; }
+        node = p;
+    }
+}
+
+// --------------------------------------------------- 7. reference views --
+template <class T, int D>
+__global__ void k_view_nodes(const TNode<T, D>* __restrict__ tnode, const int2* __restrict__ nrange, int64_t nn,
+                             int32_t* __restrict__ vf, int32_t* __restrict__ vl, int32_t* __restrict__ vc,
+                             T* __restrict__ vmin, T* __restrict__ vmax) {
+    constexpr int NCH = Dims<D>::nch;
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nn) return;
+    const TNode<T, D> nd = tnode[id];
+    const int2 rg = nrange[id];
+    vf[id] = rg.x + 1;
+    vl[id] = rg.y + 1;
+    int j = 0;
+    for (int c = 0; c < NCH; ++c) {
+        int32_t v = -1;
+        if (nd.b < 0 && (((unsigned)(-nd.b) >> c) & 1u)) v = nd.a + (j++) + 1;
+        vc[id * NCH + c] = v;
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) { vmin[id * D + d] = nd.lo[d]; vmax[id * D + d] = nd.hi[d]; }
+}
+
+template <class T, int D>
+__global__ void k_view_perm(const SPt<T, D>* __restrict__ spts, int64_t n, int32_t* __restrict__ vp) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) vp[k] = spts[k].idx + 1;
+}
+
+// ------------------------------------------------------------- host side --
+namespace {
+
+template <class T, int D, class K>
+int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
+    cudaStream_t s = ctx.stream;
+    cudaError_t err;
+    constexpr int BITS = Dims<D>::bits;
+    constexpr int NLEV = BITS + 1;
+    const T inv_cs = T(1) / radius;  // src/cpu/bin_cpu.jl:60
+    T o[3] = {T(0), T(0), T(0)};
+    for (int d = 0; d < D; ++d) o[d] = (T)t.origin[d];
+
+    // --- encode
+    if ((err = ensure(t.keys[0], (size_t)n * sizeof(K))) || (err = ensure(t.keys[1], (size_t)n * sizeof(K))) ||
+        (err = ensure(t.vals[0], (size_t)n * 4)) || (err = ensure(t.vals[1], (size_t)n * 4)))
+        return cuda_status(ctx, err, "allocating sort buffers");
+    uint64_t* morton = nullptr;
+    if (t.keep_morton) {
+        if ((err = ensure(t.morton, (size_t)n * 8))) return cuda_status(ctx, err, "allocating morton codes");
+        morton = t.morton.as<uint64_t>();
+    }
+    {
+        PhaseTimer pt_(ctx, PH_ENCODE);
+        k_encode<T, D, K><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, n, o[0], o[1], o[2], inv_cs,
+                                                                    t.keys[0].as<K>(), morton);
+        ctx.kernel_launches += 1;
+    }
+
+    // --- sort (stable: ties keep ascending original index, src/sort.jl:15-24)
+    if ((err = ensure(t.hist, (size_t)256 * sort_tiles(n) * 4))) return cuda_status(ctx, err, "allocating histograms");
+    K* kb[2] = {t.keys[0].as<K>(), t.keys[1].as<K>()};
+    int32_t* vb[2] = {t.vals[0].as<int32_t>(), t.vals[1].as<int32_t>()};
+    int src;
+    {
+        PhaseTimer pt_(ctx, PH_SORT);
+        src = radix_sort_pairs<K>(kb, vb, t.hist.as<int32_t>(), n, t.key_bits, false, s);
+        ctx.kernel_launches += 3 * t.sort_passes;
+    }
+    const K* skeys = kb[src];
+    const int32_t* perm = t.sort_passes ? vb[src] : nullptr;
+
+    // --- sorted points
+    if ((err = ensure(t.spts, (size_t)n * sizeof(SPt<T, D>)))) return cuda_status(ctx, err, "allocating points");
+    {
+        PhaseTimer pt_(ctx, PH_GATHER);
+        k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, perm, n, t.spts.as<SPt<T, D>>());
+        ctx.kernel_launches += 1;
+    }
+
+    // --- topology + refit (retried once with the exact node count on overflow)
+    const int nblocks = div_up(n, kMarkTile);
+    t.n_mark_blocks = nblocks;
+    const int64_t nbc = (int64_t)NLEV * nblocks;
+    if ((err = ensure(t.lohi, (size_t)n * 2)) || (err = ensure(t.blockcnt, (size_t)nbc * 4)) ||
+        (err = ensure(t.blockoff, (size_t)(nbc + 1) * 8)) ||
+        (err = ensure(t.scan_tmp, (size_t)scan_tmp_elems(nbc) * 8)))
+        return cuda_status(ctx, err, "allocating topology scratch");
+    int64_t est = (int64_t)Dims<D>::nch * ((n + 31) / 32) + 2 * NLEV + 64;
+    if (t.capacity < est) t.capacity = est;
+    OctHeader* hdr = t.hdr.as<OctHeader>();
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        const int64_t cap = t.capacity;
+        if ((err = ensure(t.tnode, (size_t)cap * sizeof(TNode<T, D>))) || (err = ensure(t.nrange, (size_t)cap * 8)) ||
+            (err = ensure(t.parent, (size_t)cap * 4)) || (err = ensure(t.arrive, (size_t)cap * 4)))
+            return cuda_status(ctx, err, "allocating node arrays");
+        {
+        PhaseTimer pt_(ctx, PH_TOPOLOGY);
+        k_mark<D, K><<<nblocks, kThreads, 0, s>>>(skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(), nblocks);
+        exclusive_scan_i32_i64(t.blockcnt.as<int32_t>(), t.blockoff.as<int64_t>(), nbc, &hdr->n_nodes,
+                               t.scan_tmp.as<int64_t>(), s);
+        k_emit<T, D, K><<<nblocks, kThreads, 0, s>>>(skeys, n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks,
+                                                     cap, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
+                                                     t.parent.as<int32_t>(), t.arrive.as<int32_t>(), hdr);
+        ctx.kernel_launches += 5;
+        }
+        {
+        PhaseTimer pt_(ctx, PH_REFIT);
+        k_refit<T, D><<<div_up(cap, kThreads), kThreads, 0, s>>>(cap, n, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
+                                                                  t.parent.as<int32_t>(), t.arrive.as<int32_t>(),
+                                                                  t.spts.as<SPt<T, D>>(), hdr);
+        ctx.kernel_launches += 1;
+        }
+        if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
+            (err = cudaStreamSynchronize(s)))
+            return cuda_status(ctx, err, "tree build");
+        if (t.hdr_host->status & DF_NODE_OVERFLOW) {
+            t.capacity = t.hdr_host->n_nodes + t.hdr_host->n_nodes / 8 + 64;
+            const int zero = 0;
+            cudaMemcpyAsync(&hdr->status, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
+            continue;
+        }
+        t.n_nodes = t.hdr_host->n_nodes;
+        return OK;
+    }
+    return set_error(ctx, ERR_OVERFLOW, "tree build: node capacity retry did not converge");
+}
+
+template <class T, int D>
+int build_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, double radius_d) {
+    cudaStream_t s = ctx.stream;
+    cudaError_t err;
+    const T radius = (T)radius_d;
+    if ((err = ensure(t.hdr, sizeof(OctHeader)))) return cuda_status(ctx, err, "allocating header");
+    if (!t.hdr_host) {
+        if ((err = cudaMallocHost((void**)&t.hdr_host, sizeof(OctHeader)))) return cuda_status(ctx, err, "pinned header");
+    }
+    OctHeader* hdr = t.hdr.as<OctHeader>();
+    if ((err = cudaMemsetAsync(hdr, 0, sizeof(OctHeader), s))) return cuda_status(ctx, err, "header reset");
+
+    // --- 1. bounds (one host round trip, like ext/cuda_build.jl:235)
+    const int nb = std::max(1, std::min(div_up(n, kThreads * 8), 4 * 148));
+    if ((err = ensure(t.partials, (size_t)nb * 8 * 8))) return cuda_status(ctx, err, "allocating partials");
+    {
+        PhaseTimer pt_(ctx, PH_BOUNDS);
+        k_bounds<T, D><<<nb, kThreads, 0, s>>>(coords, n, t.partials.as<double>(), hdr);
+        ctx.kernel_launches += 1;
+    }
+    if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
+        (err = cudaStreamSynchronize(s)))
+        return cuda_status(ctx, err, "bounds reduce");
+    if (t.hdr_host->nan_flag)
+        return set_error(ctx, ERR_INEXACT, "InexactError: floor(Int32, NaN/Inf) in bin_point (non-finite coordinate)");
+
+    // --- origin and key width on the host, in T (src/cpu/bin_cpu.jl:22,35,60)
+    const T inv_cs = T(1) / radius;
+    int64_t cmax_all = 0;
+    for (int d = 0; d < D; ++d) {
+        const T o = (T)t.hdr_host->gmin[d] - T(1e-6);
+        t.origin[d] = (double)o;
+        const T v = ((T)t.hdr_host->gmax[d] - o) * inv_cs;
+        const T f = std::floor(v);
+        if (!(f >= T(-2147483648.0) && f < T(2147483648.0)))
+            return set_error(ctx, ERR_INEXACT, "InexactError: floor(Int32, (p - origin) / radius) exceeds Int32");
+        int64_t c = (int64_t)f;
+        const int64_t cm = (1LL << Dims<D>::bits) - 1;
+        c = c < 0 ? 0 : (c > cm ? cm : c);
+        cmax_all = std::max(cmax_all, c);
+    }
+    int nbits_axis = 0;
+    while (nbits_axis < 63 && (cmax_all >> nbits_axis) != 0) ++nbits_axis;
+    t.key_bits = D * nbits_axis;
+    t.key_bytes = t.key_bits <= 32 ? 4 : 8;
+    t.sort_passes = (t.key_bits + 7) / 8;
+    if (t.key_bytes == 4) return run_pipeline<T, D, uint32_t>(ctx, t, coords, n, radius);
+    return run_pipeline<T, D, uint64_t>(ctx, t, coords, n, radius);
+}
+
+}  // namespace
+
+int build_tree(Ctx& ctx, Tree& t, const void* coords, int64_t n, double radius) {
+    t.built = false;
+    t.view_valid = false;
+    t.n = n;
+    t.radius = radius;
+    ++t.generation;
+    if (n == 0) {
+        t.n_nodes = 0;
+        t.built = true;
+        return OK;
+    }
+    int st;
+    if (t.dtype == 0)
+        st = t.ndims == 3 ? build_typed<float, 3>(ctx, t, (const float*)coords, n, radius)
+                          : build_typed<float, 2>(ctx, t, (const float*)coords, n, radius);
+    else
+        st = t.ndims == 3 ? build_typed<double, 3>(ctx, t, (const double*)coords, n, radius)
+                          : build_typed<double, 2>(ctx, t, (const double*)coords, n, radius);
+    if (st == OK) t.built = true;
+    return st;
+}
+
+namespace {
+template <class T, int D>
+int view_typed(Ctx& ctx, Tree& t) {
+    cudaError_t err;
+    const int64_t nn = std::max<int64_t>(t.n_nodes, 1), n = std::max<int64_t>(t.n, 1);
+    constexpr int NCH = Dims<D>::nch;
+    if ((err = ensure(t.v_first, nn * 4)) || (err = ensure(t.v_last, nn * 4)) || (err = ensure(t.v_children, nn * 4 * NCH)) ||
+        (err = ensure(t.v_bmin, nn * sizeof(T) * D)) || (err = ensure(t.v_bmax, nn * sizeof(T) * D)) ||
+        (err = ensure(t.v_perm, n * 4)))
+        return cuda_status(ctx, err, "allocating views");
+    if (t.n_nodes > 0)
+        k_view_nodes<T, D><<<div_up(t.n_nodes, kThreads), kThreads, 0, ctx.stream>>>(
+            t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(), t.n_nodes, t.v_first.as<int32_t>(), t.v_last.as<int32_t>(),
+            t.v_children.as<int32_t>(), t.v_bmin.as<T>(), t.v_bmax.as<T>());
+    if (t.n > 0)
+        k_view_perm<T, D><<<div_up(t.n, kThreads), kThreads, 0, ctx.stream>>>(t.spts.as<SPt<T, D>>(), t.n,
+                                                                               t.v_perm.as<int32_t>());
+    if ((err = cudaStreamSynchronize(ctx.stream))) return cuda_status(ctx, err, "materializing views");
+    t.view_valid = true;
+    return OK;
+}
+}  // namespace
+
+int materialize_view(Ctx& ctx, Tree& t) {
+    if (t.view_valid) return OK;
+    if (t.dtype == 0) return t.ndims == 3 ? view_typed<float, 3>(ctx, t) : view_typed<float, 2>(ctx, t);
+    return t.ndims == 3 ? view_typed<double, 3>(ctx, t) : view_typed<double, 2>(ctx, t);
+}
+
+}  // namespace oct

@@ -1,0 +1,356 @@
+// C ABI (include/octopus_b200.h): argument checks, object lifetime and error
+// reporting around the build / edge / adjoint pipelines.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/octopus_b200.h"
+#include "internal.h"
+
+struct oct_ctx {
+    oct::Ctx c;
+};
+struct oct_tree {
+    oct::Tree t;
+    oct_ctx* owner = nullptr;
+};
+
+namespace oct {
+
+cudaError_t ensure(DevBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return cudaSuccess;
+    if (b.p) {
+        cudaError_t e = cudaFree(b.p);
+        if (e != cudaSuccess) return e;
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    const size_t want = bytes + bytes / 8;  // slack so slowly growing inputs do not reallocate every call
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return e;
+    }
+    b.bytes = want;
+    return cudaSuccess;
+}
+
+void release(DevBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+cudaEvent_t Ctx::get_event() {
+    if (!event_pool.empty()) {
+        cudaEvent_t e = event_pool.back();
+        event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+PhaseTimer::PhaseTimer(Ctx& c, int ph) : ctx(&c), phase(ph) {
+    if (!c.profiling) return;
+    start = c.get_event();
+    cudaEventRecord(start, c.stream);
+}
+
+PhaseTimer::~PhaseTimer() {
+    if (!start) return;
+    cudaEvent_t stop = ctx->get_event();
+    cudaEventRecord(stop, ctx->stream);
+    ctx->prof.push_back({phase, start, stop});
+}
+
+int set_error(Ctx& ctx, int status, const std::string& msg) {
+    ctx.last_error = msg;
+    return status;
+}
+
+int cuda_status(Ctx& ctx, cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return OK;
+    ctx.last_error = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return ERR_CUDA;
+}
+
+}  // namespace oct
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void release_tree(oct::Tree& t) {
+    using oct::release;
+    for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.spts, &t.tnode, &t.nrange,
+                    &t.parent, &t.arrive, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
+                    &t.morton, &t.v_first, &t.v_last, &t.v_children, &t.v_bmin, &t.v_bmax, &t.v_perm})
+        release(*b);
+    if (t.hdr_host) cudaFreeHost(t.hdr_host);
+    t.hdr_host = nullptr;
+}
+
+bool bad_dims(int ndims) { return ndims != 2 && ndims != 3; }
+bool bad_dtype(int dtype) { return dtype != 0 && dtype != 1; }
+
+}  // namespace
+
+extern "C" {
+
+OCT_API int oct_version(void) { return 1 * 10000 + 0 * 100 + 0; }
+
+OCT_API const char* oct_status_string(int status) {
+    switch (status) {
+        case OCT_OK: return "ok";
+        case OCT_ERR_ARGUMENT: return "ArgumentError";
+        case OCT_ERR_DIMENSION: return "DimensionMismatch";
+        case OCT_ERR_INEXACT: return "InexactError";
+        case OCT_ERR_CUDA: return "CUDA error";
+        case OCT_ERR_OVERFLOW: return "capacity overflow";
+        case OCT_ERR_CAPACITY: return "buffer too small";
+        case OCT_ERR_TIMEOUT: return "device wait timed out";
+        case OCT_ERR_STATE: return "ErrorException";
+        default: return "unknown status";
+    }
+}
+
+OCT_API int oct_ctx_create(int device, oct_ctx** out) {
+    if (!out) return OCT_ERR_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return OCT_ERR_CUDA;
+    if (device < 0 || device >= ndev) return OCT_ERR_ARGUMENT;
+    oct_ctx* c = new (std::nothrow) oct_ctx();
+    if (!c) return OCT_ERR_CUDA;
+    c->c.device = device;
+    c->c.stream = nullptr;
+    *out = c;
+    return OCT_OK;
+}
+
+OCT_API int oct_ctx_destroy(oct_ctx* ctx) {
+    if (!ctx) return OCT_OK;
+    DeviceGuard g(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    using oct::release;
+    for (auto* b : {&ctx->c.counts, &ctx->c.offsets, &ctx->c.scan_tmp, &ctx->c.total, &ctx->c.dkeys[0],
+                    &ctx->c.dkeys[1], &ctx->c.dvals[0], &ctx->c.dvals[1], &ctx->c.dhist, &ctx->c.droff,
+                    &ctx->c.dsoff, &ctx->c.dstatus})
+        release(*b);
+    if (ctx->c.total_host) cudaFreeHost(ctx->c.total_host);
+    for (auto& r : ctx->c.prof) {
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    for (auto e : ctx->c.event_pool) cudaEventDestroy(e);
+    delete ctx;
+    return OCT_OK;
+}
+
+OCT_API int oct_ctx_set_stream(oct_ctx* ctx, void* stream) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.stream = (cudaStream_t)stream;
+    return OCT_OK;
+}
+
+OCT_API const char* oct_ctx_last_error(const oct_ctx* ctx) { return ctx ? ctx->c.last_error.c_str() : ""; }
+
+OCT_API int oct_synchronize(oct_ctx* ctx) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    DeviceGuard g(ctx->c.device);
+    int st = oct::cuda_status(ctx->c, cudaStreamSynchronize(ctx->c.stream), "synchronize");
+    if (st != OCT_OK || !ctx->c.dstatus.p) return st;
+    int word = 0;
+    st = oct::cuda_status(ctx->c, cudaMemcpy(&word, ctx->c.dstatus.p, 4, cudaMemcpyDeviceToHost), "status read");
+    if (st != OCT_OK) return st;
+    if (word != 0)
+        return oct::set_error(ctx->c, OCT_ERR_STATE, "edge fill found more neighbors than counted (internal error)");
+    return OCT_OK;
+}
+
+OCT_API int oct_tree_create(oct_ctx* ctx, int ndims, int dtype, oct_tree** out) {
+    if (!ctx || !out) return OCT_ERR_ARGUMENT;
+    *out = nullptr;
+    if (bad_dims(ndims)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "ndims must be 2 or 3");
+    if (bad_dtype(dtype)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "dtype must be 0 (Float32) or 1 (Float64)");
+    oct_tree* t = new (std::nothrow) oct_tree();
+    if (!t) return OCT_ERR_CUDA;
+    t->t.ndims = ndims;
+    t->t.dtype = dtype;
+    t->owner = ctx;
+    *out = t;
+    return OCT_OK;
+}
+
+OCT_API int oct_tree_destroy(oct_tree* tree) {
+    if (!tree) return OCT_OK;
+    {
+        DeviceGuard g(tree->owner ? tree->owner->c.device : 0);
+        if (tree->owner) cudaStreamSynchronize(tree->owner->c.stream);
+        release_tree(tree->t);
+    }
+    delete tree;
+    return OCT_OK;
+}
+
+OCT_API int oct_tree_build(oct_ctx* ctx, oct_tree* tree, const void* coords, int64_t n, double radius,
+                           int keep_morton) {
+    if (!ctx || !tree) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (!(radius > 0.0)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "search radius must be positive");
+    if (n < 0 || n > 2147483647LL)
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "point count must be in [0, 2^31 - 1] (Int32 indices)");
+    if (n > 0 && !coords) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "coords is NULL");
+    DeviceGuard g(ctx->c.device);
+    tree->t.keep_morton = keep_morton != 0;
+    return oct::build_tree(ctx->c, tree->t, coords, n, radius);
+}
+
+OCT_API int oct_tree_n_nodes(oct_ctx* ctx, const oct_tree* tree, int64_t* n_nodes) {
+    if (!ctx || !tree || !n_nodes) return OCT_ERR_ARGUMENT;
+    *n_nodes = tree->t.built ? tree->t.n_nodes : 0;
+    return OCT_OK;
+}
+
+OCT_API int oct_tree_view_get(oct_ctx* ctx, oct_tree* tree, oct_tree_view* out) {
+    if (!ctx || !tree || !out) return OCT_ERR_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    oct::Tree& t = tree->t;
+    out->ndims = t.ndims;
+    out->dtype = t.dtype;
+    out->radius = t.radius;
+    if (!t.built) return oct::set_error(ctx->c, OCT_ERR_STATE, "tree has not been built (call run! first)");
+    DeviceGuard g(ctx->c.device);
+    const int st = oct::materialize_view(ctx->c, t);
+    if (st != OCT_OK) return st;
+    out->n_points = t.n;
+    out->n_nodes = t.n_nodes;
+    out->node_first = t.v_first.as<int32_t>();
+    out->node_last = t.v_last.as<int32_t>();
+    out->node_children = t.v_children.as<int32_t>();
+    out->bounds_min = t.v_bmin.p;
+    out->bounds_max = t.v_bmax.p;
+    out->perm = t.v_perm.as<int32_t>();
+    out->morton = (t.keep_morton && t.n > 0) ? t.morton.as<uint64_t>() : nullptr;
+    return OCT_OK;
+}
+
+static int check_pair(oct_ctx* ctx, const oct_tree* query, const oct_tree* target) {
+    if (!query || !target) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "query/target tree is NULL");
+    if (query->t.ndims != target->t.ndims || query->t.dtype != target->t.dtype)
+        return oct::set_error(ctx->c, OCT_ERR_DIMENSION, "query and target trees differ in ndims or dtype");
+    if (!target->t.built || !query->t.built)
+        return oct::set_error(ctx->c, OCT_ERR_STATE, "query and target trees must be built before build_edges");
+    return OCT_OK;
+}
+
+OCT_API int oct_edges_count(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
+                            int64_t* n_edges) {
+    if (!ctx || !n_edges) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    *n_edges = 0;
+    int st = check_pair(ctx, query, target);
+    if (st != OCT_OK) return st;
+    if (exclude_self && query != target)
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "exclude_self requires the same tree as query and target");
+    DeviceGuard g(ctx->c.device);
+    return oct::edges_count(ctx->c, query->t, target->t, exclude_self != 0, n_edges);
+}
+
+OCT_API int oct_edges_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
+                           int32_t* senders, int32_t* receivers, void* rel_displacement, void* rel_dist_norm,
+                           int64_t capacity) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    int st = check_pair(ctx, query, target);
+    if (st != OCT_OK) return st;
+    if (capacity > 0 && (!senders || !receivers || !rel_displacement || !rel_dist_norm))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge output buffer is NULL");
+    DeviceGuard g(ctx->c.device);
+    return oct::edges_fill(ctx->c, query->t, target->t, exclude_self != 0, senders, receivers, rel_displacement,
+                           rel_dist_norm, capacity);
+}
+
+OCT_API int oct_neighbors(oct_ctx* ctx, const oct_tree* target, const void* query_coords, int64_t n_queries,
+                          int32_t* out_counts, int32_t* out_indices, int64_t cap_per_query) {
+    if (!ctx || !target) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (n_queries < 0 || cap_per_query < 0) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "negative size");
+    if (n_queries > 0 && (!query_coords || !out_counts || (cap_per_query > 0 && !out_indices)))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "NULL buffer");
+    if (!target->t.built) return oct::set_error(ctx->c, OCT_ERR_STATE, "target tree has not been built");
+    DeviceGuard g(ctx->c.device);
+    return oct::neighbors_of(ctx->c, target->t, query_coords, n_queries, out_counts, out_indices, cap_per_query);
+}
+
+OCT_API int oct_edges_diff_backward(oct_ctx* ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,
+                                    const int32_t* senders, const int32_t* receivers, const void* rel_displacement,
+                                    const void* rel_dist_norm, const void* d_rel_displacement,
+                                    const void* d_rel_dist_norm, double radius, void* grad_coords) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (bad_dims(ndims) || bad_dtype(dtype)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "bad ndims/dtype");
+    if (n_points < 0 || n_edges < 0 || n_edges > 2147483647LL || n_points > 2147483647LL)
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "sizes must fit Int32");
+    if (!(radius > 0.0)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "radius must be positive");
+    if (n_points > 0 && !grad_coords) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "grad_coords is NULL");
+    if (n_edges > 0 && (!senders || !receivers || !rel_displacement || !rel_dist_norm))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge array is NULL");
+    DeviceGuard g(ctx->c.device);
+    return oct::diff_backward(ctx->c, ndims, dtype, n_points, n_edges, senders, receivers, rel_displacement,
+                              rel_dist_norm, d_rel_displacement, d_rel_dist_norm, radius, grad_coords);
+}
+
+static const char* kPhaseNames[oct::PH_NUM] = {"bounds", "encode", "sort", "gather", "topology",
+                                               "refit", "count", "scan", "fill", "adjoint"};
+
+OCT_API int oct_profile_enable(oct_ctx* ctx, int on) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.profiling = on != 0;
+    return OCT_OK;
+}
+
+OCT_API const char* oct_profile_phase_name(int phase) {
+    return (phase >= 0 && phase < oct::PH_NUM) ? kPhaseNames[phase] : "";
+}
+
+OCT_API int64_t oct_profile_kernel_launches(const oct_ctx* ctx) { return ctx ? ctx->c.kernel_launches : 0; }
+
+OCT_API int oct_profile_read(oct_ctx* ctx, double* ms, int64_t* launches, int n_phases) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    DeviceGuard g(ctx->c.device);
+    cudaError_t e = cudaStreamSynchronize(ctx->c.stream);
+    if (e != cudaSuccess) return oct::cuda_status(ctx->c, e, "profile read");
+    for (int i = 0; i < n_phases; ++i) {
+        if (ms) ms[i] = 0.0;
+        if (launches) launches[i] = 0;
+    }
+    for (auto& r : ctx->c.prof) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.start, r.stop);
+        if (r.phase < n_phases) {
+            if (ms) ms[r.phase] += t;
+            if (launches) launches[r.phase] += 1;
+        }
+        ctx->c.event_pool.push_back(r.start);
+        ctx->c.event_pool.push_back(r.stop);
+    }
+    ctx->c.prof.clear();
+    return OCT_OK;
+}
+
+}  // extern "C"

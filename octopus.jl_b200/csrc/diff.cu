@@ -1,0 +1,142 @@
+// Adjoint of build_edges_diff for a self pair (ext/OctopusChainRulesCoreExt.jl:137-192,
+// ext/OctopusCUDAChainRulesCoreExt.jl:56-99), without floating-point atomics.
+//
+// Per edge k = (receiver i <- sender j) the cotangent contributes
+//   c_k = d_disp[:,k] / r + rel_disp[:,k] * (d_dist[k] / (rel_dist[k] * r))
+// (the second term only when rel_dist[k] > 1e-8), added to x_i and
+// subtracted from x_j.  The edges are already grouped by receiver, so the
+// receiver sum is a segmented reduction in edge order; the sender sum reads
+// the edges re-ordered by (sender, edge index) with the stable radix sort.
+// Every point sums its terms in a fixed order in double precision, so the
+// result is bit-reproducible from run to run.
+
+#include <algorithm>
+
+#include "internal.h"
+#include "sort.cuh"
+
+namespace oct {
+
+template <class T, int D>
+__device__ __forceinline__ void edge_term(int64_t k, const T* __restrict__ rel_disp, const T* __restrict__ rel_dist,
+                                          const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r,
+                                          double* out) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) out[d] = 0.0;
+    if (d_disp) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) out[d] += (double)div_rn(d_disp[(int64_t)D * k + d], r);
+    }
+    if (d_dist) {
+        const T dn = rel_dist[k];
+        if (dn > T(1e-8)) {
+            const T inv = div_rn(d_dist[k], mul_rn(dn, r));
+#pragma unroll
+            for (int d = 0; d < D; ++d) out[d] += (double)mul_rn(rel_disp[(int64_t)D * k + d], inv);
+        }
+    }
+}
+
+// off[i] = first edge whose (1-based) key is >= i + 1, for i in [0, n].
+__global__ void k_segment_starts(const int32_t* __restrict__ keys1, int64_t m, int64_t n, int64_t* __restrict__ off) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    int64_t a = 0, b = m;
+    while (a < b) {
+        const int64_t mid = (a + b) >> 1;
+        if ((int64_t)keys1[mid] >= i + 1) b = mid; else a = mid + 1;
+    }
+    off[i] = a;
+}
+
+__global__ void k_sender_keys(const int32_t* __restrict__ snd, int64_t m, uint32_t* __restrict__ keys) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) keys[k] = (uint32_t)(snd[k] - 1);
+}
+
+// off[j] = first sorted position whose 0-based sender key is >= j.
+__global__ void k_sorted_starts(const uint32_t* __restrict__ skeys, int64_t m, int64_t n, int64_t* __restrict__ off) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > n) return;
+    int64_t a = 0, b = m;
+    while (a < b) {
+        const int64_t mid = (a + b) >> 1;
+        if ((int64_t)skeys[mid] >= j) b = mid; else a = mid + 1;
+    }
+    off[j] = a;
+}
+
+template <class T, int D>
+__global__ void k_grad(int64_t n, const int64_t* __restrict__ roff, const int64_t* __restrict__ soff,
+                       const int32_t* __restrict__ sorted_edge, const T* __restrict__ rel_disp,
+                       const T* __restrict__ rel_dist, const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r,
+                       T* __restrict__ grad) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) acc[d] = 0.0;
+    double c[D];
+    for (int64_t k = roff[i]; k < roff[i + 1]; ++k) {
+        edge_term<T, D>(k, rel_disp, rel_dist, d_disp, d_dist, r, c);
+#pragma unroll
+        for (int d = 0; d < D; ++d) acc[d] += c[d];
+    }
+    for (int64_t m = soff[i]; m < soff[i + 1]; ++m) {
+        const int64_t k = sorted_edge ? sorted_edge[m] : m;
+        edge_term<T, D>(k, rel_disp, rel_dist, d_disp, d_dist, r, c);
+#pragma unroll
+        for (int d = 0; d < D; ++d) acc[d] -= c[d];
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) grad[(int64_t)D * i + d] = (T)acc[d];
+}
+
+namespace {
+
+template <class T, int D>
+int backward_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_t* rcv, const void* rel_disp,
+                   const void* rel_dist, const void* d_disp, const void* d_dist, double radius, void* grad) {
+    cudaStream_t s = ctx.stream;
+    cudaError_t err;
+    const T r = (T)radius;
+    if (m == 0 || (!d_disp && !d_dist)) {
+        return cuda_status(ctx, cudaMemsetAsync(grad, 0, sizeof(T) * D * n, s), "zero gradient");
+    }
+    if ((err = ensure(ctx.dkeys[0], m * 4)) || (err = ensure(ctx.dkeys[1], m * 4)) ||
+        (err = ensure(ctx.dvals[0], m * 4)) || (err = ensure(ctx.dvals[1], m * 4)) ||
+        (err = ensure(ctx.dhist, (size_t)256 * sort_tiles(m) * 4)) || (err = ensure(ctx.droff, (n + 1) * 8)) ||
+        (err = ensure(ctx.dsoff, (n + 1) * 8)))
+        return cuda_status(ctx, err, "allocating adjoint scratch");
+    const int tb = 256;
+    PhaseTimer pt_(ctx, PH_ADJOINT);
+    k_segment_starts<<<div_up(n + 1, tb), tb, 0, s>>>(rcv, m, n, ctx.droff.as<int64_t>());
+    k_sender_keys<<<div_up(m, tb), tb, 0, s>>>(snd, m, ctx.dkeys[0].as<uint32_t>());
+    int bits = 0;
+    while (bits < 32 && ((uint64_t)(n - 1) >> bits) != 0) ++bits;
+    uint32_t* kb[2] = {ctx.dkeys[0].as<uint32_t>(), ctx.dkeys[1].as<uint32_t>()};
+    int32_t* vb[2] = {ctx.dvals[0].as<int32_t>(), ctx.dvals[1].as<int32_t>()};
+    const int src = radix_sort_pairs<uint32_t>(kb, vb, ctx.dhist.as<int32_t>(), m, bits, false, s);
+    const int32_t* sorted_edge = bits > 0 ? vb[src] : nullptr;
+    k_sorted_starts<<<div_up(n + 1, tb), tb, 0, s>>>(kb[src], m, n, ctx.dsoff.as<int64_t>());
+    k_grad<T, D><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), ctx.dsoff.as<int64_t>(), sorted_edge,
+                                             (const T*)rel_disp, (const T*)rel_dist, (const T*)d_disp,
+                                             (const T*)d_dist, r, (T*)grad);
+    ctx.kernel_launches += 4 + 3 * ((bits + 7) / 8);
+    return cuda_status(ctx, cudaGetLastError(), "adjoint launch");
+}
+
+}  // namespace
+
+int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n, int64_t m, const int32_t* snd, const int32_t* rcv,
+                  const void* rel_disp, const void* rel_dist, const void* d_disp, const void* d_dist, double radius,
+                  void* grad) {
+    if (n == 0) return OK;
+    if (dtype == 0)
+        return ndims == 3 ? backward_typed<float, 3>(ctx, n, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist, radius, grad)
+                          : backward_typed<float, 2>(ctx, n, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist, radius, grad);
+    return ndims == 3 ? backward_typed<double, 3>(ctx, n, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist, radius, grad)
+                      : backward_typed<double, 2>(ctx, n, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist, radius, grad);
+}
+
+}  // namespace oct

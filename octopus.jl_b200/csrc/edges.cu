@@ -1,0 +1,307 @@
+// Fixed-radius traversal and flat-COO edge construction.
+//
+// Replaces _count_edges_kernel! / _fill_edges_kernel_{3d,2d}! /
+// _build_edges_cuda! (ext/OctopusCUDAExt.jl:262-415) and reproduces the CPU
+// path's output exactly (src/cpu/edges_cpu.jl:36-247):
+//
+//   * One warp serves 32 queries that are consecutive in the query set's
+//     Morton order.  The warp walks the target tree once, depth first, with
+//     the box of its 32 queries: children are tested in slot order and
+//     pushed in that order onto a shared-memory stack, so leaves pop in the
+//     same order as the reference's per-query DFS
+//     (src/cpu/iterator_cpu.jl:74-116).  The group box test is conservative
+//     (box_gap2), so every leaf a single query would visit is visited, and
+//     the exact per-pair test d2 = ((dx*dx + dy*dy) + dz*dz) <= r*r decides
+//     membership.  Each query therefore emits its neighbors in the
+//     reference's order: leaves in DFS order, points in ascending sorted
+//     position inside a leaf.  An internal node whose first child slot is
+//     empty counts as a leaf in the reference (src/cpu/iterator_cpu.jl:87),
+//     so its subtree is walked in ascending slot order, which lists its
+//     points in ascending position exactly as the reference's leaf loop.
+//   * Leaf points are staged in shared memory and broadcast to the 32 lanes.
+//   * counts -> int64 exclusive scan -> fill at the per-query cursor.
+
+#include <algorithm>
+
+#include "internal.h"
+#include "scan.cuh"
+
+namespace oct {
+
+constexpr int kEdgeWarps = 8;
+constexpr int kEdgeThreads = kEdgeWarps * 32;
+
+template <class T, int D, bool FILL>
+__global__ void __launch_bounds__(kEdgeThreads) k_edges(
+    const SPt<T, D>* __restrict__ qpts, int64_t nq, const TNode<T, D>* __restrict__ tnode,
+    const SPt<T, D>* __restrict__ tpts, int64_t n_tnodes, T r2, T inv_r, int exclude_self,
+    int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
+    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ dstatus) {
+    constexpr int SD = stack_depth<D>();
+    __shared__ int32_t stack[kEdgeWarps][SD];
+    __shared__ SPt<T, D> tgt[kEdgeWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t qbase = ((int64_t)blockIdx.x * kEdgeWarps + w) * 32;
+    if (qbase >= nq) return;  // warp-uniform
+    const bool valid = qbase + lane < nq;
+    const SPt<T, D> q = qpts[valid ? qbase + lane : qbase];
+    T qlo[D], qhi[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        qlo[d] = warp_min(q.x[d]);
+        qhi[d] = warp_max(q.x[d]);
+    }
+    int64_t cnt = 0;
+    int64_t cur = 0, cur_end = 0;
+    if (FILL && valid) {
+        cur = offsets[q.idx];
+        cur_end = offsets[q.idx + 1];
+    }
+    const bool self_pair = exclude_self != 0;
+
+    int sp = 0;
+    if (n_tnodes > 0) {
+        const TNode<T, D> root = tnode[0];
+        if (box_gap2<T, D>(qlo, qhi, root.lo, root.hi) <= r2) {
+            if (lane == 0) stack[w][0] = 0;
+            sp = 1;
+        }
+    }
+    __syncwarp();
+    while (sp > 0) {
+        const int32_t ent = stack[w][--sp];
+        const int32_t nid = ent & 0x7fffffff;
+        const bool asc = ent < 0;
+        const TNode<T, D> nd = tnode[nid];
+        if (nd.b > 0) {
+            // Leaf: per-lane point-to-box prefilter, then every pair.
+            const bool act = valid && box_gap2<T, D>(q.x, q.x, nd.lo, nd.hi) <= r2;
+            if (__any_sync(0xffffffffu, act)) {
+                for (int32_t c0 = 0; c0 < nd.b; c0 += 32) {
+                    const int m = min(32, nd.b - c0);
+                    __syncwarp();
+                    if (lane < m) tgt[w][lane] = tpts[nd.a + c0 + lane];
+                    __syncwarp();
+                    for (int j = 0; j < m; ++j) {
+                        const SPt<T, D> t = tgt[w][j];
+                        T diff[D];
+                        const T d2 = dist2<T, D>(t.x, q.x, diff);
+                        const bool hit = act && d2 <= r2;
+                        if (FILL) {
+                            if (hit && !(self_pair && t.idx == q.idx)) {
+                                if (cur >= cur_end) {  // never taken when count and fill agree
+                                    atomicOr(dstatus, 1);
+                                    continue;
+                                }
+                                senders[cur] = t.idx + 1;
+                                receivers[cur] = q.idx + 1;
+#pragma unroll
+                                for (int d = 0; d < D; ++d) rdisp[(int64_t)D * cur + d] = mul_rn(-diff[d], inv_r);
+                                rdist[cur] = mul_rn(sqrt_rn(d2), inv_r);
+                                ++cur;
+                            }
+                        } else {
+                            cnt += hit ? 1 : 0;
+                        }
+                    }
+                }
+            }
+        } else {
+            // The reference scans an internal node whose first child slot is
+            // empty as one leaf, in ascending position order
+            // (src/cpu/iterator_cpu.jl:87-101).  Below such a node the
+            // children are therefore visited in ascending slot order.
+            const unsigned slots = (unsigned)(-nd.b);
+            const bool casc = asc || !(slots & 1u);
+            const int nc = __popc(slots);
+            bool pass = false;
+            if (lane < nc) {
+                const TNode<T, D> c = tnode[nd.a + lane];
+                pass = box_gap2<T, D>(qlo, qhi, c.lo, c.hi) <= r2;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, pass);
+            const int np = __popc(m);
+            __syncwarp();
+            if (pass) {
+                const int rk = __popc(m & lanemask_lt());
+                stack[w][casc ? sp + np - 1 - rk : sp + rk] = (nd.a + lane) | (casc ? (int32_t)0x80000000 : 0);
+            }
+            sp += np;
+            __syncwarp();
+        }
+    }
+    if (!FILL && valid) counts[q.idx] = (int32_t)(cnt - (self_pair ? 1 : 0));
+}
+
+// Per-thread reference-order DFS for a handful of query points (the
+// get_neighborlist / for_each_neighbor accessors, src/api.jl:282-292 and
+// src/cpu/iterator_cpu.jl:245-263).  No self filter.
+template <class T, int D>
+__global__ void k_neighbors_of(const T* __restrict__ qcoords, int64_t nsel, const TNode<T, D>* __restrict__ tnode,
+                               const SPt<T, D>* __restrict__ tpts, int64_t n_tnodes, T r2,
+                               int32_t* __restrict__ out_counts, int32_t* __restrict__ out_idx, int64_t cap) {
+    constexpr int SD = stack_depth<D>();
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsel) return;
+    T p[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) p[d] = qcoords[(int64_t)D * s + d];
+    int32_t stack[SD];
+    int sp = 0;
+    int64_t c = 0;
+    if (n_tnodes > 0) stack[sp++] = 0;
+    while (sp > 0) {
+        const int32_t ent = stack[--sp];
+        const int32_t nid = ent & 0x7fffffff;
+        const bool asc = ent < 0;
+        const TNode<T, D> nd = tnode[nid];
+        if (box_gap2<T, D>(p, p, nd.lo, nd.hi) > r2) continue;
+        if (nd.b > 0) {
+            for (int32_t k = nd.a; k < nd.a + nd.b; ++k) {
+                const SPt<T, D> t = tpts[k];
+                T diff[D];
+                if (dist2<T, D>(t.x, p, diff) <= r2) {
+                    if (c < cap) out_idx[s * cap + c] = t.idx + 1;
+                    ++c;
+                }
+            }
+        } else {
+            const unsigned slots = (unsigned)(-nd.b);
+            const bool casc = asc || !(slots & 1u);
+            const int nc = __popc(slots);
+            int pushed[Dims<D>::nch];
+            int np = 0;
+            for (int j = 0; j < nc; ++j) {
+                const TNode<T, D> ch = tnode[nd.a + j];
+                if (box_gap2<T, D>(p, p, ch.lo, ch.hi) <= r2) pushed[np++] = nd.a + j;
+            }
+            for (int j = 0; j < np; ++j)
+                stack[sp++] = casc ? (pushed[np - 1 - j] | (int32_t)0x80000000) : pushed[j];
+        }
+    }
+    out_counts[s] = (int32_t)c;
+}
+
+namespace {
+
+template <class T, int D>
+int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64_t* n_edges) {
+    cudaError_t err;
+    cudaStream_t s = ctx.stream;
+    const int64_t nq = q.n;
+    if ((err = ensure(ctx.counts, (size_t)std::max<int64_t>(nq, 1) * 4)) ||
+        (err = ensure(ctx.offsets, (size_t)(nq + 1) * 8)) ||
+        (err = ensure(ctx.scan_tmp, (size_t)scan_tmp_elems(nq) * 8)) || (err = ensure(ctx.total, 8)) ||
+        (err = ensure(ctx.dstatus, 4)))
+        return cuda_status(ctx, err, "allocating edge scratch");
+    if ((err = cudaMemsetAsync(ctx.dstatus.p, 0, 4, s))) return cuda_status(ctx, err, "status reset");
+    if (!ctx.total_host) {
+        if ((err = cudaMallocHost((void**)&ctx.total_host, 8))) return cuda_status(ctx, err, "pinned total");
+    }
+    const T r = (T)t.radius;
+    const T r2 = r * r;  // src/cpu/edges_cpu.jl:184
+    if (t.n_nodes == 0) {
+        if ((err = cudaMemsetAsync(ctx.counts.p, 0, (size_t)nq * 4, s))) return cuda_status(ctx, err, "zero counts");
+    } else {
+        PhaseTimer pt_(ctx, PH_COUNT);
+        const int64_t groups = (nq + 31) / 32;
+        k_edges<T, D, false><<<div_up(groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
+            q.spts.as<SPt<T, D>>(), nq, t.tnode.as<TNode<T, D>>(), t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0),
+            exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+        ctx.kernel_launches += 1;
+    }
+    {
+        PhaseTimer pt_(ctx, PH_SCAN);
+        exclusive_scan_i32_i64(ctx.counts.as<int32_t>(), ctx.offsets.as<int64_t>(), nq, ctx.total.as<int64_t>(),
+                               ctx.scan_tmp.as<int64_t>(), s);
+        ctx.kernel_launches += 3;
+    }
+    if ((err = cudaMemcpyAsync(ctx.total_host, ctx.total.p, 8, cudaMemcpyDeviceToHost, s)) ||
+        (err = cudaStreamSynchronize(s)))
+        return cuda_status(ctx, err, "edge count");
+    *n_edges = *ctx.total_host;
+    return OK;
+}
+
+template <class T, int D>
+int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* senders, int32_t* receivers,
+               void* rel_disp, void* rel_dist) {
+    const int64_t nq = q.n;
+    const T r = (T)t.radius;
+    const T r2 = r * r;
+    const T inv_r = T(1) / r;  // inv(r), src/cpu/edges_cpu.jl:185
+    const int64_t groups = (nq + 31) / 32;
+    PhaseTimer pt_(ctx, PH_FILL);
+    k_edges<T, D, true><<<div_up(groups, kEdgeWarps), kEdgeThreads, 0, ctx.stream>>>(
+        q.spts.as<SPt<T, D>>(), nq, t.tnode.as<TNode<T, D>>(), t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r,
+        exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(), senders, receivers, (T*)rel_disp, (T*)rel_dist,
+        ctx.dstatus.as<int>());
+    ctx.kernel_launches += 1;
+    return cuda_status(ctx, cudaGetLastError(), "edge fill launch");
+}
+
+template <class T, int D>
+int neighbors_typed(Ctx& ctx, const Tree& t, const void* qcoords, int64_t nsel, int32_t* out_counts,
+                    int32_t* out_idx, int64_t cap) {
+    const T r = (T)t.radius;
+    const T r2 = r * r;
+    k_neighbors_of<T, D><<<div_up(nsel, 128), 128, 0, ctx.stream>>>(
+        (const T*)qcoords, nsel, t.tnode.as<TNode<T, D>>(), t.spts.as<SPt<T, D>>(), t.n_nodes, r2, out_counts,
+        out_idx, cap);
+    ctx.kernel_launches += 1;
+    return cuda_status(ctx, cudaGetLastError(), "neighbor query launch");
+}
+
+}  // namespace
+
+int edges_count(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64_t* n_edges) {
+    ctx.plan_query = nullptr;
+    int st = OK;
+    if (q.n == 0) {
+        *n_edges = 0;
+    } else if (t.dtype == 0) {
+        st = t.ndims == 3 ? count_typed<float, 3>(ctx, q, t, exclude_self, n_edges)
+                          : count_typed<float, 2>(ctx, q, t, exclude_self, n_edges);
+    } else {
+        st = t.ndims == 3 ? count_typed<double, 3>(ctx, q, t, exclude_self, n_edges)
+                          : count_typed<double, 2>(ctx, q, t, exclude_self, n_edges);
+    }
+    if (st != OK) return st;
+    ctx.plan_query = &q;
+    ctx.plan_target = &t;
+    ctx.plan_qgen = q.generation;
+    ctx.plan_tgen = t.generation;
+    ctx.plan_exclude = exclude_self ? 1 : 0;
+    ctx.plan_edges = *n_edges;
+    return OK;
+}
+
+int edges_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* senders, int32_t* receivers,
+               void* rel_disp, void* rel_dist, int64_t n_edges) {
+    if (ctx.plan_query != &q || ctx.plan_target != &t || ctx.plan_qgen != q.generation ||
+        ctx.plan_tgen != t.generation || ctx.plan_exclude != (exclude_self ? 1 : 0))
+        return set_error(ctx, ERR_STATE, "oct_edges_fill: no matching oct_edges_count for this pair and build");
+    if (n_edges < ctx.plan_edges)
+        return set_error(ctx, ERR_CAPACITY, "oct_edges_fill: output capacity is smaller than the edge count");
+    if (ctx.plan_edges == 0 || q.n == 0 || t.n_nodes == 0) return OK;
+    if (t.dtype == 0)
+        return t.ndims == 3 ? fill_typed<float, 3>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist)
+                            : fill_typed<float, 2>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist);
+    return t.ndims == 3 ? fill_typed<double, 3>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist)
+                        : fill_typed<double, 2>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist);
+}
+
+int neighbors_of(Ctx& ctx, const Tree& t, const void* qcoords, int64_t nsel, int32_t* out_counts, int32_t* out_idx,
+                 int64_t cap) {
+    if (nsel == 0) return OK;
+    if (t.n_nodes == 0) {
+        return cuda_status(ctx, cudaMemsetAsync(out_counts, 0, (size_t)nsel * 4, ctx.stream), "neighbor query");
+    }
+    if (t.dtype == 0)
+        return t.ndims == 3 ? neighbors_typed<float, 3>(ctx, t, qcoords, nsel, out_counts, out_idx, cap)
+                            : neighbors_typed<float, 2>(ctx, t, qcoords, nsel, out_counts, out_idx, cap);
+    return t.ndims == 3 ? neighbors_typed<double, 3>(ctx, t, qcoords, nsel, out_counts, out_idx, cap)
+                        : neighbors_typed<double, 2>(ctx, t, qcoords, nsel, out_counts, out_idx, cap);
+}
+
+}  // namespace oct

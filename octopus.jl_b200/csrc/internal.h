@@ -1,0 +1,136 @@
+// Library-internal objects shared by the build, edge and C-ABI translation units.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace oct {
+
+// Grow-only device allocation.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+cudaError_t ensure(DevBuf& b, size_t bytes);
+void release(DevBuf& b);
+
+struct Ctx;
+
+// Phases timed by the optional CUDA-event profiler (oct_profile_*).
+enum Phase : int {
+    PH_BOUNDS = 0, PH_ENCODE, PH_SORT, PH_GATHER, PH_TOPOLOGY, PH_REFIT,
+    PH_COUNT, PH_SCAN, PH_FILL, PH_ADJOINT, PH_NUM
+};
+
+struct ProfRecord {
+    int phase;
+    cudaEvent_t start, stop;
+};
+
+// Records one phase between its constructor and destructor when profiling
+// is on; otherwise does nothing.
+struct PhaseTimer {
+    Ctx* ctx;
+    int phase;
+    cudaEvent_t start = nullptr;
+    PhaseTimer(Ctx& c, int ph);
+    ~PhaseTimer();
+};
+
+// One point set's search structure (the reference's Octree + permutation +
+// morton_codes, src/types.jl:23-42 and src/types.jl:153-154).
+struct Tree {
+    int ndims = 3;
+    int dtype = 0;          // 0 = float32, 1 = float64
+    int64_t n = 0;
+    double radius = 0.0;
+    int32_t leaf_size = kLeafSize;
+    bool built = false;
+    bool keep_morton = false;
+    uint64_t generation = 0;
+
+    // Build results (host copies, valid after a successful build).
+    int key_bytes = 4;
+    int key_bits = 0;
+    int sort_passes = 0;
+    int64_t n_nodes = 0;
+    int64_t capacity = 0;    // node capacity of the node arrays
+    int n_mark_blocks = 0;
+    double origin[3] = {0, 0, 0};
+
+    // Device storage.
+    DevBuf keys[2], vals[2];     // radix-sort ping-pong
+    DevBuf hist;                 // radix digit histograms
+    DevBuf spts;                 // SPt<T,D>[n] in Morton order
+    DevBuf tnode;                // TNode<T,D>[capacity]
+    DevBuf nrange;               // int2 {first,last} 0-based per node
+    DevBuf parent;               // int32 per node (-1 for the root)
+    DevBuf arrive;               // int32 per node, refit arrival counters
+    DevBuf lohi;                 // uint16 per position: first | last level starting here
+    DevBuf blockcnt;             // int32 [(maxlev+1) * n_mark_blocks]
+    DevBuf blockoff;             // int64 exclusive scan of blockcnt (+1)
+    DevBuf scan_tmp;             // int64 tile sums for scans
+    DevBuf partials;             // double per-block bounds partials
+    DevBuf hdr;                  // OctHeader
+    DevBuf morton;               // uint64 per original point (refit mode)
+    OctHeader* hdr_host = nullptr;  // pinned
+
+    // Lazily materialized reference-layout views (DeviceView contract,
+    // ext/OctopusCUDAExt.jl:23-35).
+    bool view_valid = false;
+    DevBuf v_first, v_last, v_children, v_bmin, v_bmax, v_perm;
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    // Edge-count state carried from oct_edges_count to oct_edges_fill.
+    DevBuf counts;       // int32 per query point
+    DevBuf offsets;      // int64 per query point + 1
+    DevBuf scan_tmp;     // int64 tile sums
+    DevBuf total;        // int64 device total
+    DevBuf dstatus;      // int32 device error word set by kernels (bounds guards)
+    int64_t* total_host = nullptr;  // pinned
+    const Tree* plan_query = nullptr;
+    const Tree* plan_target = nullptr;
+    uint64_t plan_qgen = 0, plan_tgen = 0;
+    int plan_exclude = -1;
+    int64_t plan_edges = -1;
+    // Adjoint scratch (diff.cu).
+    DevBuf dkeys[2], dvals[2], dhist, droff, dsoff;
+    // Profiler.
+    int64_t kernel_launches = 0;  // every kernel this context has launched
+    bool profiling = false;
+    std::vector<ProfRecord> prof;
+    std::vector<cudaEvent_t> event_pool;
+    cudaEvent_t get_event();
+};
+
+// Build pipeline (build.cu).  Returns a Status.
+int build_tree(Ctx& ctx, Tree& t, const void* coords, int64_t n, double radius);
+int materialize_view(Ctx& ctx, Tree& t);
+
+// Edge pipeline (edges.cu).
+int edges_count(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64_t* n_edges);
+int edges_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* senders,
+               int32_t* receivers, void* rel_disp, void* rel_dist, int64_t n_edges);
+int neighbors_of(Ctx& ctx, const Tree& t, const void* qcoords, int64_t nsel, int32_t* out_counts,
+                 int32_t* out_idx, int64_t cap);
+
+// Adjoint (diff.cu).
+int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,
+                  const int32_t* senders, const int32_t* receivers, const void* rel_disp,
+                  const void* rel_dist, const void* d_disp, const void* d_dist, double radius,
+                  void* grad);
+
+int set_error(Ctx& ctx, int status, const std::string& msg);
+int cuda_status(Ctx& ctx, cudaError_t e, const char* where);
+
+}  // namespace oct

@@ -1,0 +1,88 @@
+// Device-wide exclusive scan, reduce-then-scan in three launches.  No kernel
+// waits on another block, so there is nothing to spin on.
+#include "scan.cuh"
+
+namespace oct {
+
+// Per-tile sums of kScanTile consecutive inputs.
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const int32_t* __restrict__ in, int64_t n,
+                                                                 int64_t* __restrict__ tile_sums) {
+    __shared__ int64_t sm[kScanThreads / 32 + 1];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    int64_t s = 0;
+#pragma unroll
+    for (int it = 0; it < kScanItems; ++it) {
+        const int64_t i = base + (int64_t)it * kScanThreads + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    int64_t tot;
+    block_exclusive_scan<int64_t>(s, sm, &tot);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+// Exclusive scan of the tile sums by one block, carrying across chunks.
+__global__ void __launch_bounds__(1024) k_scan_tiles(int64_t* __restrict__ tile_sums, int64_t ntiles,
+                                                     int64_t* __restrict__ d_total) {
+    __shared__ int64_t sm[1024 / 32 + 1];
+    int64_t carry = 0;
+    for (int64_t base = 0; base < ntiles; base += blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        const int64_t v = i < ntiles ? tile_sums[i] : 0;
+        int64_t tot;
+        const int64_t ex = block_exclusive_scan<int64_t>(v, sm, &tot);
+        if (i < ntiles) tile_sums[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && d_total) *d_total = carry;
+}
+
+// Final pass: each tile scans its items in order (blocked per thread) and
+// adds the tile offset.
+__global__ void __launch_bounds__(kScanThreads) k_scan_final(const int32_t* __restrict__ in, int64_t n,
+                                                             const int64_t* __restrict__ tile_off,
+                                                             int64_t* __restrict__ out) {
+    __shared__ int64_t sm[kScanThreads / 32 + 1];
+    __shared__ int32_t stage[kScanTile];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    // Coalesced load into shared memory, then each thread owns kScanItems
+    // consecutive elements.
+#pragma unroll
+    for (int it = 0; it < kScanItems; ++it) {
+        const int j = it * kScanThreads + threadIdx.x;
+        const int64_t i = base + j;
+        stage[j] = i < n ? in[i] : 0;
+    }
+    __syncthreads();
+    int32_t v[kScanItems];
+    int64_t s = 0;
+#pragma unroll
+    for (int it = 0; it < kScanItems; ++it) {
+        v[it] = stage[threadIdx.x * kScanItems + it];
+        s += v[it];
+    }
+    int64_t tot;
+    int64_t run = block_exclusive_scan<int64_t>(s, sm, &tot) + tile_off[blockIdx.x];
+#pragma unroll
+    for (int it = 0; it < kScanItems; ++it) {
+        const int64_t i = base + (int64_t)threadIdx.x * kScanItems + it;
+        if (i < n) out[i] = run;
+        run += v[it];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = tile_off[blockIdx.x] + tot;
+}
+
+// out[0..n] = exclusive scan of in[0..n-1]; out[n] = total (also *d_total).
+void exclusive_scan_i32_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* d_total,
+                            int64_t* tile_tmp, cudaStream_t s) {
+    if (n <= 0) {
+        cudaMemsetAsync(out, 0, sizeof(int64_t), s);
+        if (d_total) cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
+        return;
+    }
+    const int ntiles = div_up(n, kScanTile);
+    k_scan_tile_sums<<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp);
+    k_scan_tiles<<<1, 1024, 0, s>>>(tile_tmp, ntiles, d_total);
+    k_scan_final<<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp, out);
+}
+
+}  // namespace oct

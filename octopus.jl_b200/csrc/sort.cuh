@@ -1,0 +1,121 @@
+// Stable LSD radix sort of (key, int32 value) pairs on 8-bit digits.
+#pragma once
+
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace oct {
+
+constexpr int kSortThreads = 256;
+// Stable LSD radix sort on 8-bit digits: per-tile histogram, one scan of the
+// digit-major histogram, then a stable scatter that ranks equal digits with
+// warp match and per-warp shared-memory counters.
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
+
+template <class K>
+static __global__ void __launch_bounds__(kSortThreads) k_hist(const K* __restrict__ keys, int64_t n, int shift,
+                                                   int32_t* __restrict__ hist, int ntiles) {
+    __shared__ int32_t cnt[256];
+    cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const int64_t i = base + it * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&cnt[(unsigned)(keys[i] >> shift) & 255u], 1);
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// In-place exclusive scan of m int32 values by one block.
+static __global__ void __launch_bounds__(1024) k_scan_hist(int32_t* __restrict__ h, int64_t m) {
+    __shared__ int32_t sm[1024 / 32 + 1];
+    int32_t carry = 0;
+    for (int64_t base = 0; base < m; base += 1024) {
+        const int64_t i = base + threadIdx.x;
+        const int32_t v = i < m ? h[i] : 0;
+        int32_t tot;
+        const int32_t ex = block_exclusive_scan<int32_t>(v, sm, &tot);
+        if (i < m) h[i] = carry + ex;
+        carry += tot;
+    }
+}
+
+template <class K>
+static __global__ void __launch_bounds__(kSortThreads) k_scatter(const K* __restrict__ kin, const int32_t* __restrict__ vin,
+                                                      K* __restrict__ kout, int32_t* __restrict__ vout, int64_t n,
+                                                      int shift, const int32_t* __restrict__ hoff, int ntiles) {
+    __shared__ int32_t wc[kSortThreads / 32][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < kSortThreads / 32; ++j) wc[j][threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)w * (32 * kSortItems);
+    K key[kSortItems];
+    int32_t val[kSortItems], rk[kSortItems];
+    int dg[kSortItems];
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const int64_t i = wbase + it * 32 + lane;
+        const bool valid = i < n;
+        key[it] = valid ? kin[i] : K(0);
+        val[it] = valid ? (vin ? vin[i] : (int32_t)i) : 0;
+        const int d = valid ? (int)((unsigned)(key[it] >> shift) & 255u) : 256;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
+        const int before = __popc(peers & lanemask_lt());
+        const int c0 = valid ? wc[w][d] : 0;
+        __syncwarp();
+        if (valid && lane == leader) wc[w][d] = c0 + __popc(peers);
+        __syncwarp();
+        rk[it] = c0 + before;
+        dg[it] = d;
+    }
+    __syncthreads();
+    {
+        int32_t run = 0;
+#pragma unroll
+        for (int j = 0; j < kSortThreads / 32; ++j) {
+            const int32_t c = wc[j][threadIdx.x];
+            wc[j][threadIdx.x] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        if (dg[it] < 256) {
+            const int64_t dst = (int64_t)hoff[(int64_t)dg[it] * ntiles + blockIdx.x] + wc[w][dg[it]] + rk[it];
+            kout[dst] = key[it];
+            vout[dst] = val[it];
+        }
+    }
+}
+
+
+inline int sort_tiles(int64_t n) { return (int)((n + kSortTile - 1) / kSortTile); }
+
+// Sorts n pairs by the low `bits` bits of the key.  Input in (k[0], v[0])
+// (v[0] may be null for the identity 0..n-1); returns the index (0 or 1) of
+// the buffers holding the result.  With zero passes the result is the input
+// and v[0] stays untouched (the caller treats a null value buffer as iota).
+template <class K>
+int radix_sort_pairs(K* k[2], int32_t* v[2], int32_t* hist, int64_t n, int bits, bool vals_in,
+                     cudaStream_t s) {
+    const int ntiles = sort_tiles(n);
+    const int passes = (bits + 7) / 8;
+    int src = 0;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        k_hist<K><<<ntiles, kSortThreads, 0, s>>>(k[src], n, shift, hist, ntiles);
+        k_scan_hist<<<1, 1024, 0, s>>>(hist, (int64_t)256 * ntiles);
+        k_scatter<K><<<ntiles, kSortThreads, 0, s>>>(k[src], (p == 0 && !vals_in) ? nullptr : v[src], k[src ^ 1],
+                                                     v[src ^ 1], n, shift, hist, ntiles);
+        src ^= 1;
+    }
+    return src;
+}
+
+}  // namespace oct
