@@ -58,21 +58,18 @@ def config_dict(extra=None):
 
 
 # ------------------------------------------------------------- inputs -----
-def lattice_np(per, seed):
-    rng = np.random.default_rng(seed)
-    g = np.stack(np.meshgrid(*[np.arange(per)] * 3, indexing="ij"), -1).reshape(-1, 3).astype(np.float64)
-    return (g * H + rng.uniform(-JITTER, JITTER, g.shape)).astype(np.float32)
+def _workloads():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("octopus_b200_workloads",
+                                                  os.path.join(ROOT, "octopus.jl_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def snapshots_np(per, nsteps, seed):
     """Coordinates of steps 0..nsteps-1 (float32, (N,3)) on the host."""
-    rng = np.random.default_rng(seed + 1)
-    x = lattice_np(per, seed)
-    out = [x]
-    for _ in range(nsteps - 1):
-        x = (x + rng.normal(0.0, SIGMA, x.shape)).astype(np.float32)
-        out.append(x)
-    return out
+    return _workloads().sph_snapshots(per, nsteps, seed, sigma=SIGMA)
 
 
 # ------------------------------------------------------------- clocks -----
@@ -201,6 +198,7 @@ def run_ours(args, rank, world, local):
     launches0 = lib.oct_profile_kernel_launches(ctx.handle)
     clocks = ClockSampler(local)
     clocks.start()
+    time.sleep(0.5)  # let the sampler start before the timed region
     stream = torch.cuda.current_stream(dev)
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)

@@ -78,21 +78,43 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const T* __restrict__ coord
         is_last = (ticket == (int)gridDim.x - 1);
     }
     __syncthreads();
-    if (is_last && threadIdx.x == 0) {
-        __threadfence();
-        T glo[D], ghi[D];
-        for (int d = 0; d < D; ++d) { glo[d] = T(INFINITY); ghi[d] = T(-INFINITY); }
-        int anynan = 0;
-        for (unsigned b = 0; b < gridDim.x; ++b) {
-            const volatile double* p = partials + (size_t)b * 8;
-            for (int d = 0; d < D; ++d) {
-                glo[d] = jl_min(glo[d], (T)p[d]);
-                ghi[d] = jl_max(ghi[d], (T)p[3 + d]);
-            }
-            if (p[6] != 0.0) anynan = 1;
+    if (!is_last) return;
+    // Last block: fold the per-block partials in parallel.
+    __threadfence();
+    T glo[D], ghi[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) { glo[d] = T(INFINITY); ghi[d] = T(-INFINITY); }
+    int anynan = 0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        const double* p = partials + (size_t)b * 8;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            glo[d] = jl_min(glo[d], (T)__ldcg(p + d));
+            ghi[d] = jl_max(ghi[d], (T)__ldcg(p + 3 + d));
         }
-        for (int d = 0; d < D; ++d) { hdr->gmin[d] = (double)glo[d]; hdr->gmax[d] = (double)ghi[d]; }
-        hdr->nan_flag = anynan;
+        if (__ldcg(p + 6) != 0.0) anynan = 1;
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        glo[d] = warp_min(glo[d]);
+        ghi[d] = warp_max(ghi[d]);
+    }
+    anynan = __any_sync(0xffffffffu, anynan);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) { smin[w][d] = glo[d]; smax[w][d] = ghi[d]; }
+        if (anynan) atomicOr(&snan, 2);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w2 = 1; w2 < kThreads / 32; ++w2)
+            for (int d = 0; d < D; ++d) {
+                smin[0][d] = jl_min(smin[0][d], smin[w2][d]);
+                smax[0][d] = jl_max(smax[0][d], smax[w2][d]);
+            }
+        for (int d = 0; d < D; ++d) { hdr->gmin[d] = (double)smin[0][d]; hdr->gmax[d] = (double)smax[0][d]; }
+        hdr->nan_flag = (snan & 2) ? 1 : 0;
         hdr->n_blocks_done = 0;
     }
 }
@@ -194,87 +216,14 @@ __global__ void __launch_bounds__(kThreads) k_mark(const K* __restrict__ skeys, 
     }
 }
 
-// Writes node (L, k) with BFS id `id`.  first_child < 0 marks a leaf.
-template <class T, int D, class K>
-__device__ void emit_node(const K* __restrict__ skeys, int64_t n, int L, int64_t k, int32_t id,
-                          int32_t first_child, TNode<T, D>* __restrict__ tnode, int2* __restrict__ nrange,
-                          int32_t* __restrict__ parent, int32_t* __restrict__ arrive, const OctHeader* hdr) {
-    constexpr int BITS = Dims<D>::bits;
-    constexpr int NCH = Dims<D>::nch;
-    int64_t e = n;
-    if (L > 0) {
-        const int sh = D * (BITS - L);
-        const uint64_t pk = (uint64_t)skeys[k] >> sh;
-        int64_t good = k, bad = n, step = 1;
-        while (true) {
-            const int64_t p = k + step;
-            if (p >= n) break;
-            if (((uint64_t)skeys[p] >> sh) != pk) { bad = p; break; }
-            good = p;
-            step <<= 1;
-        }
-        int64_t a = good + 1, b = bad;
-        while (a < b) {
-            const int64_t mid = (a + b) >> 1;
-            if (((uint64_t)skeys[mid] >> sh) != pk) b = mid; else a = mid + 1;
-        }
-        e = a;
-    }
-    TNode<T, D> nd;
-    if (first_child < 0) {
-        nd.a = (int32_t)k;
-        nd.b = (int32_t)(e - k);
-    } else {
-        const int shd = D * BITS - D * (L + 1);
-        const uint64_t msk = (uint64_t)(NCH - 1);
-        const int d0 = (int)(((uint64_t)skeys[k] >> shd) & msk);
-        const int d1 = (int)(((uint64_t)skeys[e - 1] >> shd) & msk);
-        unsigned slots = 1u << d0;
-        if (d1 != d0) {
-            // Boundaries bnd[v] = first position in [k, e) whose digit >= v.
-            int64_t prev = k;
-            for (int v = d0 + 1; v <= d1; ++v) {
-                int64_t a = prev, b = e;
-                while (a < b) {
-                    const int64_t mid = (a + b) >> 1;
-                    if ((int)(((uint64_t)skeys[mid] >> shd) & msk) >= v) b = mid; else a = mid + 1;
-                }
-                // Digit v is present iff the next boundary is beyond this one.
-                int64_t a2 = a, b2 = e;
-                while (a2 < b2) {
-                    const int64_t mid = (a2 + b2) >> 1;
-                    if ((int)(((uint64_t)skeys[mid] >> shd) & msk) >= v + 1) b2 = mid; else a2 = mid + 1;
-                }
-                if (a2 > a) slots |= 1u << v;
-                prev = a;
-            }
-        }
-        nd.a = first_child;
-        nd.b = -(int32_t)slots;
-        const int nc = __popc(slots);
-        for (int j = 0; j < nc; ++j) parent[first_child + j] = id;
-    }
-    if (k == 0 && e == n) {
-        // A node covering every point has the global bounds.
-#pragma unroll
-        for (int d = 0; d < D; ++d) { nd.lo[d] = (T)hdr->gmin[d]; nd.hi[d] = (T)hdr->gmax[d]; }
-    } else {
-#pragma unroll
-        for (int d = 0; d < D; ++d) { nd.lo[d] = T(0); nd.hi[d] = T(0); }
-    }
-    tnode[id] = nd;
-    nrange[id] = make_int2((int)k, (int)(e - 1));
-    arrive[id] = 0;
-    if (id == 0) parent[0] = -1;
-}
-
-template <class T, int D, class K>
-__global__ void __launch_bounds__(kThreads) k_emit(const K* __restrict__ skeys, int64_t n,
-                                                   const uint16_t* __restrict__ lohi,
-                                                   const int64_t* __restrict__ blockoff, int nblocks,
-                                                   int64_t capacity, TNode<T, D>* __restrict__ tnode,
-                                                   int2* __restrict__ nrange, int32_t* __restrict__ parent,
-                                                   int32_t* __restrict__ arrive, OctHeader* hdr) {
+// Node (L, k) -> BFS id.  Writes nrange[id] = {k, L} and tnode[id].a = the
+// id of the first child (the node (L+1, k)), or -1 for a leaf; k_emit_nodes
+// completes each node from these.
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_emit_ids(int64_t n, const uint16_t* __restrict__ lohi,
+                                                       const int64_t* __restrict__ blockoff, int nblocks,
+                                                       int64_t capacity, int32_t* __restrict__ first_child,
+                                                       int2* __restrict__ nrange, OctHeader* hdr) {
     constexpr int NLEV = Dims<D>::bits + 1;
     __shared__ int32_t wpre[NLEV][kThreads / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -311,10 +260,93 @@ __global__ void __launch_bounds__(kThreads) k_emit(const K* __restrict__ skeys, 
         if (in) {
             const int32_t id = (int32_t)(blockoff[(int64_t)L * nblocks + blockIdx.x] + wpre[L][w] +
                                          __popc(b & lanemask_lt()));
-            emit_node<T, D, K>(skeys, n, L, k, id, L < hi ? prev : -1, tnode, nrange, parent, arrive, hdr);
+            nrange[id] = make_int2((int)k, L);
+            first_child[id] = L < hi ? prev : -1;
             prev = id;
         }
     }
+}
+
+// Completes node `id`: its last position (end of its level-L key group), its
+// occupied child slots and the children's parent links.
+template <class T, int D, class K>
+__global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ skeys, int64_t n, int64_t capacity,
+                                                         const int32_t* __restrict__ first_child_in,
+                                                         TNode<T, D>* __restrict__ tnode, int2* __restrict__ nrange,
+                                                         int32_t* __restrict__ parent, int32_t* __restrict__ arrive,
+                                                         const OctHeader* hdr) {
+    constexpr int BITS = Dims<D>::bits;
+    constexpr int NCH = Dims<D>::nch;
+    const int64_t nn = hdr->n_nodes;
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (nn > capacity || id >= nn) return;
+    const int2 kl = nrange[id];
+    const int64_t k = kl.x;
+    const int L = kl.y;
+    const int32_t first_child = first_child_in[id];
+    int64_t e = n;
+    if (L > 0) {
+        const int sh = D * (BITS - L);
+        const uint64_t pk = (uint64_t)skeys[k] >> sh;
+        if (((uint64_t)skeys[n - 1] >> sh) != pk) {
+            // Galloping search for the first position whose level-L prefix differs.
+            int64_t good = k, bad = n, step = 1;
+            while (true) {
+                const int64_t p = k + step;
+                if (p >= n) break;
+                if (((uint64_t)skeys[p] >> sh) != pk) { bad = p; break; }
+                good = p;
+                step <<= 1;
+            }
+            int64_t a = good + 1, b = bad;
+            while (a < b) {
+                const int64_t mid = (a + b) >> 1;
+                if (((uint64_t)skeys[mid] >> sh) != pk) b = mid; else a = mid + 1;
+            }
+            e = a;
+        }
+    }
+    TNode<T, D> nd;
+    if (first_child < 0) {
+        nd.a = (int32_t)k;
+        nd.b = (int32_t)(e - k);
+    } else {
+        const int shd = D * BITS - D * (L + 1);
+        const uint64_t msk = (uint64_t)(NCH - 1);
+        const int d0 = (int)(((uint64_t)skeys[k] >> shd) & msk);
+        const int d1 = (int)(((uint64_t)skeys[e - 1] >> shd) & msk);
+        unsigned slots = 1u << d0;
+        if (d1 != d0) {
+            // lb(v) = first position in [k, e) whose digit >= v; digit v is
+            // occupied iff lb(v) < lb(v + 1).
+            int64_t prev = k;
+            for (int v = d0 + 1; v <= d1; ++v) {
+                int64_t a = prev, b = e;
+                while (a < b) {
+                    const int64_t mid = (a + b) >> 1;
+                    if ((int)(((uint64_t)skeys[mid] >> shd) & msk) >= v) b = mid; else a = mid + 1;
+                }
+                if (a < e && (int)(((uint64_t)skeys[a] >> shd) & msk) == v) slots |= 1u << v;
+                prev = a;
+            }
+        }
+        nd.a = first_child;
+        nd.b = -(int32_t)slots;
+        const int nc = __popc(slots);
+        for (int j = 0; j < nc; ++j) parent[first_child + j] = (int32_t)id;
+    }
+    if (k == 0 && e == n) {
+        // A node covering every point has the global bounds.
+#pragma unroll
+        for (int d = 0; d < D; ++d) { nd.lo[d] = (T)hdr->gmin[d]; nd.hi[d] = (T)hdr->gmax[d]; }
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) { nd.lo[d] = T(0); nd.hi[d] = T(0); }
+    }
+    tnode[id] = nd;
+    nrange[id] = make_int2((int)k, (int)(e - 1));
+    arrive[id] = 0;
+    if (id == 0) parent[0] = -1;
 }
 
 // ------------------------------------------------------------- 6. refit --
@@ -427,14 +459,15 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
     }
 
     // --- sort (stable: ties keep ascending original index, src/sort.jl:15-24)
-    if ((err = ensure(t.hist, (size_t)256 * sort_tiles(n) * 4))) return cuda_status(ctx, err, "allocating histograms");
+    if ((err = ensure(t.hist, sort_hist_bytes(n))) || (err = ensure(t.sort_tmp, sort_scan_bytes(n))))
+        return cuda_status(ctx, err, "allocating histograms");
     K* kb[2] = {t.keys[0].as<K>(), t.keys[1].as<K>()};
     int32_t* vb[2] = {t.vals[0].as<int32_t>(), t.vals[1].as<int32_t>()};
     int src;
     {
         PhaseTimer pt_(ctx, PH_SORT);
-        src = radix_sort_pairs<K>(kb, vb, t.hist.as<int32_t>(), n, t.key_bits, false, s);
-        ctx.kernel_launches += 3 * t.sort_passes;
+        src = radix_sort_pairs<K>(kb, vb, t.hist.as<int32_t>(), t.sort_tmp.as<int64_t>(), n, t.key_bits, false, s);
+        ctx.kernel_launches += 5 * t.sort_passes;
     }
     const K* skeys = kb[src];
     const int32_t* perm = t.sort_passes ? vb[src] : nullptr;
@@ -461,17 +494,20 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
     for (int attempt = 0; attempt < 3; ++attempt) {
         const int64_t cap = t.capacity;
         if ((err = ensure(t.tnode, (size_t)cap * sizeof(TNode<T, D>))) || (err = ensure(t.nrange, (size_t)cap * 8)) ||
-            (err = ensure(t.parent, (size_t)cap * 4)) || (err = ensure(t.arrive, (size_t)cap * 4)))
+            (err = ensure(t.parent, (size_t)cap * 4)) || (err = ensure(t.arrive, (size_t)cap * 4)) ||
+            (err = ensure(t.fchild, (size_t)cap * 4)))
             return cuda_status(ctx, err, "allocating node arrays");
         {
         PhaseTimer pt_(ctx, PH_TOPOLOGY);
         k_mark<D, K><<<nblocks, kThreads, 0, s>>>(skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(), nblocks);
         exclusive_scan_i32_i64(t.blockcnt.as<int32_t>(), t.blockoff.as<int64_t>(), nbc, &hdr->n_nodes,
                                t.scan_tmp.as<int64_t>(), s);
-        k_emit<T, D, K><<<nblocks, kThreads, 0, s>>>(skeys, n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks,
-                                                     cap, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
-                                                     t.parent.as<int32_t>(), t.arrive.as<int32_t>(), hdr);
-        ctx.kernel_launches += 5;
+        k_emit_ids<D><<<nblocks, kThreads, 0, s>>>(n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks, cap,
+                                                    t.fchild.as<int32_t>(), t.nrange.as<int2>(), hdr);
+        k_emit_nodes<T, D, K><<<div_up(cap, kThreads), kThreads, 0, s>>>(
+            skeys, n, cap, t.fchild.as<int32_t>(), t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
+            t.parent.as<int32_t>(), t.arrive.as<int32_t>(), hdr);
+        ctx.kernel_launches += 6;
         }
         {
         PhaseTimer pt_(ctx, PH_REFIT);

@@ -96,8 +96,8 @@ struct DeviceGuard {
 
 void release_tree(oct::Tree& t) {
     using oct::release;
-    for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.spts, &t.tnode, &t.nrange,
-                    &t.parent, &t.arrive, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
+    for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.sort_tmp, &t.spts, &t.tnode, &t.nrange,
+                    &t.parent, &t.fchild, &t.arrive, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
                     &t.morton, &t.v_first, &t.v_last, &t.v_children, &t.v_bmin, &t.v_bmax, &t.v_perm})
         release(*b);
     if (t.hdr_host) cudaFreeHost(t.hdr_host);
@@ -148,7 +148,7 @@ OCT_API int oct_ctx_destroy(oct_ctx* ctx) {
     cudaStreamSynchronize(ctx->c.stream);
     using oct::release;
     for (auto* b : {&ctx->c.counts, &ctx->c.offsets, &ctx->c.scan_tmp, &ctx->c.total, &ctx->c.dkeys[0],
-                    &ctx->c.dkeys[1], &ctx->c.dvals[0], &ctx->c.dvals[1], &ctx->c.dhist, &ctx->c.droff,
+                    &ctx->c.dkeys[1], &ctx->c.dvals[0], &ctx->c.dvals[1], &ctx->c.dhist, &ctx->c.dsort_tmp, &ctx->c.droff,
                     &ctx->c.dsoff, &ctx->c.dstatus})
         release(*b);
     if (ctx->c.total_host) cudaFreeHost(ctx->c.total_host);

@@ -105,7 +105,8 @@ int backward_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int
     }
     if ((err = ensure(ctx.dkeys[0], m * 4)) || (err = ensure(ctx.dkeys[1], m * 4)) ||
         (err = ensure(ctx.dvals[0], m * 4)) || (err = ensure(ctx.dvals[1], m * 4)) ||
-        (err = ensure(ctx.dhist, (size_t)256 * sort_tiles(m) * 4)) || (err = ensure(ctx.droff, (n + 1) * 8)) ||
+        (err = ensure(ctx.dhist, sort_hist_bytes(m))) || (err = ensure(ctx.dsort_tmp, sort_scan_bytes(m))) ||
+        (err = ensure(ctx.droff, (n + 1) * 8)) ||
         (err = ensure(ctx.dsoff, (n + 1) * 8)))
         return cuda_status(ctx, err, "allocating adjoint scratch");
     const int tb = 256;
@@ -116,13 +117,14 @@ int backward_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int
     while (bits < 32 && ((uint64_t)(n - 1) >> bits) != 0) ++bits;
     uint32_t* kb[2] = {ctx.dkeys[0].as<uint32_t>(), ctx.dkeys[1].as<uint32_t>()};
     int32_t* vb[2] = {ctx.dvals[0].as<int32_t>(), ctx.dvals[1].as<int32_t>()};
-    const int src = radix_sort_pairs<uint32_t>(kb, vb, ctx.dhist.as<int32_t>(), m, bits, false, s);
+    const int src = radix_sort_pairs<uint32_t>(kb, vb, ctx.dhist.as<int32_t>(), ctx.dsort_tmp.as<int64_t>(), m, bits,
+                                               false, s);
     const int32_t* sorted_edge = bits > 0 ? vb[src] : nullptr;
     k_sorted_starts<<<div_up(n + 1, tb), tb, 0, s>>>(kb[src], m, n, ctx.dsoff.as<int64_t>());
     k_grad<T, D><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), ctx.dsoff.as<int64_t>(), sorted_edge,
                                              (const T*)rel_disp, (const T*)rel_dist, (const T*)d_disp,
                                              (const T*)d_dist, r, (T*)grad);
-    ctx.kernel_launches += 4 + 3 * ((bits + 7) / 8);
+    ctx.kernel_launches += 4 + 5 * ((bits + 7) / 8);
     return cuda_status(ctx, cudaGetLastError(), "adjoint launch");
 }
 

@@ -38,7 +38,9 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ dstatus) {
     constexpr int SD = stack_depth<D>();
-    __shared__ int32_t stack[kEdgeWarps][SD];
+    // Stack entries are the pushed node's (a, b) record; bit 31 of a marks
+    // ascending-order subtrees (see below).
+    __shared__ int2 stack[kEdgeWarps][SD];
     __shared__ SPt<T, D> tgt[kEdgeWarps][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t qbase = ((int64_t)blockIdx.x * kEdgeWarps + w) * 32;
@@ -63,46 +65,43 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     if (n_tnodes > 0) {
         const TNode<T, D> root = tnode[0];
         if (box_gap2<T, D>(qlo, qhi, root.lo, root.hi) <= r2) {
-            if (lane == 0) stack[w][0] = 0;
+            if (lane == 0) stack[w][0] = make_int2(root.a, root.b);
             sp = 1;
         }
     }
     __syncwarp();
     while (sp > 0) {
-        const int32_t ent = stack[w][--sp];
-        const int32_t nid = ent & 0x7fffffff;
-        const bool asc = ent < 0;
-        const TNode<T, D> nd = tnode[nid];
-        if (nd.b > 0) {
-            // Leaf: per-lane point-to-box prefilter, then every pair.
-            const bool act = valid && box_gap2<T, D>(q.x, q.x, nd.lo, nd.hi) <= r2;
-            if (__any_sync(0xffffffffu, act)) {
-                for (int32_t c0 = 0; c0 < nd.b; c0 += 32) {
-                    const int m = min(32, nd.b - c0);
-                    __syncwarp();
-                    if (lane < m) tgt[w][lane] = tpts[nd.a + c0 + lane];
-                    __syncwarp();
-                    for (int j = 0; j < m; ++j) {
-                        const SPt<T, D> t = tgt[w][j];
-                        T diff[D];
-                        const T d2 = dist2<T, D>(t.x, q.x, diff);
-                        const bool hit = act && d2 <= r2;
-                        if (FILL) {
-                            if (hit && !(self_pair && t.idx == q.idx)) {
-                                if (cur >= cur_end) {  // never taken when count and fill agree
-                                    atomicOr(dstatus, 1);
-                                    continue;
-                                }
-                                senders[cur] = t.idx + 1;
-                                receivers[cur] = q.idx + 1;
-#pragma unroll
-                                for (int d = 0; d < D; ++d) rdisp[(int64_t)D * cur + d] = mul_rn(-diff[d], inv_r);
-                                rdist[cur] = mul_rn(sqrt_rn(d2), inv_r);
-                                ++cur;
+        const int2 ent = stack[w][--sp];
+        const bool asc = ent.x < 0;
+        const int32_t na = ent.x & 0x7fffffff;
+        const int32_t nb = ent.y;
+        if (nb > 0) {
+            // Leaf: every (query, point) pair, points in ascending position.
+            for (int32_t c0 = 0; c0 < nb; c0 += 32) {
+                const int m = min(32, nb - c0);
+                __syncwarp();
+                if (lane < m) tgt[w][lane] = tpts[na + c0 + lane];
+                __syncwarp();
+                for (int j = 0; j < m; ++j) {
+                    const SPt<T, D> t = tgt[w][j];
+                    T diff[D];
+                    const T d2 = dist2<T, D>(t.x, q.x, diff);
+                    const bool hit = valid && d2 <= r2;
+                    if (FILL) {
+                        if (hit && !(self_pair && t.idx == q.idx)) {
+                            if (cur >= cur_end) {  // never taken when count and fill agree
+                                atomicOr(dstatus, 1);
+                                continue;
                             }
-                        } else {
-                            cnt += hit ? 1 : 0;
+                            senders[cur] = t.idx + 1;
+                            receivers[cur] = q.idx + 1;
+#pragma unroll
+                            for (int d = 0; d < D; ++d) rdisp[(int64_t)D * cur + d] = mul_rn(-diff[d], inv_r);
+                            rdist[cur] = mul_rn(sqrt_rn(d2), inv_r);
+                            ++cur;
                         }
+                    } else {
+                        cnt += hit ? 1 : 0;
                     }
                 }
             }
@@ -111,20 +110,21 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             // empty as one leaf, in ascending position order
             // (src/cpu/iterator_cpu.jl:87-101).  Below such a node the
             // children are therefore visited in ascending slot order.
-            const unsigned slots = (unsigned)(-nd.b);
+            const unsigned slots = (unsigned)(-nb);
             const bool casc = asc || !(slots & 1u);
             const int nc = __popc(slots);
             bool pass = false;
+            int2 rec = make_int2(0, 0);
             if (lane < nc) {
-                const TNode<T, D> c = tnode[nd.a + lane];
+                const TNode<T, D> c = tnode[na + lane];
                 pass = box_gap2<T, D>(qlo, qhi, c.lo, c.hi) <= r2;
+                rec = make_int2(c.a | (casc ? (int32_t)0x80000000 : 0), c.b);
             }
             const unsigned m = __ballot_sync(0xffffffffu, pass);
             const int np = __popc(m);
-            __syncwarp();
             if (pass) {
                 const int rk = __popc(m & lanemask_lt());
-                stack[w][casc ? sp + np - 1 - rk : sp + rk] = (nd.a + lane) | (casc ? (int32_t)0x80000000 : 0);
+                stack[w][casc ? sp + np - 1 - rk : sp + rk] = rec;
             }
             sp += np;
             __syncwarp();

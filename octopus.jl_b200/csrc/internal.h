@@ -66,11 +66,13 @@ struct Tree {
 
     // Device storage.
     DevBuf keys[2], vals[2];     // radix-sort ping-pong
-    DevBuf hist;                 // radix digit histograms
+    DevBuf hist;                 // radix digit histograms (+1 total slot)
+    DevBuf sort_tmp;             // int64 tile sums of the histogram scan
     DevBuf spts;                 // SPt<T,D>[n] in Morton order
     DevBuf tnode;                // TNode<T,D>[capacity]
     DevBuf nrange;               // int2 {first,last} 0-based per node
     DevBuf parent;               // int32 per node (-1 for the root)
+    DevBuf fchild;               // int32 per node: first child id from the id pass
     DevBuf arrive;               // int32 per node, refit arrival counters
     DevBuf lohi;                 // uint16 per position: first | last level starting here
     DevBuf blockcnt;             // int32 [(maxlev+1) * n_mark_blocks]
@@ -104,7 +106,7 @@ struct Ctx {
     int plan_exclude = -1;
     int64_t plan_edges = -1;
     // Adjoint scratch (diff.cu).
-    DevBuf dkeys[2], dvals[2], dhist, droff, dsoff;
+    DevBuf dkeys[2], dvals[2], dhist, dsort_tmp, droff, dsoff;
     // Profiler.
     int64_t kernel_launches = 0;  // every kernel this context has launched
     bool profiling = false;

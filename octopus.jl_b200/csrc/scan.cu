@@ -5,7 +5,8 @@
 namespace oct {
 
 // Per-tile sums of kScanTile consecutive inputs.
-__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const int32_t* __restrict__ in, int64_t n,
+template <class In>
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const In* __restrict__ in, int64_t n,
                                                                  int64_t* __restrict__ tile_sums) {
     __shared__ int64_t sm[kScanThreads / 32 + 1];
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
@@ -38,11 +39,11 @@ __global__ void __launch_bounds__(1024) k_scan_tiles(int64_t* __restrict__ tile_
 
 // Final pass: each tile scans its items in order (blocked per thread) and
 // adds the tile offset.
-__global__ void __launch_bounds__(kScanThreads) k_scan_final(const int32_t* __restrict__ in, int64_t n,
-                                                             const int64_t* __restrict__ tile_off,
-                                                             int64_t* __restrict__ out) {
+template <class In, class Out>
+__global__ void __launch_bounds__(kScanThreads) k_scan_final(const In* in, int64_t n,
+                                                             const int64_t* __restrict__ tile_off, Out* out) {
     __shared__ int64_t sm[kScanThreads / 32 + 1];
-    __shared__ int32_t stage[kScanTile];
+    __shared__ In stage[kScanTile];
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
     // Coalesced load into shared memory, then each thread owns kScanItems
     // consecutive elements.
@@ -53,7 +54,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const int32_t* __re
         stage[j] = i < n ? in[i] : 0;
     }
     __syncthreads();
-    int32_t v[kScanItems];
+    In v[kScanItems];
     int64_t s = 0;
 #pragma unroll
     for (int it = 0; it < kScanItems; ++it) {
@@ -65,24 +66,34 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const int32_t* __re
 #pragma unroll
     for (int it = 0; it < kScanItems; ++it) {
         const int64_t i = base + (int64_t)threadIdx.x * kScanItems + it;
-        if (i < n) out[i] = run;
+        if (i < n) out[i] = (Out)run;
         run += v[it];
     }
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = tile_off[blockIdx.x] + tot;
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = (Out)(tile_off[blockIdx.x] + tot);
 }
 
 // out[0..n] = exclusive scan of in[0..n-1]; out[n] = total (also *d_total).
-void exclusive_scan_i32_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* d_total,
-                            int64_t* tile_tmp, cudaStream_t s) {
+// `in` and `out` may alias: each tile stages its inputs before writing.
+template <class In, class Out>
+void exclusive_scan(const In* in, Out* out, int64_t n, int64_t* d_total, int64_t* tile_tmp, cudaStream_t s) {
     if (n <= 0) {
-        cudaMemsetAsync(out, 0, sizeof(int64_t), s);
+        cudaMemsetAsync(out, 0, sizeof(Out), s);
         if (d_total) cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
         return;
     }
     const int ntiles = div_up(n, kScanTile);
-    k_scan_tile_sums<<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp);
+    k_scan_tile_sums<In><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp);
     k_scan_tiles<<<1, 1024, 0, s>>>(tile_tmp, ntiles, d_total);
-    k_scan_final<<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp, out);
+    k_scan_final<In, Out><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp, out);
+}
+
+void exclusive_scan_i32_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* d_total, int64_t* tile_tmp,
+                            cudaStream_t s) {
+    exclusive_scan<int32_t, int64_t>(in, out, n, d_total, tile_tmp, s);
+}
+
+void exclusive_scan_i32_i32(const int32_t* in, int32_t* out, int64_t n, int64_t* tile_tmp, cudaStream_t s) {
+    exclusive_scan<int32_t, int32_t>(in, out, n, nullptr, tile_tmp, s);
 }
 
 }  // namespace oct

@@ -42,6 +42,8 @@ template <class T> __device__ __forceinline__ T block_exclusive_scan(T v, T* sme
 
 void exclusive_scan_i32_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* d_total,
                             int64_t* tile_tmp, cudaStream_t s);
+// In-place capable int32 scan; `out` holds n + 1 elements.
+void exclusive_scan_i32_i32(const int32_t* in, int32_t* out, int64_t n, int64_t* tile_tmp, cudaStream_t s);
 inline int64_t scan_tmp_elems(int64_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
 
 }  // namespace oct

@@ -29,20 +29,6 @@ static __global__ void __launch_bounds__(kSortThreads) k_hist(const K* __restric
     hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = cnt[threadIdx.x];
 }
 
-// In-place exclusive scan of m int32 values by one block.
-static __global__ void __launch_bounds__(1024) k_scan_hist(int32_t* __restrict__ h, int64_t m) {
-    __shared__ int32_t sm[1024 / 32 + 1];
-    int32_t carry = 0;
-    for (int64_t base = 0; base < m; base += 1024) {
-        const int64_t i = base + threadIdx.x;
-        const int32_t v = i < m ? h[i] : 0;
-        int32_t tot;
-        const int32_t ex = block_exclusive_scan<int32_t>(v, sm, &tot);
-        if (i < m) h[i] = carry + ex;
-        carry += tot;
-    }
-}
-
 template <class K>
 static __global__ void __launch_bounds__(kSortThreads) k_scatter(const K* __restrict__ kin, const int32_t* __restrict__ vin,
                                                       K* __restrict__ kout, int32_t* __restrict__ vout, int64_t n,
@@ -96,21 +82,25 @@ static __global__ void __launch_bounds__(kSortThreads) k_scatter(const K* __rest
 
 
 inline int sort_tiles(int64_t n) { return (int)((n + kSortTile - 1) / kSortTile); }
+// Histogram buffer: 256 digit counts per tile plus the scan's total slot.
+inline size_t sort_hist_bytes(int64_t n) { return (size_t)(256 * (int64_t)sort_tiles(n) + 1) * 4; }
+// Scan scratch (int64 tile sums) for the histogram scan.
+inline size_t sort_scan_bytes(int64_t n) { return (size_t)scan_tmp_elems(256 * (int64_t)sort_tiles(n)) * 8; }
 
-// Sorts n pairs by the low `bits` bits of the key.  Input in (k[0], v[0])
+// Sorts n pairs by the low `bits` bits of the key; 5 launches per 8-bit pass.  Input in (k[0], v[0])
 // (v[0] may be null for the identity 0..n-1); returns the index (0 or 1) of
 // the buffers holding the result.  With zero passes the result is the input
 // and v[0] stays untouched (the caller treats a null value buffer as iota).
 template <class K>
-int radix_sort_pairs(K* k[2], int32_t* v[2], int32_t* hist, int64_t n, int bits, bool vals_in,
-                     cudaStream_t s) {
+int radix_sort_pairs(K* k[2], int32_t* v[2], int32_t* hist, int64_t* scan_tmp, int64_t n, int bits,
+                     bool vals_in, cudaStream_t s) {
     const int ntiles = sort_tiles(n);
     const int passes = (bits + 7) / 8;
     int src = 0;
     for (int p = 0; p < passes; ++p) {
         const int shift = 8 * p;
         k_hist<K><<<ntiles, kSortThreads, 0, s>>>(k[src], n, shift, hist, ntiles);
-        k_scan_hist<<<1, 1024, 0, s>>>(hist, (int64_t)256 * ntiles);
+        exclusive_scan_i32_i32(hist, hist, (int64_t)256 * ntiles, scan_tmp, s);
         k_scatter<K><<<ntiles, kSortThreads, 0, s>>>(k[src], (p == 0 && !vals_in) ? nullptr : v[src], k[src ^ 1],
                                                      v[src ^ 1], n, shift, hist, ntiles);
         src ^= 1;

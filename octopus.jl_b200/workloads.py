@@ -1,0 +1,107 @@
+"""Seeded synthetic inputs with the shapes of the benchmark configurations,
+and a small runner used for device profiling.
+
+    python octopus.jl_b200/workloads.py <workload> [--steps S] [--scale F]
+
+runs S time steps of run! + build_edges on cuda:0 (used as the target of
+ncu captures; it prints the edge count per step).
+
+Workloads (float32):
+  uniform100k  3D, 100,000 points U[0,1)^3, r = 0.04
+  sph          3D, 100^3 lattice, h = 0.01, jitter +-0.1h, r = 2h, Gaussian
+               steps of sigma = 0.005h (``--scale`` shrinks the lattice side)
+  mix2d        2D, 4,000,000 points: 64 Gaussians (sigma U[0.005, 0.05],
+               Dirichlet(1) weights) + 10% uniform, in [0,1)^2, r = 0.002
+  diff2m       3D, 2,000,000 points U[0,1)^3, r = 0.012
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+H = 0.01
+
+
+def lattice(per: int, seed: int, h: float = H, jitter: float = 0.1 * H, ndims: int = 3) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(*[np.arange(per)] * ndims, indexing="ij"), -1).reshape(-1, ndims).astype(np.float64)
+    return (g * h + rng.uniform(-jitter, jitter, g.shape)).astype(np.float32)
+
+
+def sph_snapshots(per: int, nsteps: int, seed: int, sigma: float = 0.005 * H) -> list[np.ndarray]:
+    """Coordinates of time steps 0..nsteps-1: a jittered lattice moved by
+    independent Gaussian displacements each step."""
+    rng = np.random.default_rng(seed + 1)
+    x = lattice(per, seed)
+    out = [x]
+    for _ in range(nsteps - 1):
+        x = (x + rng.normal(0.0, sigma, x.shape)).astype(np.float32)
+        out.append(x)
+    return out
+
+
+def uniform(n: int, ndims: int, seed: int, dtype=np.float32) -> np.ndarray:
+    return np.random.default_rng(seed).random((n, ndims)).astype(dtype)
+
+
+def gaussian_mixture_2d(n: int, k: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    centers = rng.random((k, 2))
+    sig = rng.uniform(0.005, 0.05, k)
+    w = rng.dirichlet(np.ones(k))
+    nb = n // 10
+    comp = rng.choice(k, size=n - nb, p=w)
+    pts = centers[comp] + sig[comp, None] * rng.standard_normal((n - nb, 2))
+    bad = ((pts < 0) | (pts >= 1)).any(1)
+    while bad.any():
+        pts[bad] = centers[comp[bad]] + sig[comp[bad], None] * rng.standard_normal((int(bad.sum()), 2))
+        bad = ((pts < 0) | (pts >= 1)).any(1)
+    return np.concatenate([pts, rng.random((nb, 2))]).astype(np.float32)
+
+
+def _run(name: str, steps: int, scale: float):
+    import torch
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.dirname(here))
+    import __graft_entry__
+    ob = __graft_entry__.load_package()
+    if name == "sph":
+        per = max(4, int(round(100 * scale)))
+        xs = sph_snapshots(per, steps, 12345)
+        r = 2 * H
+    elif name == "uniform100k":
+        xs = [uniform(int(100_000 * scale), 3, 2024)] * steps
+        r = 0.04
+    elif name == "mix2d":
+        xs = [gaussian_mixture_2d(int(4_000_000 * scale), 64, 2026)] * steps
+        r = 0.002
+    elif name == "diff2m":
+        xs = [uniform(int(2_000_000 * scale), 3, 2025)] * steps
+        r = 0.012
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    d = xs[0].shape[1]
+    tns = ob.TNS(torch.float32, ndims=d)
+    ob.set_search_radius_(tns, r)
+    ob.set_refit_mode_(tns, True)
+    dev = [torch.from_numpy(x).cuda().t() for x in xs]
+    sid = ob.add_point_set_(tns, dev[0])
+    ob.set_active_search_(tns, sid, sid)
+    for x in dev:
+        ob.update_point_set_(tns, sid, x)
+        ob.run_(tns)
+        e = ob.build_edges(tns, sid, sid)
+        ob.synchronize(tns)
+        print(f"{name}: n={x.shape[1]} edges={e.senders.numel()}")
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("workload")
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--scale", type=float, default=1.0)
+    a = ap.parse_args()
+    _run(a.workload, a.steps, a.scale)
