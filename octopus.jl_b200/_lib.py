@@ -66,7 +66,7 @@ SIGNATURES = [
     ("oct_profile_kernel_launches", I64, [P]),
 ]
 
-PHASES = ["bounds", "encode", "sort", "gather", "topology", "refit", "count", "scan", "fill", "adjoint"]
+PHASES = ["bounds", "encode", "sort", "gather", "topology", "refit", "count", "scan", "fill", "adjoint", "groups"]
 
 _LIB = None
 _LOCK = threading.Lock()

@@ -401,7 +401,63 @@ __global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n,
     }
 }
 
-// --------------------------------------------------- 7. reference views --
+// ------------------------------------------------------- 7. query groups --
+// A query group is a run of consecutive sibling leaves holding at most 32
+// points in total (a leaf of more than 32 points, possible at the last
+// level, is cut into chunks of 32).  Siblings share a parent box, so a
+// group's points are spatially compact; a window of 32 consecutive sorted
+// positions can instead straddle a jump of the Morton curve and span the
+// whole domain.  pass 0 counts the groups formed under each node, pass 1
+// writes them at the scanned offsets.
+template <class T, int D, int PASS>
+__global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restrict__ tnode, int64_t capacity,
+                                                     int32_t* __restrict__ gcnt, const int64_t* __restrict__ goff,
+                                                     int2* __restrict__ groups, const OctHeader* hdr) {
+    const int64_t nn = hdr->n_nodes;
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (nn > capacity || id >= capacity) return;
+    if (id >= nn) {
+        if (!PASS) gcnt[id] = 0;  // the scan runs over the whole capacity
+        return;
+    }
+    const TNode<T, D> nd = tnode[id];
+    int64_t out = PASS ? goff[id] : 0;
+    int32_t ng = 0;
+    auto emit = [&](int32_t first, int32_t count) {
+        if (PASS) groups[out + ng] = make_int2(first, count);
+        ++ng;
+    };
+    if (nd.b > 0) {
+        // Only a leaf root forms groups of its own.
+        if (id == 0)
+            for (int32_t c0 = 0; c0 < nd.b; c0 += 32) emit(nd.a + c0, min(32, nd.b - c0));
+    } else {
+        const int nc = __popc((unsigned)(-nd.b));
+        int32_t gfirst = 0, gcount = 0;
+        for (int j = 0; j < nc; ++j) {
+            const TNode<T, D> c = tnode[nd.a + j];
+            if (c.b <= 0) {  // internal child: close the open group
+                if (gcount) emit(gfirst, gcount);
+                gcount = 0;
+            } else if (c.b > 32) {
+                if (gcount) emit(gfirst, gcount);
+                gcount = 0;
+                for (int32_t c0 = 0; c0 < c.b; c0 += 32) emit(c.a + c0, min(32, c.b - c0));
+            } else {
+                if (gcount + c.b > 32) {
+                    emit(gfirst, gcount);
+                    gcount = 0;
+                }
+                if (gcount == 0) gfirst = c.a;
+                gcount += c.b;
+            }
+        }
+        if (gcount) emit(gfirst, gcount);
+    }
+    if (!PASS) gcnt[id] = ng;
+}
+
+// --------------------------------------------------- 8. reference views --
 template <class T, int D>
 __global__ void k_view_nodes(const TNode<T, D>* __restrict__ tnode, const int2* __restrict__ nrange, int64_t nn,
                              int32_t* __restrict__ vf, int32_t* __restrict__ vl, int32_t* __restrict__ vc,
@@ -495,7 +551,10 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
         const int64_t cap = t.capacity;
         if ((err = ensure(t.tnode, (size_t)cap * sizeof(TNode<T, D>))) || (err = ensure(t.nrange, (size_t)cap * 8)) ||
             (err = ensure(t.parent, (size_t)cap * 4)) || (err = ensure(t.arrive, (size_t)cap * 4)) ||
-            (err = ensure(t.fchild, (size_t)cap * 4)))
+            (err = ensure(t.fchild, (size_t)cap * 4)) || (err = ensure(t.gcnt, (size_t)cap * 4)) ||
+            (err = ensure(t.goff, (size_t)(cap + 1) * 8)) ||
+            (err = ensure(t.scan_tmp, (size_t)std::max(scan_tmp_elems(nbc), scan_tmp_elems(cap)) * 8)) ||
+            (err = ensure(t.groups, (size_t)(cap + n / 32 + 2) * 8)))
             return cuda_status(ctx, err, "allocating node arrays");
         {
         PhaseTimer pt_(ctx, PH_TOPOLOGY);
@@ -516,6 +575,17 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
                                                                   t.spts.as<SPt<T, D>>(), hdr);
         ctx.kernel_launches += 1;
         }
+        {
+            PhaseTimer pt_(ctx, PH_GROUPS);
+            k_groups<T, D, 0><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
+                                                                        t.gcnt.as<int32_t>(), nullptr, nullptr, hdr);
+            exclusive_scan_i32_i64(t.gcnt.as<int32_t>(), t.goff.as<int64_t>(), cap, &hdr->n_groups,
+                                   t.scan_tmp.as<int64_t>(), s);
+            k_groups<T, D, 1><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
+                                                                        t.gcnt.as<int32_t>(), t.goff.as<int64_t>(),
+                                                                        t.groups.as<int2>(), hdr);
+            ctx.kernel_launches += 5;
+        }
         if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
             (err = cudaStreamSynchronize(s)))
             return cuda_status(ctx, err, "tree build");
@@ -526,6 +596,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
             continue;
         }
         t.n_nodes = t.hdr_host->n_nodes;
+        t.n_groups = t.hdr_host->n_groups;
         return OK;
     }
     return set_error(ctx, ERR_OVERFLOW, "tree build: node capacity retry did not converge");

@@ -97,7 +97,7 @@ struct DeviceGuard {
 void release_tree(oct::Tree& t) {
     using oct::release;
     for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.sort_tmp, &t.spts, &t.tnode, &t.nrange,
-                    &t.parent, &t.fchild, &t.arrive, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
+                    &t.parent, &t.fchild, &t.arrive, &t.groups, &t.gcnt, &t.goff, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
                     &t.morton, &t.v_first, &t.v_last, &t.v_children, &t.v_bmin, &t.v_bmax, &t.v_perm})
         release(*b);
     if (t.hdr_host) cudaFreeHost(t.hdr_host);
@@ -316,7 +316,7 @@ OCT_API int oct_edges_diff_backward(oct_ctx* ctx, int ndims, int dtype, int64_t 
 }
 
 static const char* kPhaseNames[oct::PH_NUM] = {"bounds", "encode", "sort", "gather", "topology",
-                                               "refit", "count", "scan", "fill", "adjoint"};
+                                               "refit", "count", "scan", "fill", "adjoint", "groups"};
 
 OCT_API int oct_profile_enable(oct_ctx* ctx, int on) {
     if (!ctx) return OCT_ERR_ARGUMENT;

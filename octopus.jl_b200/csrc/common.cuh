@@ -66,6 +66,7 @@ struct OctHeader {
     double gmax[3];
     int32_t n_blocks_done;
     int32_t pad;
+    int64_t n_groups;
 };
 
 // --------------------------------------------------- Julia float semantics --

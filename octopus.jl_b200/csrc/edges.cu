@@ -4,8 +4,9 @@
 // _build_edges_cuda! (ext/OctopusCUDAExt.jl:262-415) and reproduces the CPU
 // path's output exactly (src/cpu/edges_cpu.jl:36-247):
 //
-//   * One warp serves 32 queries that are consecutive in the query set's
-//     Morton order.  The warp walks the target tree once, depth first, with
+//   * One warp serves one query group of the query set's tree: a run of
+//     sibling leaves with at most 32 points (built with the tree), so the
+//     group's box is compact.  The warp walks the target tree once, depth first, with
 //     the box of its 32 queries: children are tested in slot order and
 //     pushed in that order onto a shared-memory stack, so leaves pop in the
 //     same order as the reference's per-query DFS
@@ -33,7 +34,8 @@ constexpr int kEdgeThreads = kEdgeWarps * 32;
 
 template <class T, int D, bool FILL>
 __global__ void __launch_bounds__(kEdgeThreads) k_edges(
-    const SPt<T, D>* __restrict__ qpts, int64_t nq, const TNode<T, D>* __restrict__ tnode,
+    const SPt<T, D>* __restrict__ qpts, const int2* __restrict__ qgroups, int64_t n_groups,
+    const TNode<T, D>* __restrict__ tnode,
     const SPt<T, D>* __restrict__ tpts, int64_t n_tnodes, T r2, T inv_r, int exclude_self,
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ dstatus) {
@@ -43,10 +45,11 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     __shared__ int2 stack[kEdgeWarps][SD];
     __shared__ SPt<T, D> tgt[kEdgeWarps][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t qbase = ((int64_t)blockIdx.x * kEdgeWarps + w) * 32;
-    if (qbase >= nq) return;  // warp-uniform
-    const bool valid = qbase + lane < nq;
-    const SPt<T, D> q = qpts[valid ? qbase + lane : qbase];
+    const int64_t g = (int64_t)blockIdx.x * kEdgeWarps + w;
+    if (g >= n_groups) return;  // warp-uniform
+    const int2 grp = qgroups[g];
+    const bool valid = lane < grp.y;
+    const SPt<T, D> q = qpts[grp.x + (valid ? lane : 0)];
     T qlo[D], qhi[D];
 #pragma unroll
     for (int d = 0; d < D; ++d) {
@@ -204,9 +207,8 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
         if ((err = cudaMemsetAsync(ctx.counts.p, 0, (size_t)nq * 4, s))) return cuda_status(ctx, err, "zero counts");
     } else {
         PhaseTimer pt_(ctx, PH_COUNT);
-        const int64_t groups = (nq + 31) / 32;
-        k_edges<T, D, false><<<div_up(groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
-            q.spts.as<SPt<T, D>>(), nq, t.tnode.as<TNode<T, D>>(), t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0),
+        k_edges<T, D, false><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
+            q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0),
             exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
         ctx.kernel_launches += 1;
     }
@@ -230,10 +232,9 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
     const T r = (T)t.radius;
     const T r2 = r * r;
     const T inv_r = T(1) / r;  // inv(r), src/cpu/edges_cpu.jl:185
-    const int64_t groups = (nq + 31) / 32;
     PhaseTimer pt_(ctx, PH_FILL);
-    k_edges<T, D, true><<<div_up(groups, kEdgeWarps), kEdgeThreads, 0, ctx.stream>>>(
-        q.spts.as<SPt<T, D>>(), nq, t.tnode.as<TNode<T, D>>(), t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r,
+    k_edges<T, D, true><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, ctx.stream>>>(
+        q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r,
         exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(), senders, receivers, (T*)rel_disp, (T*)rel_dist,
         ctx.dstatus.as<int>());
     ctx.kernel_launches += 1;

@@ -25,7 +25,7 @@ struct Ctx;
 // Phases timed by the optional CUDA-event profiler (oct_profile_*).
 enum Phase : int {
     PH_BOUNDS = 0, PH_ENCODE, PH_SORT, PH_GATHER, PH_TOPOLOGY, PH_REFIT,
-    PH_COUNT, PH_SCAN, PH_FILL, PH_ADJOINT, PH_NUM
+    PH_COUNT, PH_SCAN, PH_FILL, PH_ADJOINT, PH_GROUPS, PH_NUM
 };
 
 struct ProfRecord {
@@ -81,6 +81,11 @@ struct Tree {
     DevBuf partials;             // double per-block bounds partials
     DevBuf hdr;                  // OctHeader
     DevBuf morton;               // uint64 per original point (refit mode)
+    DevBuf groups;               // int2 {first position, count <= 32}: query groups
+    DevBuf gcnt;                 // int32 per node: groups formed under it
+    DevBuf goff;                 // int64 exclusive scan of gcnt (+1)
+    int64_t n_groups = 0;
+    int64_t group_capacity = 0;
     OctHeader* hdr_host = nullptr;  // pinned
 
     // Lazily materialized reference-layout views (DeviceView contract,
