@@ -365,14 +365,24 @@ def _pair_index(tns: TNS, q: int, t: int) -> int:
 
 
 def _resize_buffer(buf: EdgeBuffer, T, ndims, n_edges, device):
+    """Size the buffer's arrays to n_edges.  The arrays are views of grow-only
+    backing storage (1.25x slack), so a time-stepping loop whose edge count
+    fluctuates does not reallocate every step; like the reference, the arrays
+    are replaced whenever the edge count changes."""
     dev = f"cuda:{device}"
-    if buf.senders.numel() != n_edges:
-        buf.senders = torch.empty(n_edges, dtype=torch.int32, device=dev)
-        buf.receivers = torch.empty(n_edges, dtype=torch.int32, device=dev)
-    if buf.rel_displacement.shape[1] != n_edges:
-        buf.rel_displacement = torch.empty((n_edges, ndims), dtype=T, device=dev).t()
-    if buf.rel_dist_norm.shape[1] != n_edges:
-        buf.rel_dist_norm = torch.empty((n_edges, 1), dtype=T, device=dev).t()
+    cap = getattr(buf, "_capacity", -1)
+    if n_edges > cap:
+        cap = n_edges + n_edges // 4
+        buf._capacity = cap
+        buf._snd = torch.empty(cap, dtype=torch.int32, device=dev)
+        buf._rcv = torch.empty(cap, dtype=torch.int32, device=dev)
+        buf._disp = torch.empty((cap, ndims), dtype=T, device=dev)
+        buf._dist = torch.empty((cap, 1), dtype=T, device=dev)
+    if buf.senders.numel() != n_edges or buf.senders.data_ptr() != buf._snd.data_ptr():
+        buf.senders = buf._snd[:n_edges]
+        buf.receivers = buf._rcv[:n_edges]
+        buf.rel_displacement = buf._disp[:n_edges].t()
+        buf.rel_dist_norm = buf._dist[:n_edges].t()
     buf.n_edges = n_edges
 
 

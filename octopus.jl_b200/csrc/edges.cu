@@ -31,6 +31,7 @@ namespace oct {
 
 constexpr int kEdgeWarps = 8;
 constexpr int kEdgeThreads = kEdgeWarps * 32;
+constexpr int kStage = 16;  // staged hits per lane, and points per leaf sub-chunk
 
 template <class T, int D, bool FILL>
 __global__ void __launch_bounds__(kEdgeThreads) k_edges(
@@ -44,6 +45,9 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     // ascending-order subtrees (see below).
     __shared__ int2 stack[kEdgeWarps][SD];
     __shared__ SPt<T, D> tgt[kEdgeWarps][32];
+    // Fill pass: each lane stages the sorted positions of its next hits; a
+    // flush writes them as runs of consecutive edges of one query segment.
+    __shared__ int32_t obuf[FILL ? kEdgeWarps : 1][32][FILL ? kStage + 1 : 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t g = (int64_t)blockIdx.x * kEdgeWarps + w;
     if (g >= n_groups) return;  // warp-uniform
@@ -63,6 +67,44 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
         cur_end = offsets[q.idx + 1];
     }
     const bool self_pair = exclude_self != 0;
+    int ocnt = 0;
+
+    // Two queries per round: lanes 0-15 write query 2r's staged edges, lanes
+    // 16-31 query 2r+1's, each lane one edge.
+    auto flush = [&]() {
+        __syncwarp();
+        const int half = lane >> 4, e = lane & 15;
+        const unsigned busy = __ballot_sync(0xffffffffu, ocnt > 0);
+        for (int base = 0; base < 32; base += 2) {
+            if (!((busy >> base) & 3u)) continue;
+            const int ql = base + half;
+            const int nql = __shfl_sync(0xffffffffu, ocnt, ql);
+            const long long cq = __shfl_sync(0xffffffffu, (long long)cur, ql);
+            const long long ce = __shfl_sync(0xffffffffu, (long long)cur_end, ql);
+            const int32_t qi = __shfl_sync(0xffffffffu, q.idx, ql);
+            T px[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) px[d] = __shfl_sync(0xffffffffu, q.x[d], ql);
+            if (e < nql) {
+                const int64_t k = cq + e;
+                if (k < ce) {
+                    const SPt<T, D> t = tpts[obuf[w][ql][e]];
+                    T diff[D];
+                    const T d2 = dist2<T, D>(t.x, px, diff);
+                    senders[k] = t.idx + 1;
+                    receivers[k] = qi + 1;
+#pragma unroll
+                    for (int d = 0; d < D; ++d) rdisp[(int64_t)D * k + d] = mul_rn(-diff[d], inv_r);
+                    rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
+                } else {
+                    atomicOr(dstatus, 1);  // never taken when count and fill agree
+                }
+            }
+        }
+        cur += ocnt;
+        ocnt = 0;
+        __syncwarp();
+    };
 
     int sp = 0;
     if (n_tnodes > 0) {
@@ -79,9 +121,13 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
         const int32_t na = ent.x & 0x7fffffff;
         const int32_t nb = ent.y;
         if (nb > 0) {
-            // Leaf: every (query, point) pair, points in ascending position.
-            for (int32_t c0 = 0; c0 < nb; c0 += 32) {
-                const int m = min(32, nb - c0);
+            // Leaf: every (query, point) pair, points in ascending position,
+            // in sub-chunks of at most kStage points.
+            for (int32_t c0 = 0; c0 < nb; c0 += kStage) {
+                const int m = min(kStage, nb - c0);
+                if (FILL && __any_sync(0xffffffffu, ocnt + m > kStage)) {
+                    flush();
+                }
                 __syncwarp();
                 if (lane < m) tgt[w][lane] = tpts[na + c0 + lane];
                 __syncwarp();
@@ -91,18 +137,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                     const T d2 = dist2<T, D>(t.x, q.x, diff);
                     const bool hit = valid && d2 <= r2;
                     if (FILL) {
-                        if (hit && !(self_pair && t.idx == q.idx)) {
-                            if (cur >= cur_end) {  // never taken when count and fill agree
-                                atomicOr(dstatus, 1);
-                                continue;
-                            }
-                            senders[cur] = t.idx + 1;
-                            receivers[cur] = q.idx + 1;
-#pragma unroll
-                            for (int d = 0; d < D; ++d) rdisp[(int64_t)D * cur + d] = mul_rn(-diff[d], inv_r);
-                            rdist[cur] = mul_rn(sqrt_rn(d2), inv_r);
-                            ++cur;
-                        }
+                        if (hit && !(self_pair && t.idx == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j;
                     } else {
                         cnt += hit ? 1 : 0;
                     }
@@ -133,6 +168,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             __syncwarp();
         }
     }
+    if (FILL) flush();
     if (!FILL && valid) counts[q.idx] = (int32_t)(cnt - (self_pair ? 1 : 0));
 }
 
