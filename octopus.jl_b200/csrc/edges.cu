@@ -29,9 +29,9 @@
 
 namespace oct {
 
-constexpr int kEdgeWarps = 8;
+constexpr int kEdgeWarps = 4;
 constexpr int kEdgeThreads = kEdgeWarps * 32;
-constexpr int kStage = 16;  // staged hits per lane, and points per leaf sub-chunk
+constexpr int kStage = 32;  // staged hits per lane, and points per leaf sub-chunk
 
 template <class T, int D, bool FILL>
 __global__ void __launch_bounds__(kEdgeThreads) k_edges(
@@ -69,15 +69,14 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     const bool self_pair = exclude_self != 0;
     int ocnt = 0;
 
-    // Two queries per round: lanes 0-15 write query 2r's staged edges, lanes
-    // 16-31 query 2r+1's, each lane one edge.
+    // One query per round: lane e writes the query's e-th staged edge, so a
+    // round stores a run of consecutive edges of one segment.
     auto flush = [&]() {
         __syncwarp();
-        const int half = lane >> 4, e = lane & 15;
-        const unsigned busy = __ballot_sync(0xffffffffu, ocnt > 0);
-        for (int base = 0; base < 32; base += 2) {
-            if (!((busy >> base) & 3u)) continue;
-            const int ql = base + half;
+        unsigned busy = __ballot_sync(0xffffffffu, ocnt > 0);
+        while (busy) {
+            const int ql = __ffs(busy) - 1;
+            busy &= busy - 1;
             const int nql = __shfl_sync(0xffffffffu, ocnt, ql);
             const long long cq = __shfl_sync(0xffffffffu, (long long)cur, ql);
             const long long ce = __shfl_sync(0xffffffffu, (long long)cur_end, ql);
@@ -85,10 +84,10 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             T px[D];
 #pragma unroll
             for (int d = 0; d < D; ++d) px[d] = __shfl_sync(0xffffffffu, q.x[d], ql);
-            if (e < nql) {
-                const int64_t k = cq + e;
+            if (lane < nql) {
+                const int64_t k = cq + lane;
                 if (k < ce) {
-                    const SPt<T, D> t = tpts[obuf[w][ql][e]];
+                    const SPt<T, D> t = tpts[obuf[w][ql][lane]];
                     T diff[D];
                     const T d2 = dist2<T, D>(t.x, px, diff);
                     senders[k] = t.idx + 1;
@@ -264,7 +263,6 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
 template <class T, int D>
 int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* senders, int32_t* receivers,
                void* rel_disp, void* rel_dist) {
-    const int64_t nq = q.n;
     const T r = (T)t.radius;
     const T r2 = r * r;
     const T inv_r = T(1) / r;  // inv(r), src/cpu/edges_cpu.jl:185
