@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
                                                          const int32_t* __restrict__ first_child_in,
                                                          TNode<T, D>* __restrict__ tnode, int2* __restrict__ nrange,
                                                          int32_t* __restrict__ parent, int32_t* __restrict__ arrive,
-                                                         const OctHeader* hdr) {
+                                                         int32_t* __restrict__ chain, const OctHeader* hdr) {
     constexpr int BITS = Dims<D>::bits;
     constexpr int NCH = Dims<D>::nch;
     const int64_t nn = hdr->n_nodes;
@@ -339,6 +339,10 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
         // A node covering every point has the global bounds.
 #pragma unroll
         for (int d = 0; d < D; ++d) { nd.lo[d] = (T)hdr->gmin[d]; nd.hi[d] = (T)hdr->gmax[d]; }
+        // Full-range nodes form the root's chain: chain[L] = id, and
+        // chain[32 + L] = 1 when the node's only child sits in slot 0.
+        chain[L] = (int32_t)id;
+        chain[32 + L] = (nd.b == -1) ? 1 : 0;
     } else {
 #pragma unroll
         for (int d = 0; d < D; ++d) { nd.lo[d] = T(0); nd.hi[d] = T(0); }
@@ -412,9 +416,18 @@ __global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n,
 template <class T, int D, int PASS>
 __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restrict__ tnode, int64_t capacity,
                                                      int32_t* __restrict__ gcnt, const int64_t* __restrict__ goff,
-                                                     int2* __restrict__ groups, const OctHeader* hdr) {
+                                                     int2* __restrict__ groups, const int32_t* __restrict__ chain,
+                                                     OctHeader* hdr) {
     const int64_t nn = hdr->n_nodes;
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (!PASS && id == 0 && nn <= capacity) {
+        // The DFS may start at the first chain node that is not an internal
+        // node with a single child in slot 0: every node above it covers all
+        // points (its box holds every query) and keeps descending order.
+        int L = 0;
+        while (L < 32 && chain[32 + L] == 1) ++L;
+        hdr->dfs_start = chain[L];
+    }
     if (nn > capacity || id >= capacity) return;
     if (id >= nn) {
         if (!PASS) gcnt[id] = 0;  // the scan runs over the whole capacity
@@ -554,8 +567,9 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
             (err = ensure(t.fchild, (size_t)cap * 4)) || (err = ensure(t.gcnt, (size_t)cap * 4)) ||
             (err = ensure(t.goff, (size_t)(cap + 1) * 8)) ||
             (err = ensure(t.scan_tmp, (size_t)std::max(scan_tmp_elems(nbc), scan_tmp_elems(cap)) * 8)) ||
-            (err = ensure(t.groups, (size_t)(cap + n / 32 + 2) * 8)))
+            (err = ensure(t.groups, (size_t)(cap + n / 32 + 2) * 8)) || (err = ensure(t.chain, 64 * 4)))
             return cuda_status(ctx, err, "allocating node arrays");
+        if ((err = cudaMemsetAsync(t.chain.p, 0xff, 64 * 4, s))) return cuda_status(ctx, err, "chain reset");
         {
         PhaseTimer pt_(ctx, PH_TOPOLOGY);
         k_mark<D, K><<<nblocks, kThreads, 0, s>>>(skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(), nblocks);
@@ -565,7 +579,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
                                                     t.fchild.as<int32_t>(), t.nrange.as<int2>(), hdr);
         k_emit_nodes<T, D, K><<<div_up(cap, kThreads), kThreads, 0, s>>>(
             skeys, n, cap, t.fchild.as<int32_t>(), t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
-            t.parent.as<int32_t>(), t.arrive.as<int32_t>(), hdr);
+            t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.chain.as<int32_t>(), hdr);
         ctx.kernel_launches += 6;
         }
         {
@@ -578,12 +592,13 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
         {
             PhaseTimer pt_(ctx, PH_GROUPS);
             k_groups<T, D, 0><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
-                                                                        t.gcnt.as<int32_t>(), nullptr, nullptr, hdr);
+                                                                        t.gcnt.as<int32_t>(), nullptr, nullptr,
+                                                                        t.chain.as<int32_t>(), hdr);
             exclusive_scan_i32_i64(t.gcnt.as<int32_t>(), t.goff.as<int64_t>(), cap, &hdr->n_groups,
                                    t.scan_tmp.as<int64_t>(), s);
             k_groups<T, D, 1><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
                                                                         t.gcnt.as<int32_t>(), t.goff.as<int64_t>(),
-                                                                        t.groups.as<int2>(), hdr);
+                                                                        t.groups.as<int2>(), t.chain.as<int32_t>(), hdr);
             ctx.kernel_launches += 5;
         }
         if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
@@ -597,6 +612,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
         }
         t.n_nodes = t.hdr_host->n_nodes;
         t.n_groups = t.hdr_host->n_groups;
+        t.dfs_start = t.hdr_host->dfs_start;
         return OK;
     }
     return set_error(ctx, ERR_OVERFLOW, "tree build: node capacity retry did not converge");

@@ -97,7 +97,7 @@ struct DeviceGuard {
 void release_tree(oct::Tree& t) {
     using oct::release;
     for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.sort_tmp, &t.spts, &t.tnode, &t.nrange,
-                    &t.parent, &t.fchild, &t.arrive, &t.groups, &t.gcnt, &t.goff, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
+                    &t.parent, &t.fchild, &t.arrive, &t.groups, &t.gcnt, &t.goff, &t.chain, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
                     &t.morton, &t.v_first, &t.v_last, &t.v_children, &t.v_bmin, &t.v_bmax, &t.v_perm})
         release(*b);
     if (t.hdr_host) cudaFreeHost(t.hdr_host);

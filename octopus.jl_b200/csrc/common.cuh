@@ -67,7 +67,32 @@ struct OctHeader {
     int32_t n_blocks_done;
     int32_t pad;
     int64_t n_groups;
+    int32_t dfs_start;  // first node of the DFS below the root's single-child chain
+    int32_t pad2;
 };
+
+// Packed pairs of floats with per-element IEEE round-to-nearest (sm_100+).
+// Each element is rounded exactly as the scalar __f*_rn operation.
+__device__ __forceinline__ unsigned long long sub2_rn(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long mul2_rn(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long add2_rn(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    return ((unsigned long long)__float_as_uint(hi) << 32) | __float_as_uint(lo);
+}
+__device__ __forceinline__ float lo2(unsigned long long v) { return __uint_as_float((unsigned)v); }
+__device__ __forceinline__ float hi2(unsigned long long v) { return __uint_as_float((unsigned)(v >> 32)); }
 
 // --------------------------------------------------- Julia float semantics --
 // Base.min/max on IEEE floats for non-NaN operands: -0.0 orders below +0.0.

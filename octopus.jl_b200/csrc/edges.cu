@@ -23,6 +23,7 @@
 //   * counts -> int64 exclusive scan -> fill at the per-query cursor.
 
 #include <algorithm>
+#include <type_traits>
 
 #include "internal.h"
 #include "scan.cuh"
@@ -36,7 +37,7 @@ constexpr int kStage = 32;  // staged hits per lane, and points per leaf sub-chu
 template <class T, int D, bool FILL>
 __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     const SPt<T, D>* __restrict__ qpts, const int2* __restrict__ qgroups, int64_t n_groups,
-    const TNode<T, D>* __restrict__ tnode,
+    const TNode<T, D>* __restrict__ tnode, int32_t start_node,
     const SPt<T, D>* __restrict__ tpts, int64_t n_tnodes, T r2, T inv_r, int exclude_self,
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ dstatus) {
@@ -44,7 +45,9 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     // Stack entries are the pushed node's (a, b) record; bit 31 of a marks
     // ascending-order subtrees (see below).
     __shared__ int2 stack[kEdgeWarps][SD];
-    __shared__ SPt<T, D> tgt[kEdgeWarps][32];
+    // The current leaf chunk, structure of arrays so pairs load as 8 bytes.
+    __shared__ __align__(16) T sx[kEdgeWarps][D][32];
+    __shared__ int32_t sid[kEdgeWarps][32];
     // Fill pass: each lane stages the sorted positions of its next hits; a
     // flush writes them as runs of consecutive edges of one query segment.
     __shared__ int32_t obuf[FILL ? kEdgeWarps : 1][32][FILL ? kStage + 1 : 1];
@@ -107,7 +110,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
 
     int sp = 0;
     if (n_tnodes > 0) {
-        const TNode<T, D> root = tnode[0];
+        const TNode<T, D> root = tnode[start_node];
         if (box_gap2<T, D>(qlo, qhi, root.lo, root.hi) <= r2) {
             if (lane == 0) stack[w][0] = make_int2(root.a, root.b);
             sp = 1;
@@ -124,21 +127,58 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             // in sub-chunks of at most kStage points.
             for (int32_t c0 = 0; c0 < nb; c0 += kStage) {
                 const int m = min(kStage, nb - c0);
+                const int mp = (m + 1) & ~1;  // padded to whole pairs with +inf points
                 if (FILL && __any_sync(0xffffffffu, ocnt + m > kStage)) {
                     flush();
                 }
                 __syncwarp();
-                if (lane < m) tgt[w][lane] = tpts[na + c0 + lane];
+                if (lane < m) {
+                    const SPt<T, D> t = tpts[na + c0 + lane];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) sx[w][d][lane] = t.x[d];
+                    sid[w][lane] = t.idx;
+                } else if (lane < mp) {
+#pragma unroll
+                    for (int d = 0; d < D; ++d) sx[w][d][lane] = T(INFINITY);
+                    sid[w][lane] = -1;
+                }
                 __syncwarp();
-                for (int j = 0; j < m; ++j) {
-                    const SPt<T, D> t = tgt[w][j];
-                    T diff[D];
-                    const T d2 = dist2<T, D>(t.x, q.x, diff);
-                    const bool hit = valid && d2 <= r2;
-                    if (FILL) {
-                        if (hit && !(self_pair && t.idx == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j;
-                    } else {
-                        cnt += hit ? 1 : 0;
+                if constexpr (std::is_same<T, float>::value) {
+                    unsigned long long P[D];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) P[d] = pack2(q.x[d], q.x[d]);
+                    for (int j = 0; j < mp; j += 2) {
+                        // Two targets at once: ((dx*dx + dy*dy) + dz*dz), each
+                        // element rounded as the scalar path.
+                        unsigned long long S = 0;
+#pragma unroll
+                        for (int d = 0; d < D; ++d) {
+                            const unsigned long long dd =
+                                sub2_rn(*reinterpret_cast<const unsigned long long*>(&sx[w][d][j]), P[d]);
+                            const unsigned long long sq = mul2_rn(dd, dd);
+                            S = (d == 0) ? sq : add2_rn(S, sq);
+                        }
+                        const bool h0 = valid && lo2(S) <= r2;
+                        const bool h1 = valid && hi2(S) <= r2;
+                        if (FILL) {
+                            if (h0 && !(self_pair && sid[w][j] == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j;
+                            if (h1 && !(self_pair && sid[w][j + 1] == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j + 1;
+                        } else {
+                            cnt += (h0 ? 1 : 0) + (h1 ? 1 : 0);
+                        }
+                    }
+                } else {
+                    for (int j = 0; j < m; ++j) {
+                        T t[D], diff[D];
+#pragma unroll
+                        for (int d = 0; d < D; ++d) t[d] = sx[w][d][j];
+                        const T d2 = dist2<T, D>(t, q.x, diff);
+                        const bool hit = valid && d2 <= r2;
+                        if (FILL) {
+                            if (hit && !(self_pair && sid[w][j] == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j;
+                        } else {
+                            cnt += hit ? 1 : 0;
+                        }
                     }
                 }
             }
@@ -243,7 +283,7 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
     } else {
         PhaseTimer pt_(ctx, PH_COUNT);
         k_edges<T, D, false><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
-            q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0),
+            q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start, t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0),
             exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
         ctx.kernel_launches += 1;
     }
@@ -268,7 +308,7 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
     const T inv_r = T(1) / r;  // inv(r), src/cpu/edges_cpu.jl:185
     PhaseTimer pt_(ctx, PH_FILL);
     k_edges<T, D, true><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, ctx.stream>>>(
-        q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r,
+        q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start, t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r,
         exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(), senders, receivers, (T*)rel_disp, (T*)rel_dist,
         ctx.dstatus.as<int>());
     ctx.kernel_launches += 1;

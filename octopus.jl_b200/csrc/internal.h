@@ -85,6 +85,8 @@ struct Tree {
     DevBuf gcnt;                 // int32 per node: groups formed under it
     DevBuf goff;                 // int64 exclusive scan of gcnt (+1)
     int64_t n_groups = 0;
+    int32_t dfs_start = 0;
+    DevBuf chain;                // int32[64]: full-range chain node ids and flags
     int64_t group_capacity = 0;
     OctHeader* hdr_host = nullptr;  // pinned
 
