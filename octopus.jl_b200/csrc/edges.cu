@@ -148,18 +148,19 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
 #pragma unroll
                     for (int d = 0; d < D; ++d) P[d] = pack2(q.x[d], q.x[d]);
                     for (int j = 0; j < mp; j += 2) {
-                        // Two targets at once: ((dx*dx + dy*dy) + dz*dz), each
-                        // element rounded as the scalar path.
-                        unsigned long long S = 0;
+                        // Two targets at once: packed differences and squares,
+                        // scalar sums ((dx*dx + dy*dy) + dz*dz) per element.
+                        float s0 = 0.f, s1 = 0.f;
 #pragma unroll
                         for (int d = 0; d < D; ++d) {
                             const unsigned long long dd =
                                 sub2_rn(*reinterpret_cast<const unsigned long long*>(&sx[w][d][j]), P[d]);
                             const unsigned long long sq = mul2_rn(dd, dd);
-                            S = (d == 0) ? sq : add2_rn(S, sq);
+                            s0 = (d == 0) ? lo2(sq) : __fadd_rn(s0, lo2(sq));
+                            s1 = (d == 0) ? hi2(sq) : __fadd_rn(s1, hi2(sq));
                         }
-                        const bool h0 = valid && lo2(S) <= r2;
-                        const bool h1 = valid && hi2(S) <= r2;
+                        const bool h0 = valid && s0 <= r2;
+                        const bool h1 = valid && s1 <= r2;
                         if (FILL) {
                             if (h0 && !(self_pair && sid[w][j] == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j;
                             if (h1 && !(self_pair && sid[w][j + 1] == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j + 1;

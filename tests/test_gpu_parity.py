@@ -78,11 +78,30 @@ def assert_tree_equal(tree, ot):
     assert np.array_equal(a["perm"].cpu().numpy(), ot.perm)
 
 
+def describe_mismatch(e, oe):
+    """Where the GPU COO first departs from the oracle's, for the failure message."""
+    gs, gr = e.senders.cpu().numpy(), e.receivers.cpu().numpy()
+    os_, or_ = oe["senders"], oe["receivers"]
+    msg = [f"n_edges gpu={len(gs)} oracle={len(os_)}"]
+    m = min(len(gs), len(os_))
+    bad = np.nonzero((gs[:m] != os_[:m]) | (gr[:m] != or_[:m]))[0]
+    if len(bad):
+        k = int(bad[0])
+        i = int(or_[k])
+        off = oe["offsets"]
+        seg_o = os_[off[i - 1]:off[i]]
+        seg_g = gs[gr == i]
+        msg.append(f"first diff at edge {k}: receiver gpu={gr[k]} oracle={i}; diffs={len(bad)}")
+        msg.append(f"receiver {i}: same set={sorted(seg_g.tolist()) == sorted(seg_o.tolist())} "
+                   f"gpu={seg_g.tolist()[:40]} oracle={seg_o.tolist()[:40]}")
+    return "; ".join(msg)
+
+
 def assert_edges_equal(e, oe, tns=None):
     if tns is not None:
         import octopus_b200
         octopus_b200.synchronize(tns)
-    assert np.array_equal(e.senders.cpu().numpy(), oe["senders"])
+    assert np.array_equal(e.senders.cpu().numpy(), oe["senders"]), describe_mismatch(e, oe)
     assert np.array_equal(e.receivers.cpu().numpy(), oe["receivers"])
     assert np.array_equal(e.rel_displacement.t().cpu().numpy(), oe["rel_displacement"])
     assert np.array_equal(e.rel_dist_norm.reshape(-1).cpu().numpy(), oe["rel_dist_norm"])
@@ -108,8 +127,9 @@ def test_config1_full_size(ob, oracle_mod):
     tns, sid = gpu_run(ob, x, r)
     e = ob.build_edges(tns, sid, sid)
     ot = oracle_mod.build_tree(x, r)
+    assert_tree_equal(tns.trees[sid - 1], ot)
     oe = oracle_mod.build_edges(ot, x, exclude_self=True)
-    assert_edges_equal(e, oe)
+    assert_edges_equal(e, oe, tns)
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
