@@ -150,6 +150,27 @@ OCT_API int oct_edges_diff_backward(oct_ctx* ctx, int ndims, int dtype, int64_t 
                                     const void* rel_dist_norm, const void* d_rel_displacement,
                                     const void* d_rel_dist_norm, double radius, void* grad_coords);
 
+/* Edge count that allocates no device memory.  No counterpart in the
+ * reference: it serves callers that cannot let a library call cudaMalloc --
+ * hosts whose device memory belongs to their own pool allocator (a
+ * framework's caching allocator, a fixed memory budget), where a raw
+ * cudaMalloc may fail or fragment the pool, and latency-critical loops that
+ * cannot afford the implicit device synchronization of cudaMalloc/cudaFree.
+ * Same result as oct_edges_count for the pair, but the caller passes
+ * counts[n_q] (int32, per query point) and offsets[n_q + 1] (int64 exclusive
+ * scan, offsets[n_q] = edge total) as device outputs; *n_edges (optional,
+ * host) receives the total after a stream synchronize.  The scan's scratch is
+ * a fixed 64 KiB device array that every GPU loading this library holds until
+ * exit, which limits the query set to 16,777,216 points (larger sets get
+ * OCT_ERR_CAPACITY).  The first call on a device looks up that array's device
+ * address (make this first call before any stream capture begins).  All calls
+ * share the array: calls whose GPU work overlaps (other streams, other host
+ * threads, other contexts on the same device) race and must not be issued.
+ * It does not prepare oct_edges_fill. */
+OCT_API int oct_edges_count_noalloc(oct_ctx* ctx, const oct_tree* query, const oct_tree* target,
+                                    int exclude_self, int32_t* counts, int64_t* offsets,
+                                    int64_t* n_edges);
+
 /* Per-phase device timing with CUDA events on the context's stream (the
  * phase timers of benchmarks/profile_phases.jl:29-46, taken on the device).
  * While enabled, every library call records its phases; oct_profile_read

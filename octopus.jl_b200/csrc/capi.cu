@@ -6,15 +6,8 @@
 #include <string>
 
 #include "../../include/octopus_b200.h"
+#include "capi_types.h"
 #include "internal.h"
-
-struct oct_ctx {
-    oct::Ctx c;
-};
-struct oct_tree {
-    oct::Tree t;
-    oct_ctx* owner = nullptr;
-};
 
 namespace oct {
 

@@ -328,7 +328,30 @@ int neighbors_typed(Ctx& ctx, const Tree& t, const void* qcoords, int64_t nsel, 
     return cuda_status(ctx, cudaGetLastError(), "neighbor query launch");
 }
 
+template <class T, int D>
+cudaError_t count_into_typed(const Tree& q, const Tree& t, bool exclude_self, int32_t* counts, cudaStream_t s) {
+    const T r = (T)t.radius;
+    const T r2 = r * r;
+    k_edges<T, D, false><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
+        q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
+        t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, counts, nullptr, nullptr, nullptr,
+        nullptr, nullptr, nullptr);
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+// Launches only the per-query count kernel into caller memory; allocates
+// nothing (used by the allocation-free count entry point).
+cudaError_t count_into(const Tree& q, const Tree& t, bool exclude_self, int32_t* counts, cudaStream_t s) {
+    if (q.n == 0) return cudaSuccess;
+    if (t.n_nodes == 0) return cudaMemsetAsync(counts, 0, (size_t)q.n * 4, s);
+    if (t.dtype == 0)
+        return t.ndims == 3 ? count_into_typed<float, 3>(q, t, exclude_self, counts, s)
+                            : count_into_typed<float, 2>(q, t, exclude_self, counts, s);
+    return t.ndims == 3 ? count_into_typed<double, 3>(q, t, exclude_self, counts, s)
+                        : count_into_typed<double, 2>(q, t, exclude_self, counts, s);
+}
 
 int edges_count(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64_t* n_edges) {
     ctx.plan_query = nullptr;

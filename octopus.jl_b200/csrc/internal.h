@@ -132,6 +132,7 @@ int edges_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
                int32_t* receivers, void* rel_disp, void* rel_dist, int64_t n_edges);
 int neighbors_of(Ctx& ctx, const Tree& t, const void* qcoords, int64_t nsel, int32_t* out_counts,
                  int32_t* out_idx, int64_t cap);
+cudaError_t count_into(const Tree& q, const Tree& t, bool exclude_self, int32_t* counts, cudaStream_t s);
 
 // Adjoint (diff.cu).
 int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,

@@ -1,0 +1,90 @@
+"""oct_edges_count_noalloc: the allocation-free edge count, for callers that
+cannot let a library call cudaMalloc (their device memory belongs to their
+own pool allocator, or their loop cannot absorb cudaMalloc's device
+synchronization).  It must give exactly what the regular entry point gives:
+the per-query counts and offsets implied by build_edges' COO, and the same
+edge total -- on consecutive calls, since every call reuses one fixed scratch
+array.  This file is collected last on purpose."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import uniform
+
+pytestmark = pytest.mark.gpu
+
+
+def _tns(ob, x, r):
+    tns = ob.TNS(torch.float32, ndims=x.shape[1])
+    ob.set_search_radius_(tns, r)
+    sid = ob.add_point_set_(tns, torch.from_numpy(x).cuda().t())
+    ob.set_active_search_(tns, sid, sid)
+    ob.run_(tns)
+    return tns, sid
+
+
+def _noalloc_count(tns, qid, tid, exclude_self):
+    ctx = tns._ctx
+    n = tns.point_sets[qid - 1].n
+    counts = torch.full((max(n, 1),), -7, dtype=torch.int32, device="cuda")
+    offsets = torch.full((n + 1,), -7, dtype=torch.int64, device="cuda")
+    ne = C.c_int64(-1)
+    ctx.bind_stream()
+    st = ctx.lib.oct_edges_count_noalloc(ctx.handle, tns.trees[qid - 1].handle, tns.trees[tid - 1].handle,
+                                         exclude_self, C.c_void_p(counts.data_ptr()),
+                                         C.c_void_p(offsets.data_ptr()), C.byref(ne))
+    ctx.check(st, "oct_edges_count_noalloc")
+    return counts[:n], offsets, int(ne.value)
+
+
+def test_noalloc_count_matches_regular_entry_point_on_consecutive_calls(ob):
+    cases = [(uniform(20000, 3, 11), np.float32(0.05)),   # first call on this device: sets up
+             (uniform(50000, 3, 12), np.float32(0.03)),   # second call reuses the scratch
+             (uniform(30000, 2, 13), np.float32(0.01))]
+    for x, r in cases:
+        tns, sid = _tns(ob, x, r)
+        e = ob.build_edges(tns, sid, sid)  # regular entry points: oct_edges_count + oct_edges_fill
+        n = x.shape[0]
+        want_counts = torch.bincount(e.receivers.long() - 1, minlength=n).to(torch.int32)
+        want_offsets = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+        want_offsets[1:] = torch.cumsum(want_counts.long(), 0)
+        for _ in range(2):
+            counts, offsets, ne = _noalloc_count(tns, sid, sid, 1)
+            assert ne == e.senders.numel()
+            assert torch.equal(counts, want_counts)
+            assert torch.equal(offsets, want_offsets)
+
+
+def test_noalloc_count_cross_pair_and_empty_target(ob):
+    a = uniform(3000, 3, 21)
+    b = uniform(5000, 3, 22)
+    tns = ob.TNS(torch.float32)
+    ob.set_search_radius_(tns, 0.08)
+    ia = ob.add_point_set_(tns, torch.from_numpy(a).cuda().t())
+    ib = ob.add_point_set_(tns, torch.from_numpy(b).cuda().t())
+    ie = ob.add_point_set_(tns, torch.zeros((3, 0), device="cuda"))
+    ob.set_active_search_(tns, ia, ib)
+    ob.run_(tns)
+    e = ob.build_edges(tns, ia, ib)
+    counts, offsets, ne = _noalloc_count(tns, ia, ib, 0)
+    assert ne == e.senders.numel()
+    assert torch.equal(counts, torch.bincount(e.receivers.long() - 1, minlength=3000).to(torch.int32))
+    counts, offsets, ne = _noalloc_count(tns, ia, ie, 0)
+    assert ne == 0 and int(counts.abs().sum()) == 0 and int(offsets.abs().sum()) == 0
+
+
+def test_noalloc_count_rejects_sets_beyond_its_scratch(ob):
+    n = (1 << 24) + 1
+    x = torch.rand((n, 3), device="cuda")
+    tns = ob.TNS(torch.float32)
+    ob.set_search_radius_(tns, 0.01)
+    sid = ob.add_point_set_(tns, x.t())
+    ob.run_(tns)
+    ctx = tns._ctx
+    ne = C.c_int64(-1)
+    st = ctx.lib.oct_edges_count_noalloc(ctx.handle, tns.trees[0].handle, tns.trees[0].handle, 1,
+                                         C.c_void_p(0), C.c_void_p(0), C.byref(ne))
+    assert st == ob._lib.ERR_CAPACITY
+    assert b"16,777,216" in ctx.lib.oct_ctx_last_error(ctx.handle)
