@@ -101,6 +101,23 @@ OCT_API int oct_tree_destroy(oct_tree* tree);
 OCT_API int oct_tree_build(oct_ctx* ctx, oct_tree* tree, const void* coords, int64_t n,
                            double radius, int keep_morton);
 
+/* Batched run! for many independent point sets ("clouds") in one pass; no
+ * counterpart in the reference, which builds one TNS per radius
+ * (src/api.jl:24-29): cloud c is the points [cloud_offsets[c],
+ * cloud_offsets[c+1]) of `coords` (host array, n_clouds + 1 entries) with
+ * search radius radii[c] (host array).  Each cloud gets exactly the tree a
+ * TNS of that cloud alone builds; the clouds share one forest, one sort and
+ * one set of launches.  Searched with oct_edges_count / oct_edges_fill
+ * (query == target, exclude_self = 1): the COO concatenates the clouds in
+ * order, each cloud's edges exactly as a standalone build_edges, with
+ * 1-based indices local to the cloud. */
+OCT_API int oct_tree_build_batch(oct_ctx* ctx, oct_tree* tree, const void* coords, int64_t n,
+                                 const int64_t* cloud_offsets, const double* radii, int32_t n_clouds);
+
+/* After oct_edges_count on a batched tree: edge_offsets (host, n_clouds + 1)
+ * receives where each cloud's edges start in the concatenated COO. */
+OCT_API int oct_batch_edge_offsets(oct_ctx* ctx, oct_tree* tree, int64_t* edge_offsets);
+
 /* Number of nodes of the last build (synchronizes). */
 OCT_API int oct_tree_n_nodes(oct_ctx* ctx, const oct_tree* tree, int64_t* n_nodes);
 

@@ -10,7 +10,7 @@ from .api import (  # noqa: F401
     set_search_radius_, set_refit_mode_, add_point_set_, resize_point_set_,
     update_point_set_, set_active_search_, run_, build_edges_, build_edges,
     for_each_neighbor, get_neighborlist, materialize_all_neighbors_,
-    device_view, build_edges_diff, colmajor, synchronize,
+    device_view, build_edges_diff, colmajor, synchronize, BatchedSearch, BatchedEdges,
 )
 from . import _lib  # noqa: F401
 

@@ -54,6 +54,8 @@ SIGNATURES = [
     ("oct_tree_create", I, [P, I, I, C.POINTER(P)]),
     ("oct_tree_destroy", I, [P]),
     ("oct_tree_build", I, [P, P, P, I64, D, I]),
+    ("oct_tree_build_batch", I, [P, P, P, I64, P, P, C.c_int32]),
+    ("oct_batch_edge_offsets", I, [P, P, P]),
     ("oct_tree_n_nodes", I, [P, P, C.POINTER(I64)]),
     ("oct_tree_view_get", I, [P, P, C.POINTER(TreeView)]),
     ("oct_edges_count", I, [P, P, P, I, C.POINTER(I64)]),

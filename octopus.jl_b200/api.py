@@ -533,3 +533,74 @@ def build_edges_diff(coords: torch.Tensor, tns: TNS, set_id: int, radius) -> Edg
     a self pair; gradients flow to ``coords`` through a deterministic
     adjoint kernel."""
     return EdgesTuple(*_EdgesDiff.apply(coords, tns, set_id, radius))
+
+
+# ----------------------------------------------------------- batched clouds --
+BatchedEdges = namedtuple("BatchedEdges", ["senders", "receivers", "rel_displacement", "rel_dist_norm",
+                                           "edge_offsets"])
+
+
+class BatchedSearch:
+    """Many independent point clouds searched in one pass (no counterpart in
+    the reference, which needs one TNS per radius, src/api.jl:24-29).
+
+    ``run_(coords, sizes, radii)`` builds every cloud -- cloud ``c`` is the
+    next ``sizes[c]`` columns of the ``(NDIMS, N)`` tensor ``coords`` with
+    search radius ``radii[c]`` -- and ``build_edges()`` returns one
+    concatenated COO (cloud by cloud, each exactly what ``build_edges`` of a
+    TNS holding that cloud alone returns, with 1-based cloud-local indices)
+    plus ``edge_offsets`` (numpy int64, ``n_clouds + 1``)."""
+
+    def __init__(self, T: torch.dtype = torch.float32, ndims: int = 3, device: int | None = None):
+        if ndims not in (2, 3):
+            raise ArgumentError("ndims must be 2 or 3")
+        self.T, self.ndims = T, ndims
+        self.device = torch.cuda.current_device() if device is None else device
+        self._ctx = _Context.get(self.device)
+        self.tree = Octree(self._ctx, ndims, _dtype_code(T))
+        self.n_clouds = 0
+        self._buf = EdgeBuffer(T, ndims, self.device)
+
+    def run_(self, coords: torch.Tensor, sizes, radii) -> "BatchedSearch":
+        if coords.dim() != 2 or coords.shape[0] != self.ndims:
+            raise DimensionMismatch(f"coords must be ({self.ndims}, N)")
+        if coords.dtype != self.T:
+            raise TypeError(f"coords element type {coords.dtype} does not match {self.T}")
+        if not coords.is_cuda:
+            raise ArgumentError("coords must be a CUDA tensor: this backend runs on the GPU only")
+        sizes = np.asarray(sizes, dtype=np.int64)
+        radii = np.ascontiguousarray(np.asarray(radii, dtype=np.float64))
+        if len(sizes) != len(radii) or len(sizes) == 0:
+            raise DimensionMismatch("sizes and radii need one entry per cloud")
+        # radii in the element type, like set_search_radius! (src/api.jl:26)
+        radii = np.asarray([float(torch.tensor(float(r), dtype=self.T).item()) for r in radii], np.float64)
+        coff = np.zeros(len(sizes) + 1, np.int64)
+        coff[1:] = np.cumsum(sizes)
+        self.coords = colmajor(coords)
+        self.n_clouds = len(sizes)
+        self.coff = coff
+        ctx = self._ctx
+        ctx.bind_stream()
+        ctx.check(ctx.lib.oct_tree_build_batch(ctx.handle, self.tree.handle, _ptr(self.coords),
+                                               int(self.coords.shape[1]), coff.ctypes.data_as(C.c_void_p),
+                                               radii.ctypes.data_as(C.c_void_p), self.n_clouds), "batched run!")
+        self.tree.built = True
+        return self
+
+    def build_edges(self) -> BatchedEdges:
+        ctx = self._ctx
+        ctx.bind_stream()
+        buf = self._buf
+        ne = C.c_int64()
+        ctx.check(ctx.lib.oct_edges_count(ctx.handle, self.tree.handle, self.tree.handle, 1, C.byref(ne)),
+                  "batched build_edges")
+        n_edges = int(ne.value)
+        _resize_buffer(buf, self.T, self.ndims, n_edges, self.device)
+        eoff = np.zeros(self.n_clouds + 1, np.int64)
+        ctx.check(ctx.lib.oct_batch_edge_offsets(ctx.handle, self.tree.handle, eoff.ctypes.data_as(C.c_void_p)),
+                  "batched build_edges")
+        if n_edges > 0:
+            ctx.check(ctx.lib.oct_edges_fill(ctx.handle, self.tree.handle, self.tree.handle, 1, _ptr(buf.senders),
+                                             _ptr(buf.receivers), _ptr(buf.rel_displacement.t()),
+                                             _ptr(buf.rel_dist_norm), n_edges), "batched build_edges")
+        return BatchedEdges(buf.senders, buf.receivers, buf.rel_displacement, buf.rel_dist_norm, eoff)

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "internal.h"
 #include "scan.cuh"
@@ -125,10 +126,20 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const T* __restrict__ coord
 template <class T, int D, class K>
 __global__ void __launch_bounds__(kThreads) k_encode(const T* __restrict__ coords, int64_t n, T o0, T o1, T o2,
                                                      T inv_cs, K* __restrict__ keys,
-                                                     uint64_t* __restrict__ morton_out) {
+                                                     uint64_t* __restrict__ morton_out, Batch bt) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const T o[3] = {o0, o1, o2};
+    T o[3] = {o0, o1, o2};
+    int cloud = 0;
+    if (bt.n_clouds) {
+        // Each cloud has its own origin and cell size (one TNS per cloud).
+        cloud = cloud_of_position(bt, i);
+        const double* cp = bt.cparam + (size_t)cloud * kCloudParams;
+        o[0] = (T)cp[0];
+        o[1] = (T)cp[1];
+        o[2] = (T)cp[2];
+        inv_cs = (T)cp[3];
+    }
     constexpr int64_t cmax = (1LL << Dims<D>::bits) - 1;
     uint64_t c[3] = {0, 0, 0};
 #pragma unroll
@@ -140,7 +151,7 @@ __global__ void __launch_bounds__(kThreads) k_encode(const T* __restrict__ coord
     }
     const uint64_t key = (D == 3) ? ((split_by_3(c[2]) << 2) | (split_by_3(c[1]) << 1) | split_by_3(c[0]))
                                   : ((split_by_2(c[1]) << 1) | split_by_2(c[0]));
-    keys[i] = (K)key;
+    keys[i] = bt.n_clouds ? (K)(((uint64_t)cloud << bt.kbits) | key) : (K)key;
     if (morton_out) morton_out[i] = key;
 }
 
@@ -167,6 +178,21 @@ template <int D, class K> __device__ __forceinline__ int common_levels(K a, K b)
     return Dims<D>::bits - 1 - hb / D;
 }
 
+// Same, where keys of different clouds share no level (-1).
+template <int D, class K> __device__ __forceinline__ int common_levels_b(K a, K b, const Batch& bt) {
+    if (!bt.n_clouds) return common_levels<D, K>(a, b);
+    if ((uint64_t)a >> bt.kbits != (uint64_t)b >> bt.kbits) return -1;
+    const uint64_t m = (1ULL << bt.kbits) - 1;
+    return common_levels<D, uint64_t>((uint64_t)a & m, (uint64_t)b & m);
+}
+
+// Digit (child slot) of a key at level L, from its Morton part.
+template <int D, class K> __device__ __forceinline__ int slot_digit(K key, int shd, const Batch& bt) {
+    uint64_t v = (uint64_t)key;
+    if (bt.n_clouds) v &= (1ULL << bt.kbits) - 1;
+    return (int)((v >> shd) & (uint64_t)(Dims<D>::nch - 1));
+}
+
 constexpr int kMarkTile = kThreads;  // positions per block in mark / emit
 
 // lohi[k] = lo | hi << 8: the levels whose node starts at position k are
@@ -175,7 +201,7 @@ constexpr int kMarkTile = kThreads;  // positions per block in mark / emit
 template <int D, class K>
 __global__ void __launch_bounds__(kThreads) k_mark(const K* __restrict__ skeys, int64_t n,
                                                    uint16_t* __restrict__ lohi, int32_t* __restrict__ blockcnt,
-                                                   int nblocks) {
+                                                   int nblocks, Batch bt) {
     constexpr int MAXLEV = Dims<D>::bits;
     constexpr int NLEV = MAXLEV + 1;
     __shared__ K sk[kMarkTile + 64];
@@ -189,13 +215,13 @@ __global__ void __launch_bounds__(kThreads) k_mark(const K* __restrict__ skeys, 
     __syncthreads();
     for (int i = threadIdx.x; i < kMarkTile + 32; i += kThreads) {
         const int64_t j = base - 32 + i;
-        sc[i] = (j >= 0 && j + 32 <= n - 1) ? (int8_t)common_levels<D, K>(sk[i], sk[i + 32]) : (int8_t)-1;
+        sc[i] = (j >= 0 && j + 32 <= n - 1) ? (int8_t)common_levels_b<D, K>(sk[i], sk[i + 32], bt) : (int8_t)-1;
     }
     __syncthreads();
     const int64_t k = base + threadIdx.x;
     int lo = 1, hi = 0;
     if (k < n) {
-        lo = (k == 0) ? 0 : common_levels<D, K>(sk[threadIdx.x + 31], sk[threadIdx.x + 32]) + 1;
+        lo = (k == 0) ? 0 : common_levels_b<D, K>(sk[threadIdx.x + 31], sk[threadIdx.x + 32], bt) + 1;
         int m = -1;
 #pragma unroll 11
         for (int t = 0; t <= 32; ++t) m = max(m, (int)sc[threadIdx.x + t]);
@@ -223,7 +249,7 @@ template <int D>
 __global__ void __launch_bounds__(kThreads) k_emit_ids(int64_t n, const uint16_t* __restrict__ lohi,
                                                        const int64_t* __restrict__ blockoff, int nblocks,
                                                        int64_t capacity, int32_t* __restrict__ first_child,
-                                                       int2* __restrict__ nrange, OctHeader* hdr) {
+                                                       int2* __restrict__ nrange, OctHeader* hdr, Batch bt) {
     constexpr int NLEV = Dims<D>::bits + 1;
     __shared__ int32_t wpre[NLEV][kThreads / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -262,6 +288,7 @@ __global__ void __launch_bounds__(kThreads) k_emit_ids(int64_t n, const uint16_t
                                          __popc(b & lanemask_lt()));
             nrange[id] = make_int2((int)k, L);
             first_child[id] = L < hi ? prev : -1;
+            if (L == 0 && bt.n_clouds) bt.croot[cloud_of_position(bt, k)] = id;
             prev = id;
         }
     }
@@ -274,7 +301,7 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
                                                          const int32_t* __restrict__ first_child_in,
                                                          TNode<T, D>* __restrict__ tnode, int2* __restrict__ nrange,
                                                          int32_t* __restrict__ parent, int32_t* __restrict__ arrive,
-                                                         int32_t* __restrict__ chain, const OctHeader* hdr) {
+                                                         int32_t* __restrict__ chain, const OctHeader* hdr, Batch bt) {
     constexpr int BITS = Dims<D>::bits;
     constexpr int NCH = Dims<D>::nch;
     const int64_t nn = hdr->n_nodes;
@@ -284,16 +311,25 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
     const int64_t k = kl.x;
     const int L = kl.y;
     const int32_t first_child = first_child_in[id];
-    int64_t e = n;
+    // The point set holding k: [s0, s1) (a cloud, or everything).
+    int cloud = 0;
+    int64_t s0 = 0, s1 = n;
+    if (bt.n_clouds) {
+        cloud = cloud_of_position(bt, k);
+        s0 = bt.coff[cloud];
+        s1 = bt.coff[cloud + 1];
+    }
+    int64_t e = s1;
     if (L > 0) {
+        // Within one cloud, comparing whole keys >> sh compares Morton prefixes.
         const int sh = D * (BITS - L);
         const uint64_t pk = (uint64_t)skeys[k] >> sh;
-        if (((uint64_t)skeys[n - 1] >> sh) != pk) {
+        if (((uint64_t)skeys[s1 - 1] >> sh) != pk) {
             // Galloping search for the first position whose level-L prefix differs.
-            int64_t good = k, bad = n, step = 1;
+            int64_t good = k, bad = s1, step = 1;
             while (true) {
                 const int64_t p = k + step;
-                if (p >= n) break;
+                if (p >= s1) break;
                 if (((uint64_t)skeys[p] >> sh) != pk) { bad = p; break; }
                 good = p;
                 step <<= 1;
@@ -312,9 +348,8 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
         nd.b = (int32_t)(e - k);
     } else {
         const int shd = D * BITS - D * (L + 1);
-        const uint64_t msk = (uint64_t)(NCH - 1);
-        const int d0 = (int)(((uint64_t)skeys[k] >> shd) & msk);
-        const int d1 = (int)(((uint64_t)skeys[e - 1] >> shd) & msk);
+        const int d0 = slot_digit<D, K>(skeys[k], shd, bt);
+        const int d1 = slot_digit<D, K>(skeys[e - 1], shd, bt);
         unsigned slots = 1u << d0;
         if (d1 != d0) {
             // lb(v) = first position in [k, e) whose digit >= v; digit v is
@@ -324,9 +359,9 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
                 int64_t a = prev, b = e;
                 while (a < b) {
                     const int64_t mid = (a + b) >> 1;
-                    if ((int)(((uint64_t)skeys[mid] >> shd) & msk) >= v) b = mid; else a = mid + 1;
+                    if (slot_digit<D, K>(skeys[mid], shd, bt) >= v) b = mid; else a = mid + 1;
                 }
-                if (a < e && (int)(((uint64_t)skeys[a] >> shd) & msk) == v) slots |= 1u << v;
+                if (a < e && slot_digit<D, K>(skeys[a], shd, bt) == v) slots |= 1u << v;
                 prev = a;
             }
         }
@@ -335,14 +370,20 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
         const int nc = __popc(slots);
         for (int j = 0; j < nc; ++j) parent[first_child + j] = (int32_t)id;
     }
-    if (k == 0 && e == n) {
-        // A node covering every point has the global bounds.
+    if (k == s0 && e == s1) {
+        // A node covering its whole point set has that set's bounds.
+        if (bt.n_clouds) {
+            const double* cp = bt.cparam + (size_t)cloud * kCloudParams;
 #pragma unroll
-        for (int d = 0; d < D; ++d) { nd.lo[d] = (T)hdr->gmin[d]; nd.hi[d] = (T)hdr->gmax[d]; }
-        // Full-range nodes form the root's chain: chain[L] = id, and
-        // chain[32 + L] = 1 when the node's only child sits in slot 0.
-        chain[L] = (int32_t)id;
-        chain[32 + L] = (nd.b == -1) ? 1 : 0;
+            for (int d = 0; d < D; ++d) { nd.lo[d] = (T)cp[6 + d]; nd.hi[d] = (T)cp[9 + d]; }
+        } else {
+#pragma unroll
+            for (int d = 0; d < D; ++d) { nd.lo[d] = (T)hdr->gmin[d]; nd.hi[d] = (T)hdr->gmax[d]; }
+            // Full-range nodes form the root's chain: chain[L] = id, and
+            // chain[32 + L] = 1 when the node's only child sits in slot 0.
+            chain[L] = (int32_t)id;
+            chain[32 + L] = (nd.b == -1) ? 1 : 0;
+        }
     } else {
 #pragma unroll
         for (int d = 0; d < D; ++d) { nd.lo[d] = T(0); nd.hi[d] = T(0); }
@@ -350,7 +391,7 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
     tnode[id] = nd;
     nrange[id] = make_int2((int)k, (int)(e - 1));
     arrive[id] = 0;
-    if (id == 0) parent[0] = -1;
+    if (L == 0) parent[id] = -1;  // a root (one per cloud in a batch)
 }
 
 // ------------------------------------------------------------- 6. refit --
@@ -361,7 +402,7 @@ template <class T, int D>
 __global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n, TNode<T, D>* tnode,
                                                     const int2* __restrict__ nrange, const int32_t* __restrict__ parent,
                                                     int32_t* arrive, const SPt<T, D>* __restrict__ spts,
-                                                    const OctHeader* hdr) {
+                                                    const OctHeader* hdr, Batch bt) {
     const int64_t nn = hdr->n_nodes;
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (nn > capacity || id >= nn) return;
@@ -382,7 +423,13 @@ __global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n,
         const int32_t p = parent[node];
         if (p < 0) break;
         const int2 rg = nrange[p];
-        if (rg.x == 0 && (int64_t)rg.y == n - 1) break;  // bounds preset from the global reduce
+        int64_t s0 = 0, s1 = n;
+        if (bt.n_clouds) {
+            const int c = cloud_of_position(bt, rg.x);
+            s0 = bt.coff[c];
+            s1 = bt.coff[c + 1];
+        }
+        if (rg.x == s0 && (int64_t)rg.y == s1 - 1) break;  // bounds preset from the set's reduce
         const int32_t pa = tnode[p].a, pb = tnode[p].b;
         const int nc = __popc((unsigned)(-pb));
         __threadfence();
@@ -498,11 +545,85 @@ __global__ void k_view_perm(const SPt<T, D>* __restrict__ spts, int64_t n, int32
     if (k < n) vp[k] = spts[k].idx + 1;
 }
 
+// --------------------------------------------------------- 9. batches ----
+// Per-cloud min/max (Julia order) and non-finite flag, one block per cloud:
+// out[c*8 + 0..2] = min, [3..5] = max, [6] = non-finite.
+template <class T, int D>
+__global__ void __launch_bounds__(kThreads) k_cloud_bounds(const T* __restrict__ coords, const int64_t* __restrict__ coff,
+                                                           double* __restrict__ out) {
+    __shared__ T smin[kThreads / 32][D], smax[kThreads / 32][D];
+    __shared__ int snan;
+    const int c = blockIdx.x;
+    const int64_t s0 = coff[c], s1 = coff[c + 1];
+    if (threadIdx.x == 0) snan = 0;
+    __syncthreads();
+    T lo[D], hi[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) { lo[d] = T(INFINITY); hi[d] = T(-INFINITY); }
+    int bad = 0;
+    for (int64_t i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const T x = coords[D * i + d];
+            if (!isfinite(x)) bad = 1;
+            lo[d] = jl_min(lo[d], x);
+            hi[d] = jl_max(hi[d], x);
+        }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        lo[d] = warp_min(lo[d]);
+        hi[d] = warp_max(hi[d]);
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&snan, 1);
+    if (lane == 0) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) { smin[w][d] = lo[d]; smax[w][d] = hi[d]; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w2 = 1; w2 < kThreads / 32; ++w2)
+            for (int d = 0; d < D; ++d) {
+                smin[0][d] = jl_min(smin[0][d], smin[w2][d]);
+                smax[0][d] = jl_max(smax[0][d], smax[w2][d]);
+            }
+        double* p = out + (size_t)c * 8;
+        for (int d = 0; d < D; ++d) { p[d] = (double)smin[0][d]; p[3 + d] = (double)smax[0][d]; }
+        p[6] = snan ? 1.0 : 0.0;
+    }
+}
+
+// Each cloud's DFS starts below its root's single-child chain (children in
+// slot 0 only), whose nodes all cover the whole cloud.
+template <class T, int D>
+__global__ void k_cloud_start(const TNode<T, D>* __restrict__ tnode, Batch bt, int64_t capacity,
+                              const OctHeader* hdr) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= bt.n_clouds || hdr->n_nodes > capacity) return;
+    int32_t node = bt.croot[c];
+    if (node >= 0) {
+        for (int it = 0; it < 64; ++it) {
+            const TNode<T, D> nd = tnode[node];
+            if (nd.b != -1) break;
+            node = nd.a;
+        }
+    }
+    bt.cstart[c] = node;
+}
+
+__global__ void k_gather_edge_offsets(const int64_t* __restrict__ offsets, const int64_t* __restrict__ coff,
+                                      int n_clouds, int64_t* __restrict__ eoff) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c <= n_clouds) eoff[c] = offsets[coff[c]];
+}
+
 // ------------------------------------------------------------- host side --
 namespace {
 
 template <class T, int D, class K>
 int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
+    const Batch bt = t.batch();
     cudaStream_t s = ctx.stream;
     cudaError_t err;
     constexpr int BITS = Dims<D>::bits;
@@ -523,7 +644,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
     {
         PhaseTimer pt_(ctx, PH_ENCODE);
         k_encode<T, D, K><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, n, o[0], o[1], o[2], inv_cs,
-                                                                    t.keys[0].as<K>(), morton);
+                                                                    t.keys[0].as<K>(), morton, bt);
         ctx.kernel_launches += 1;
     }
 
@@ -570,23 +691,26 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
             (err = ensure(t.groups, (size_t)(cap + n / 32 + 2) * 8)) || (err = ensure(t.chain, 64 * 4)))
             return cuda_status(ctx, err, "allocating node arrays");
         if ((err = cudaMemsetAsync(t.chain.p, 0xff, 64 * 4, s))) return cuda_status(ctx, err, "chain reset");
+        if (bt.n_clouds && (err = cudaMemsetAsync(bt.croot, 0xff, (size_t)bt.n_clouds * 4, s)))
+            return cuda_status(ctx, err, "cloud root reset");
         {
         PhaseTimer pt_(ctx, PH_TOPOLOGY);
-        k_mark<D, K><<<nblocks, kThreads, 0, s>>>(skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(), nblocks);
+        k_mark<D, K><<<nblocks, kThreads, 0, s>>>(skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(), nblocks,
+                                                  bt);
         exclusive_scan_i32_i64(t.blockcnt.as<int32_t>(), t.blockoff.as<int64_t>(), nbc, &hdr->n_nodes,
                                t.scan_tmp.as<int64_t>(), s);
         k_emit_ids<D><<<nblocks, kThreads, 0, s>>>(n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks, cap,
-                                                    t.fchild.as<int32_t>(), t.nrange.as<int2>(), hdr);
+                                                    t.fchild.as<int32_t>(), t.nrange.as<int2>(), hdr, bt);
         k_emit_nodes<T, D, K><<<div_up(cap, kThreads), kThreads, 0, s>>>(
             skeys, n, cap, t.fchild.as<int32_t>(), t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
-            t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.chain.as<int32_t>(), hdr);
+            t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.chain.as<int32_t>(), hdr, bt);
         ctx.kernel_launches += 6;
         }
         {
         PhaseTimer pt_(ctx, PH_REFIT);
         k_refit<T, D><<<div_up(cap, kThreads), kThreads, 0, s>>>(cap, n, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
                                                                   t.parent.as<int32_t>(), t.arrive.as<int32_t>(),
-                                                                  t.spts.as<SPt<T, D>>(), hdr);
+                                                                  t.spts.as<SPt<T, D>>(), hdr, bt);
         ctx.kernel_launches += 1;
         }
         {
@@ -600,6 +724,10 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
                                                                         t.gcnt.as<int32_t>(), t.goff.as<int64_t>(),
                                                                         t.groups.as<int2>(), t.chain.as<int32_t>(), hdr);
             ctx.kernel_launches += 5;
+            if (bt.n_clouds) {
+                k_cloud_start<T, D><<<div_up(bt.n_clouds, 128), 128, 0, s>>>(t.tnode.as<TNode<T, D>>(), bt, cap, hdr);
+                ctx.kernel_launches += 1;
+            }
         }
         if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
             (err = cudaStreamSynchronize(s)))
@@ -668,13 +796,127 @@ int build_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, double radius_d) 
     return run_pipeline<T, D, uint64_t>(ctx, t, coords, n, radius);
 }
 
+template <class T, int D>
+int build_batch_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, const int64_t* coff_host,
+                      const double* radii_host, int32_t nc) {
+    cudaStream_t s = ctx.stream;
+    cudaError_t err;
+    if ((err = ensure(t.hdr, sizeof(OctHeader))) || (err = ensure(t.b_coff, (size_t)(nc + 1) * 8)) ||
+        (err = ensure(t.b_cparam, (size_t)nc * kCloudParams * 8)) || (err = ensure(t.b_croot, (size_t)nc * 4)) ||
+        (err = ensure(t.b_cstart, (size_t)nc * 4)) || (err = ensure(t.b_cbounds, (size_t)nc * 8 * 8)) ||
+        (err = ensure(t.b_eoff, (size_t)(nc + 1) * 8)))
+        return cuda_status(ctx, err, "allocating batch arrays");
+    if (!t.hdr_host) {
+        if ((err = cudaMallocHost((void**)&t.hdr_host, sizeof(OctHeader)))) return cuda_status(ctx, err, "pinned header");
+    }
+    if ((err = cudaMemsetAsync(t.hdr.p, 0, sizeof(OctHeader), s)) ||
+        (err = cudaMemcpyAsync(t.b_coff.p, coff_host, (size_t)(nc + 1) * 8, cudaMemcpyHostToDevice, s)))
+        return cuda_status(ctx, err, "batch upload");
+    {
+        PhaseTimer pt_(ctx, PH_BOUNDS);
+        k_cloud_bounds<T, D><<<nc, kThreads, 0, s>>>(coords, t.b_coff.as<int64_t>(), t.b_cbounds.as<double>());
+        ctx.kernel_launches += 1;
+    }
+    std::vector<double> cb((size_t)nc * 8);
+    if ((err = cudaMemcpyAsync(cb.data(), t.b_cbounds.p, cb.size() * 8, cudaMemcpyDeviceToHost, s)) ||
+        (err = cudaStreamSynchronize(s)))
+        return cuda_status(ctx, err, "cloud bounds");
+    // Per cloud, in T, exactly what a TNS of that cloud alone computes
+    // (src/cpu/bin_cpu.jl:22,35,60; src/cpu/edges_cpu.jl:184-185).
+    std::vector<double> cp((size_t)nc * kCloudParams, 0.0);
+    int64_t cmax_all = 0;
+    for (int c = 0; c < nc; ++c) {
+        if (coff_host[c + 1] == coff_host[c]) continue;
+        const double* b = cb.data() + (size_t)c * 8;
+        if (b[6] != 0.0)
+            return set_error(ctx, ERR_INEXACT, "InexactError: floor(Int32, NaN/Inf) in bin_point (non-finite coordinate)");
+        const T r = (T)radii_host[c];
+        const T inv_cs = T(1) / r;
+        double* p = cp.data() + (size_t)c * kCloudParams;
+        for (int d = 0; d < D; ++d) {
+            const T o = (T)b[d] - T(1e-6);
+            p[d] = (double)o;
+            const T f = std::floor(((T)b[3 + d] - o) * inv_cs);
+            if (!(f >= T(-2147483648.0) && f < T(2147483648.0)))
+                return set_error(ctx, ERR_INEXACT, "InexactError: floor(Int32, (p - origin) / radius) exceeds Int32");
+            int64_t ci = (int64_t)f;
+            const int64_t cm = (1LL << Dims<D>::bits) - 1;
+            ci = ci < 0 ? 0 : (ci > cm ? cm : ci);
+            cmax_all = std::max(cmax_all, ci);
+            p[6 + d] = b[d];
+            p[9 + d] = b[3 + d];
+        }
+        p[3] = (double)inv_cs;
+        p[4] = (double)(r * r);
+        p[5] = (double)(T(1) / r);
+    }
+    if ((err = cudaMemcpyAsync(t.b_cparam.p, cp.data(), cp.size() * 8, cudaMemcpyHostToDevice, s)))
+        return cuda_status(ctx, err, "cloud parameters");
+    int nbits_axis = 0;
+    while (nbits_axis < 63 && (cmax_all >> nbits_axis) != 0) ++nbits_axis;
+    int cbits = 0;
+    while (cbits < 31 && ((int64_t)(nc - 1) >> cbits) != 0) ++cbits;
+    t.kbits = D * nbits_axis;
+    t.key_bits = t.kbits + cbits;
+    if (t.key_bits > 64) return set_error(ctx, ERR_ARGUMENT, "batch: cloud id and Morton code exceed 64 key bits");
+    t.key_bytes = t.key_bits <= 32 ? 4 : 8;
+    t.sort_passes = (t.key_bits + 7) / 8;
+    if (t.key_bytes == 4) return run_pipeline<T, D, uint32_t>(ctx, t, coords, n, T(0));
+    return run_pipeline<T, D, uint64_t>(ctx, t, coords, n, T(0));
+}
+
 }  // namespace
+
+int build_tree_batch(Ctx& ctx, Tree& t, const void* coords, int64_t n, const int64_t* coff_host,
+                     const double* radii_host, int32_t n_clouds) {
+    t.built = false;
+    t.view_valid = false;
+    t.n = n;
+    t.radius = 0.0;
+    t.keep_morton = false;
+    ++t.generation;
+    t.n_clouds = n_clouds;
+    if (n == 0) {
+        t.n_nodes = 0;
+        t.n_groups = 0;
+        t.built = true;
+        return OK;
+    }
+    int st;
+    if (t.dtype == 0)
+        st = t.ndims == 3 ? build_batch_typed<float, 3>(ctx, t, (const float*)coords, n, coff_host, radii_host, n_clouds)
+                          : build_batch_typed<float, 2>(ctx, t, (const float*)coords, n, coff_host, radii_host, n_clouds);
+    else
+        st = t.ndims == 3 ? build_batch_typed<double, 3>(ctx, t, (const double*)coords, n, coff_host, radii_host, n_clouds)
+                          : build_batch_typed<double, 2>(ctx, t, (const double*)coords, n, coff_host, radii_host, n_clouds);
+    if (st == OK) t.built = true;
+    return st;
+}
+
+int batch_edge_offsets(Ctx& ctx, Tree& t, int64_t* out_host) {
+    const int nc = t.n_clouds;
+    cudaError_t err;
+    if (ctx.plan_query != &t || ctx.plan_target != &t || ctx.plan_qgen != t.generation)
+        return set_error(ctx, ERR_STATE, "batch edge offsets: no matching oct_edges_count for this tree");
+    if (t.n == 0 || ctx.plan_edges <= 0) {
+        for (int c = 0; c <= nc; ++c) out_host[c] = 0;
+        return OK;
+    }
+    k_gather_edge_offsets<<<div_up(nc + 1, 128), 128, 0, ctx.stream>>>(ctx.offsets.as<int64_t>(), t.b_coff.as<int64_t>(),
+                                                                        nc, t.b_eoff.as<int64_t>());
+    ctx.kernel_launches += 1;
+    if ((err = cudaMemcpyAsync(out_host, t.b_eoff.p, (size_t)(nc + 1) * 8, cudaMemcpyDeviceToHost, ctx.stream)) ||
+        (err = cudaStreamSynchronize(ctx.stream)))
+        return cuda_status(ctx, err, "batch edge offsets");
+    return OK;
+}
 
 int build_tree(Ctx& ctx, Tree& t, const void* coords, int64_t n, double radius) {
     t.built = false;
     t.view_valid = false;
     t.n = n;
     t.radius = radius;
+    t.n_clouds = 0;
     ++t.generation;
     if (n == 0) {
         t.n_nodes = 0;

@@ -89,6 +89,8 @@ struct DeviceGuard {
 
 void release_tree(oct::Tree& t) {
     using oct::release;
+    for (auto* b : {&t.b_coff, &t.b_cparam, &t.b_croot, &t.b_cstart, &t.b_cbounds, &t.b_eoff})
+        release(*b);
     for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.sort_tmp, &t.spts, &t.tnode, &t.nrange,
                     &t.parent, &t.fchild, &t.arrive, &t.groups, &t.gcnt, &t.goff, &t.chain, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
                     &t.morton, &t.v_first, &t.v_last, &t.v_children, &t.v_bmin, &t.v_bmax, &t.v_perm})
@@ -213,6 +215,35 @@ OCT_API int oct_tree_build(oct_ctx* ctx, oct_tree* tree, const void* coords, int
     return oct::build_tree(ctx->c, tree->t, coords, n, radius);
 }
 
+OCT_API int oct_tree_build_batch(oct_ctx* ctx, oct_tree* tree, const void* coords, int64_t n,
+                                 const int64_t* cloud_offsets, const double* radii, int32_t n_clouds) {
+    if (!ctx || !tree) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (n_clouds < 1 || !cloud_offsets || !radii)
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "batch: need n_clouds >= 1, cloud_offsets and radii");
+    if (n < 0 || n > 2147483647LL)
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "point count must be in [0, 2^31 - 1] (Int32 indices)");
+    if (cloud_offsets[0] != 0 || cloud_offsets[n_clouds] != n)
+        return oct::set_error(ctx->c, OCT_ERR_DIMENSION, "batch: cloud_offsets must start at 0 and end at n");
+    for (int32_t c = 0; c < n_clouds; ++c) {
+        if (cloud_offsets[c + 1] < cloud_offsets[c])
+            return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "batch: cloud_offsets must be non-decreasing");
+        if (!(radii[c] > 0.0)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "search radius must be positive");
+    }
+    if (n > 0 && !coords) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "coords is NULL");
+    DeviceGuard g(ctx->c.device);
+    return oct::build_tree_batch(ctx->c, tree->t, coords, n, cloud_offsets, radii, n_clouds);
+}
+
+OCT_API int oct_batch_edge_offsets(oct_ctx* ctx, oct_tree* tree, int64_t* edge_offsets) {
+    if (!ctx || !tree || !edge_offsets) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (!tree->t.built || tree->t.n_clouds < 1)
+        return oct::set_error(ctx->c, OCT_ERR_STATE, "batch edge offsets: the tree is not a built batch");
+    DeviceGuard g(ctx->c.device);
+    return oct::batch_edge_offsets(ctx->c, tree->t, edge_offsets);
+}
+
 OCT_API int oct_tree_n_nodes(oct_ctx* ctx, const oct_tree* tree, int64_t* n_nodes) {
     if (!ctx || !tree || !n_nodes) return OCT_ERR_ARGUMENT;
     *n_nodes = tree->t.built ? tree->t.n_nodes : 0;
@@ -227,6 +258,7 @@ OCT_API int oct_tree_view_get(oct_ctx* ctx, oct_tree* tree, oct_tree_view* out) 
     out->dtype = t.dtype;
     out->radius = t.radius;
     if (!t.built) return oct::set_error(ctx->c, OCT_ERR_STATE, "tree has not been built (call run! first)");
+    if (t.n_clouds > 0) return oct::set_error(ctx->c, OCT_ERR_STATE, "a batched tree has no single-tree view");
     DeviceGuard g(ctx->c.device);
     const int st = oct::materialize_view(ctx->c, t);
     if (st != OCT_OK) return st;
@@ -260,6 +292,8 @@ OCT_API int oct_edges_count(oct_ctx* ctx, const oct_tree* query, const oct_tree*
     if (st != OCT_OK) return st;
     if (exclude_self && query != target)
         return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "exclude_self requires the same tree as query and target");
+    if ((query->t.n_clouds > 0 || target->t.n_clouds > 0) && (query != target || !exclude_self))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "a batched tree is searched against itself, self pairs excluded");
     DeviceGuard g(ctx->c.device);
     return oct::edges_count(ctx->c, query->t, target->t, exclude_self != 0, n_edges);
 }
@@ -286,6 +320,7 @@ OCT_API int oct_neighbors(oct_ctx* ctx, const oct_tree* target, const void* quer
     if (n_queries > 0 && (!query_coords || !out_counts || (cap_per_query > 0 && !out_indices)))
         return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "NULL buffer");
     if (!target->t.built) return oct::set_error(ctx->c, OCT_ERR_STATE, "target tree has not been built");
+    if (target->t.n_clouds > 0) return oct::set_error(ctx->c, OCT_ERR_STATE, "neighbor queries need a single-set tree");
     DeviceGuard g(ctx->c.device);
     return oct::neighbors_of(ctx->c, target->t, query_coords, n_queries, out_counts, out_indices, cap_per_query);
 }

@@ -94,6 +94,30 @@ __device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
 __device__ __forceinline__ float lo2(unsigned long long v) { return __uint_as_float((unsigned)v); }
 __device__ __forceinline__ float hi2(unsigned long long v) { return __uint_as_float((unsigned)(v >> 32)); }
 
+// A batch of independent point sets ("clouds") built as one forest.  Cloud c
+// occupies positions [coff[c], coff[c+1]) both in input order and in sorted
+// order, because the sort key is (c << kbits) | morton.  n_clouds == 0 means
+// a single point set (every field unused).
+constexpr int kCloudParams = 12;  // origin[3], inv_cs, r2, inv_r, bmin[3], bmax[3]
+struct Batch {
+    int32_t n_clouds = 0;
+    int32_t kbits = 0;
+    const int64_t* coff = nullptr;   // [n_clouds + 1]
+    const double* cparam = nullptr;  // [n_clouds * kCloudParams], values exact in the element type
+    int32_t* croot = nullptr;        // [n_clouds] root node id (-1 for an empty cloud)
+    int32_t* cstart = nullptr;       // [n_clouds] first DFS node of each cloud's tree
+};
+
+// Cloud containing input (== sorted) position i: binary search of coff.
+__device__ __forceinline__ int cloud_of_position(const Batch& b, int64_t i) {
+    int lo = 0, hi = b.n_clouds - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (b.coff[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 // --------------------------------------------------- Julia float semantics --
 // Base.min/max on IEEE floats for non-NaN operands: -0.0 orders below +0.0.
 template <class T> __host__ __device__ __forceinline__ T jl_min(T x, T y) {

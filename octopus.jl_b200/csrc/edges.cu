@@ -40,7 +40,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     const TNode<T, D>* __restrict__ tnode, int32_t start_node,
     const SPt<T, D>* __restrict__ tpts, int64_t n_tnodes, T r2, T inv_r, int exclude_self,
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
-    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ dstatus) {
+    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ dstatus,
+    Batch bt) {
     constexpr int SD = stack_depth<D>();
     // Stack entries are the pushed node's (a, b) record; bit 31 of a marks
     // ascending-order subtrees (see below).
@@ -57,6 +58,17 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     const int2 grp = qgroups[g];
     const bool valid = lane < grp.y;
     const SPt<T, D> q = qpts[grp.x + (valid ? lane : 0)];
+    // A batch searches each cloud in its own tree with its own radius and
+    // reports cloud-local indices.
+    int32_t base = 0;
+    if (bt.n_clouds) {
+        const int c = cloud_of_position(bt, grp.x);
+        const double* cp = bt.cparam + (size_t)c * kCloudParams;
+        r2 = (T)cp[4];
+        inv_r = (T)cp[5];
+        start_node = bt.cstart[c];
+        base = (int32_t)bt.coff[c];
+    }
     T qlo[D], qhi[D];
 #pragma unroll
     for (int d = 0; d < D; ++d) {
@@ -93,8 +105,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                     const SPt<T, D> t = tpts[obuf[w][ql][lane]];
                     T diff[D];
                     const T d2 = dist2<T, D>(t.x, px, diff);
-                    senders[k] = t.idx + 1;
-                    receivers[k] = qi + 1;
+                    senders[k] = t.idx - base + 1;
+                    receivers[k] = qi - base + 1;
 #pragma unroll
                     for (int d = 0; d < D; ++d) rdisp[(int64_t)D * k + d] = mul_rn(-diff[d], inv_r);
                     rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
@@ -285,7 +297,8 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
         PhaseTimer pt_(ctx, PH_COUNT);
         k_edges<T, D, false><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
             q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start, t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0),
-            exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+            exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+            t.batch());
         ctx.kernel_launches += 1;
     }
     {
@@ -311,7 +324,7 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
     k_edges<T, D, true><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, ctx.stream>>>(
         q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start, t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r,
         exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(), senders, receivers, (T*)rel_disp, (T*)rel_dist,
-        ctx.dstatus.as<int>());
+        ctx.dstatus.as<int>(), t.batch());
     ctx.kernel_launches += 1;
     return cuda_status(ctx, cudaGetLastError(), "edge fill launch");
 }
@@ -335,7 +348,7 @@ cudaError_t count_into_typed(const Tree& q, const Tree& t, bool exclude_self, in
     k_edges<T, D, false><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
         q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
         t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr);
+        nullptr, nullptr, nullptr, t.batch());
     return cudaGetLastError();
 }
 

@@ -87,6 +87,25 @@ struct Tree {
     int64_t n_groups = 0;
     int32_t dfs_start = 0;
     DevBuf chain;                // int32[64]: full-range chain node ids and flags
+
+    // Batched build (many clouds in one forest); n_clouds == 0 otherwise.
+    int32_t n_clouds = 0;
+    int32_t kbits = 0;
+    DevBuf b_coff;               // int64 [n_clouds + 1]
+    DevBuf b_cparam;             // double [n_clouds * kCloudParams]
+    DevBuf b_croot, b_cstart;    // int32 [n_clouds]
+    DevBuf b_cbounds;            // double [n_clouds * 8] per-cloud reduce
+    DevBuf b_eoff;               // int64 [n_clouds + 1] per-cloud edge offsets
+    Batch batch() const {
+        Batch b;
+        b.n_clouds = n_clouds;
+        b.kbits = kbits;
+        b.coff = b_coff.as<int64_t>();
+        b.cparam = b_cparam.as<double>();
+        b.croot = b_croot.as<int32_t>();
+        b.cstart = b_cstart.as<int32_t>();
+        return b;
+    }
     int64_t group_capacity = 0;
     OctHeader* hdr_host = nullptr;  // pinned
 
@@ -124,6 +143,9 @@ struct Ctx {
 
 // Build pipeline (build.cu).  Returns a Status.
 int build_tree(Ctx& ctx, Tree& t, const void* coords, int64_t n, double radius);
+int build_tree_batch(Ctx& ctx, Tree& t, const void* coords, int64_t n, const int64_t* coff_host,
+                     const double* radii_host, int32_t n_clouds);
+int batch_edge_offsets(Ctx& ctx, Tree& t, int64_t* out_host);
 int materialize_view(Ctx& ctx, Tree& t);
 
 // Edge pipeline (edges.cu).
