@@ -464,7 +464,7 @@ template <class T, int D, int PASS>
 __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restrict__ tnode, int64_t capacity,
                                                      int32_t* __restrict__ gcnt, const int64_t* __restrict__ goff,
                                                      int2* __restrict__ groups, const int32_t* __restrict__ chain,
-                                                     OctHeader* hdr) {
+                                                     const int32_t* __restrict__ parent, OctHeader* hdr) {
     const int64_t nn = hdr->n_nodes;
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (!PASS && id == 0 && nn <= capacity) {
@@ -488,8 +488,9 @@ __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restri
         ++ng;
     };
     if (nd.b > 0) {
-        // Only a leaf root forms groups of its own.
-        if (id == 0)
+        // Only a leaf root (one per cloud in a batch) forms groups of its own;
+        // other leaves are grouped by their parent.
+        if (parent[id] < 0)
             for (int32_t c0 = 0; c0 < nd.b; c0 += 32) emit(nd.a + c0, min(32, nd.b - c0));
     } else {
         const int nc = __popc((unsigned)(-nd.b));
@@ -717,12 +718,14 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
             PhaseTimer pt_(ctx, PH_GROUPS);
             k_groups<T, D, 0><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
                                                                         t.gcnt.as<int32_t>(), nullptr, nullptr,
-                                                                        t.chain.as<int32_t>(), hdr);
+                                                                        t.chain.as<int32_t>(), t.parent.as<int32_t>(),
+                                                                        hdr);
             exclusive_scan_i32_i64(t.gcnt.as<int32_t>(), t.goff.as<int64_t>(), cap, &hdr->n_groups,
                                    t.scan_tmp.as<int64_t>(), s);
             k_groups<T, D, 1><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
                                                                         t.gcnt.as<int32_t>(), t.goff.as<int64_t>(),
-                                                                        t.groups.as<int2>(), t.chain.as<int32_t>(), hdr);
+                                                                        t.groups.as<int2>(), t.chain.as<int32_t>(),
+                                                                        t.parent.as<int32_t>(), hdr);
             ctx.kernel_launches += 5;
             if (bt.n_clouds) {
                 k_cloud_start<T, D><<<div_up(bt.n_clouds, 128), 128, 0, s>>>(t.tnode.as<TNode<T, D>>(), bt, cap, hdr);
