@@ -281,6 +281,7 @@ def run_ours(args, rank, world, local):
 
     result = None
     if rank == 0:
+        sec = secondary_configs(ob, torch, dev)
         cpu = cpu_baseline(args)
         result = {
             "metric": METRIC,
@@ -312,8 +313,153 @@ def run_ours(args, rank, world, local):
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": cpu,
+            "other_configs": sec,
         }
     return result
+
+
+# ------------------------------------------------- other configurations -----
+def _timed(torch, stream, fn, reps):
+    """Device time (ms) of `reps` calls of fn, CUDA events on the stream."""
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    acc = 0
+    for _ in range(reps):
+        acc += fn()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1), acc
+
+
+def secondary_configs(ob, torch, dev):
+    """The other configurations of the path, each at its full size:
+    uniform 100k (r = 0.04), nonuniform 2D 4M (r = 0.002), 512 batched clouds
+    against a per-cloud loop of the same kernels, and the differentiable 2M
+    configuration with its FP64 central-difference gradient check."""
+    wl = _workloads()
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+
+    def plain(name, x, r, reps):
+        tns = ob.TNS(torch.float32, ndims=x.shape[1])
+        ob.set_search_radius_(tns, r)
+        xd = torch.from_numpy(x).to(dev).t()
+        sid = ob.add_point_set_(tns, xd)
+        ob.set_active_search_(tns, sid, sid)
+
+        def step():
+            ob.update_point_set_(tns, sid, xd)
+            ob.run_(tns)
+            return ob.build_edges(tns, sid, sid).senders.numel()
+
+        step()
+        ms, edges = _timed(torch, stream, step, reps)
+        out[name] = {"n_points": int(x.shape[0]), "radius": r, "edges_per_step": edges // reps,
+                     "ms_per_step": ms / reps, "edges_per_s": edges / (ms / 1e3)}
+        del tns, xd
+        torch.cuda.empty_cache()
+
+    plain("uniform_100k_r0.04", wl.uniform(100_000, 3, 2024), 0.04, 10)
+    plain("nonuniform2d_4M_r0.002_seed2026", wl.gaussian_mixture_2d(4_000_000, 64, 2026), 0.002, 2)
+
+    # --- batched: 512 clouds, sizes log-uniform [500, 20000], r ~ U[0.03, 0.08]
+    rng = np.random.default_rng(4)
+    sizes = np.exp(rng.uniform(np.log(500), np.log(20000), 512)).astype(np.int64)
+    radii = rng.uniform(0.03, 0.08, 512)
+    clouds = [rng.random((int(n), 3)).astype(np.float32) for n in sizes]
+    cat = torch.from_numpy(np.concatenate(clouds)).to(dev).t()
+    bs = ob.BatchedSearch(torch.float32, 3)
+
+    def batched():
+        bs.run_(cat, sizes, radii)
+        return bs.build_edges().senders.numel()
+
+    batched()
+    ms_b, e_b = _timed(torch, stream, batched, 5)
+    tnss = []
+    for x, r in zip(clouds, radii):
+        t = ob.TNS(torch.float32)
+        ob.set_search_radius_(t, float(r))
+        xd = torch.from_numpy(x).to(dev).t()
+        i = ob.add_point_set_(t, xd)
+        ob.set_active_search_(t, i, i)
+        tnss.append((t, i, xd))
+
+    def loop():
+        m = 0
+        for t, i, xd in tnss:
+            ob.update_point_set_(t, i, xd)
+            ob.run_(t)
+            m += ob.build_edges(t, i, i).senders.numel()
+        return m
+
+    loop()
+    ms_l, e_l = _timed(torch, stream, loop, 1)
+    out["batched_512_clouds"] = {
+        "n_points": int(sizes.sum()), "edges": e_b // 5, "ms_batched": ms_b / 5, "ms_per_cloud_loop": ms_l,
+        "edges_per_s_batched": e_b / (ms_b / 1e3), "edges_per_s_loop": e_l / (ms_l / 1e3),
+        "speedup_vs_loop": (ms_l) / (ms_b / 5), "same_edge_count": e_l == e_b // 5}
+    del tnss, bs, cat
+    torch.cuda.empty_cache()
+
+    # --- differentiable: 2M uniform, r = 0.012, fwd + adjoint, FP64 FD check
+    x = wl.uniform(2_000_000, 3, 2025)
+    r = 0.012
+    tns = ob.TNS(torch.float32)
+    ob.set_search_radius_(tns, r)
+    xd = torch.from_numpy(x).to(dev).t()
+    sid = ob.add_point_set_(tns, xd)
+    ob.set_active_search_(tns, sid, sid)
+    state = {}
+
+    def fwd_bwd():
+        c = xd.detach().clone().requires_grad_(True)
+        ob.update_point_set_(tns, sid, c.detach())
+        ob.run_(tns)
+        e = ob.build_edges_diff(c, tns, sid, r)
+        loss = (e.rel_displacement ** 2).sum() + 0.5 * (e.rel_dist_norm ** 2).sum()
+        loss.backward()
+        state["grad"], state["e"] = c.grad, e
+        return e.senders.numel()
+
+    fwd_bwd()
+    ms_d, e_d = _timed(torch, stream, fwd_bwd, 3)
+    g = state["grad"].t().cpu().numpy().astype(np.float64)
+    e = state["e"]
+    rcv = e.receivers.cpu().numpy()
+    snd = e.senders.cpu().numpy()
+    rf = float(np.float32(r))
+    x64 = x.astype(np.float64)
+    pick = np.random.default_rng(0).choice(x.size, 1000, replace=False)
+    lo = np.searchsorted(rcv, np.arange(1, x.shape[0] + 1), "left")
+    hi = np.searchsorted(rcv, np.arange(1, x.shape[0] + 1), "right")
+    errs, fds = [], []
+    h = 1e-4
+    for k in pick:
+        p, d = divmod(int(k), 3)
+        nb = snd[lo[p]:hi[p]] - 1  # frozen neighbor set; each pair is two directed edges
+
+        def f(delta):
+            xp = x64[p].copy()
+            xp[d] += delta
+            dd = (xp[None, :] - x64[nb]) / rf
+            return 2 * 1.5 * (dd * dd).sum()
+
+        fd = (-f(2 * h) + 8 * f(h) - 8 * f(-h) + f(-2 * h)) / (12 * h)
+        errs.append(abs(g[p, d] - fd))
+        fds.append(abs(fd))
+    errs, fds = np.array(errs), np.array(fds)
+    out["diff_2M_r0.012"] = {
+        "n_points": int(x.shape[0]), "edges": e_d // 3, "ms_fwd_bwd": ms_d / 3,
+        "edges_per_s_fwd_bwd": e_d / (ms_d / 1e3),
+        "grad_max_abs_err_over_max_abs_fd": float(errs.max() / fds.max()),
+        "grad_median_rel_err": float(np.median(errs / np.maximum(fds, 1e-30))),
+        "fd": "4-point central differences in FP64, h = 1e-4, frozen edge set, 1000 random coordinates"}
+    del tns, xd, state
+    torch.cuda.empty_cache()
+    return out
 
 
 def cpu_baseline(args, budget_s=None):
