@@ -85,10 +85,11 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     int ocnt = 0;
 
     // One query per round: lane e writes the query's e-th staged edge, so a
-    // round stores a run of consecutive edges of one segment.
-    auto flush = [&]() {
+    // round stores a run of consecutive edges of one segment.  Only the lanes
+    // passing `need` are flushed, so each query leaves in long runs.
+    auto flush = [&](bool need) {
         __syncwarp();
-        unsigned busy = __ballot_sync(0xffffffffu, ocnt > 0);
+        unsigned busy = __ballot_sync(0xffffffffu, need && ocnt > 0);
         while (busy) {
             const int ql = __ffs(busy) - 1;
             busy &= busy - 1;
@@ -115,8 +116,10 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 }
             }
         }
-        cur += ocnt;
-        ocnt = 0;
+        if (need) {
+            cur += ocnt;
+            ocnt = 0;
+        }
         __syncwarp();
     };
 
@@ -141,7 +144,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 const int m = min(kStage, nb - c0);
                 const int mp = (m + 1) & ~1;  // padded to whole pairs with +inf points
                 if (FILL && __any_sync(0xffffffffu, ocnt + m > kStage)) {
-                    flush();
+                    flush(ocnt + m > kStage);
                 }
                 __syncwarp();
                 if (lane < m) {
@@ -220,7 +223,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             __syncwarp();
         }
     }
-    if (FILL) flush();
+    if (FILL) flush(true);
     if (!FILL && valid) counts[q.idx] = (int32_t)(cnt - (self_pair ? 1 : 0));
 }
 
