@@ -167,6 +167,17 @@ OCT_API int oct_edges_diff_backward(oct_ctx* ctx, int ndims, int dtype, int64_t 
                                     const void* rel_dist_norm, const void* d_rel_displacement,
                                     const void* d_rel_dist_norm, double radius, void* grad_coords);
 
+/* The same pullback without the stored features: rel_displacement and
+ * rel_dist_norm are recomputed from `coords` ((ndims, n_points), the
+ * coordinates the edges were built from) with the forward's exact arithmetic,
+ * so a caller short of memory need not keep them for the backward pass.
+ * Requires the self-pair COO of one point set (every edge has its mirror). */
+OCT_API int oct_edges_diff_backward_recompute(oct_ctx* ctx, int ndims, int dtype, int64_t n_points,
+                                              int64_t n_edges, const int32_t* senders,
+                                              const int32_t* receivers, const void* coords,
+                                              const void* d_rel_displacement, const void* d_rel_dist_norm,
+                                              double radius, void* grad_coords);
+
 /* Edge count that allocates no device memory.  No counterpart in the
  * reference: it serves callers that cannot let a library call cudaMalloc --
  * hosts whose device memory belongs to their own pool allocator (a

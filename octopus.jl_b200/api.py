@@ -500,7 +500,7 @@ def device_view(tns: TNS, qid: int, tid: int) -> DeviceView:
 # --------------------------------------------------------- build_edges_diff --
 class _EdgesDiff(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, coords, tns, set_id, radius):
+    def forward(ctx, coords, tns, set_id, radius, recompute):
         e = build_edges(tns, set_id, set_id)
         snd, rcv = e.senders.clone(), e.receivers.clone()
         disp = e.rel_displacement.t().contiguous().t()  # fresh copy, column-major
@@ -508,31 +508,46 @@ class _EdgesDiff(torch.autograd.Function):
         ctx.tns = tns
         ctx.radius = float(radius)
         ctx.coords_shape = coords.shape
-        ctx.save_for_backward(snd, rcv, disp, dist)
+        ctx.recompute = bool(recompute)
+        if ctx.recompute:
+            # Keep only the indices and the coordinates: the backward pass
+            # recomputes the features (memory-lean mode).
+            ctx.save_for_backward(snd, rcv, colmajor(coords.detach()))
+        else:
+            ctx.save_for_backward(snd, rcv, disp, dist)
         ctx.mark_non_differentiable(snd, rcv)
         return snd, rcv, disp, dist
 
     @staticmethod
     def backward(ctx, g_snd, g_rcv, g_disp, g_dist):
-        snd, rcv, disp, dist = ctx.saved_tensors
         tns = ctx.tns
         d, n = ctx.coords_shape
-        grad = torch.empty((n, d), dtype=disp.dtype, device=disp.device)
+        T = tns.T
+        dev = f"cuda:{tns.device}"
+        grad = torch.empty((n, d), dtype=T, device=dev)
         dd = None if g_disp is None else g_disp.t().contiguous()
         dn = None if g_dist is None else g_dist.reshape(-1).contiguous()
         lc = tns._ctx
         lc.bind_stream()
-        lc.check(lc.lib.oct_edges_diff_backward(
-            lc.handle, d, _dtype_code(disp.dtype), n, snd.numel(), _ptr(snd), _ptr(rcv), _ptr(disp.t()),
-            _ptr(dist), _ptr(dd), _ptr(dn), ctx.radius, _ptr(grad)), "build_edges_diff pullback")
-        return grad.t(), None, None, None
+        if ctx.recompute:
+            snd, rcv, xc = ctx.saved_tensors
+            lc.check(lc.lib.oct_edges_diff_backward_recompute(
+                lc.handle, d, _dtype_code(T), n, snd.numel(), _ptr(snd), _ptr(rcv), _ptr(xc), _ptr(dd), _ptr(dn),
+                ctx.radius, _ptr(grad)), "build_edges_diff pullback")
+        else:
+            snd, rcv, disp, dist = ctx.saved_tensors
+            lc.check(lc.lib.oct_edges_diff_backward(
+                lc.handle, d, _dtype_code(T), n, snd.numel(), _ptr(snd), _ptr(rcv), _ptr(disp.t()), _ptr(dist),
+                _ptr(dd), _ptr(dn), ctx.radius, _ptr(grad)), "build_edges_diff pullback")
+        return grad.t(), None, None, None, None
 
 
-def build_edges_diff(coords: torch.Tensor, tns: TNS, set_id: int, radius) -> EdgesTuple:
+def build_edges_diff(coords: torch.Tensor, tns: TNS, set_id: int, radius, recompute: bool = False) -> EdgesTuple:
     """ext/OctopusChainRulesCoreExt.jl:103-192: differentiable build_edges for
     a self pair; gradients flow to ``coords`` through a deterministic
-    adjoint kernel."""
-    return EdgesTuple(*_EdgesDiff.apply(coords, tns, set_id, radius))
+    adjoint kernel.  ``recompute=True`` keeps no feature arrays for the
+    backward pass and recomputes them from ``coords`` (identical values)."""
+    return EdgesTuple(*_EdgesDiff.apply(coords, tns, set_id, radius, recompute))
 
 
 # ----------------------------------------------------------- batched clouds --

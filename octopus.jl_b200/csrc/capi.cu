@@ -340,7 +340,26 @@ OCT_API int oct_edges_diff_backward(oct_ctx* ctx, int ndims, int dtype, int64_t 
         return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge array is NULL");
     DeviceGuard g(ctx->c.device);
     return oct::diff_backward(ctx->c, ndims, dtype, n_points, n_edges, senders, receivers, rel_displacement,
-                              rel_dist_norm, d_rel_displacement, d_rel_dist_norm, radius, grad_coords);
+                              rel_dist_norm, d_rel_displacement, d_rel_dist_norm, radius, grad_coords, nullptr);
+}
+
+OCT_API int oct_edges_diff_backward_recompute(oct_ctx* ctx, int ndims, int dtype, int64_t n_points,
+                                              int64_t n_edges, const int32_t* senders, const int32_t* receivers,
+                                              const void* coords, const void* d_rel_displacement,
+                                              const void* d_rel_dist_norm, double radius, void* grad_coords) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (bad_dims(ndims) || bad_dtype(dtype)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "bad ndims/dtype");
+    if (n_points < 0 || n_edges < 0 || n_edges > 2147483647LL || n_points > 2147483647LL)
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "sizes must fit Int32");
+    if (!(radius > 0.0)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "radius must be positive");
+    if (n_points > 0 && (!grad_coords || !coords))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "coords/grad_coords is NULL");
+    if (n_edges > 0 && (!senders || !receivers))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge array is NULL");
+    DeviceGuard g(ctx->c.device);
+    return oct::diff_backward(ctx->c, ndims, dtype, n_points, n_edges, senders, receivers, nullptr, nullptr,
+                              d_rel_displacement, d_rel_dist_norm, radius, grad_coords, coords);
 }
 
 static const char* kPhaseNames[oct::PH_NUM] = {"bounds", "encode", "sort", "gather", "topology",

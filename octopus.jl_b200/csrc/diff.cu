@@ -92,7 +92,103 @@ __global__ void k_grad(int64_t n, const int64_t* __restrict__ roff, const int64_
     for (int d = 0; d < D; ++d) grad[(int64_t)D * i + d] = (T)acc[d];
 }
 
+// Edge term recomputed from the coordinates instead of the stored features:
+// rel_disp = (x_i - x_j) * inv_r and rel_dist = sqrt(d2) * inv_r with the
+// forward's exact operation order, so the values are identical.
+template <class T, int D>
+__device__ __forceinline__ void edge_term_recompute(int64_t k, int32_t i, int32_t j, const T* __restrict__ coords,
+                                                    const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r,
+                                                    T inv_r, double* out) {
+    T diff[D];
+    const T d2 = dist2<T, D>(coords + (int64_t)D * j, coords + (int64_t)D * i, diff);  // x_j - x_i
+#pragma unroll
+    for (int d = 0; d < D; ++d) out[d] = 0.0;
+    if (d_disp) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) out[d] += (double)div_rn(d_disp[(int64_t)D * k + d], r);
+    }
+    if (d_dist) {
+        const T dn = mul_rn(sqrt_rn(d2), inv_r);
+        if (dn > T(1e-8)) {
+            const T inv = div_rn(d_dist[k], mul_rn(dn, r));
+#pragma unroll
+            for (int d = 0; d < D; ++d) out[d] += (double)mul_rn(mul_rn(-diff[d], inv_r), inv);
+        }
+    }
+}
+
+// Self-pair adjoint without a sort.  The neighbor relation of a self pair is
+// symmetric, so the edge (i <- j) of point i's segment has a twin (j <- i) in
+// j's segment; point i's gradient is the sum over its own segment of
+// term(k) - term(twin(k)), in segment order.  A missing twin (the edges are
+// not a self-pair COO) raises the flag and the caller uses the sorted path.
+template <class T, int D, bool RECOMPUTE>
+__global__ void k_grad_twins(int64_t n, const int64_t* __restrict__ roff, const int32_t* __restrict__ snd,
+                             const T* __restrict__ rel_disp, const T* __restrict__ rel_dist,
+                             const T* __restrict__ coords, const T* __restrict__ d_disp, const T* __restrict__ d_dist,
+                             T r, T inv_r, T* __restrict__ grad, int* __restrict__ missing) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc[D], c[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) acc[d] = 0.0;
+    const int64_t k0 = roff[i], k1 = roff[i + 1];
+    for (int64_t k = k0; k < k1; ++k) {
+        const int32_t j = snd[k] - 1;
+        if (RECOMPUTE) edge_term_recompute<T, D>(k, (int32_t)i, j, coords, d_disp, d_dist, r, inv_r, c);
+        else edge_term<T, D>(k, rel_disp, rel_dist, d_disp, d_dist, r, c);
+#pragma unroll
+        for (int d = 0; d < D; ++d) acc[d] += c[d];
+        int64_t tw = -1;
+        const int64_t m1 = roff[j + 1];
+        for (int64_t m = roff[j]; m < m1; ++m)
+            if (snd[m] - 1 == (int32_t)i) { tw = m; break; }
+        if (tw < 0) {
+            atomicOr(missing, 1);
+            return;
+        }
+        if (RECOMPUTE) edge_term_recompute<T, D>(tw, j, (int32_t)i, coords, d_disp, d_dist, r, inv_r, c);
+        else edge_term<T, D>(tw, rel_disp, rel_dist, d_disp, d_dist, r, c);
+#pragma unroll
+        for (int d = 0; d < D; ++d) acc[d] -= c[d];
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) grad[(int64_t)D * i + d] = (T)acc[d];
+}
+
 namespace {
+
+template <class T, int D>
+int twins_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_t* rcv, const void* rel_disp,
+                const void* rel_dist, const void* coords, const void* d_disp, const void* d_dist, double radius,
+                void* grad, bool* ok) {
+    cudaStream_t s = ctx.stream;
+    cudaError_t err;
+    const T r = (T)radius;
+    const T inv_r = T(1) / r;
+    if ((err = ensure(ctx.droff, (n + 1) * 8)) || (err = ensure(ctx.dstatus, 4)))
+        return cuda_status(ctx, err, "allocating adjoint scratch");
+    const int tb = 256;
+    PhaseTimer pt_(ctx, PH_ADJOINT);
+    if ((err = cudaMemsetAsync(ctx.dstatus.p, 0, 4, s))) return cuda_status(ctx, err, "status reset");
+    k_segment_starts<<<div_up(n + 1, tb), tb, 0, s>>>(rcv, m, n, ctx.droff.as<int64_t>());
+    if (coords)
+        k_grad_twins<T, D, true><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), snd, nullptr, nullptr,
+                                                               (const T*)coords, (const T*)d_disp, (const T*)d_dist,
+                                                               r, inv_r, (T*)grad, ctx.dstatus.as<int>());
+    else
+        k_grad_twins<T, D, false><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), snd, (const T*)rel_disp,
+                                                                (const T*)rel_dist, nullptr, (const T*)d_disp,
+                                                                (const T*)d_dist, r, inv_r, (T*)grad,
+                                                                ctx.dstatus.as<int>());
+    ctx.kernel_launches += 2;
+    int missing = 0;
+    if ((err = cudaMemcpyAsync(&missing, ctx.dstatus.p, 4, cudaMemcpyDeviceToHost, s)) ||
+        (err = cudaStreamSynchronize(s)))
+        return cuda_status(ctx, err, "adjoint");
+    *ok = missing == 0;
+    return OK;
+}
 
 template <class T, int D>
 int backward_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_t* rcv, const void* rel_disp,
@@ -132,8 +228,29 @@ int backward_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int
 
 int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n, int64_t m, const int32_t* snd, const int32_t* rcv,
                   const void* rel_disp, const void* rel_dist, const void* d_disp, const void* d_dist, double radius,
-                  void* grad) {
+                  void* grad, const void* coords) {
     if (n == 0) return OK;
+    // The twin search scans a neighbor's whole segment per edge: worthwhile
+    // for the sparse graphs of this path (tens of neighbors), while dense
+    // graphs go through the sorted path.
+    const bool twins = coords != nullptr || m <= 64 * n;
+    if (m > 0 && (d_disp || d_dist) && twins) {
+        bool ok = false;
+        int st;
+        if (dtype == 0)
+            st = ndims == 3 ? twins_typed<float, 3>(ctx, n, m, snd, rcv, rel_disp, rel_dist, coords, d_disp, d_dist,
+                                                    radius, grad, &ok)
+                            : twins_typed<float, 2>(ctx, n, m, snd, rcv, rel_disp, rel_dist, coords, d_disp, d_dist,
+                                                    radius, grad, &ok);
+        else
+            st = ndims == 3 ? twins_typed<double, 3>(ctx, n, m, snd, rcv, rel_disp, rel_dist, coords, d_disp, d_dist,
+                                                     radius, grad, &ok)
+                            : twins_typed<double, 2>(ctx, n, m, snd, rcv, rel_disp, rel_dist, coords, d_disp, d_dist,
+                                                     radius, grad, &ok);
+        if (st != OK || ok) return st;
+        if (coords)
+            return set_error(ctx, ERR_ARGUMENT, "build_edges_diff adjoint: recomputing needs a self-pair COO");
+    }
     if (dtype == 0)
         return ndims == 3 ? backward_typed<float, 3>(ctx, n, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist, radius, grad)
                           : backward_typed<float, 2>(ctx, n, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist, radius, grad);

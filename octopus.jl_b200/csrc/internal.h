@@ -160,7 +160,7 @@ cudaError_t count_into(const Tree& q, const Tree& t, bool exclude_self, int32_t*
 int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,
                   const int32_t* senders, const int32_t* receivers, const void* rel_disp,
                   const void* rel_dist, const void* d_disp, const void* d_dist, double radius,
-                  void* grad);
+                  void* grad, const void* coords);
 
 int set_error(Ctx& ctx, int status, const std::string& msg);
 int cuda_status(Ctx& ctx, cudaError_t e, const char* where);

@@ -83,6 +83,8 @@ def _run(name: str, steps: int, scale: float):
         r = 0.012
     else:
         raise SystemExit(f"unknown workload {name}")
+    if name == "diff2m":
+        return _run_diff(ob, torch, xs, r)
     d = xs[0].shape[1]
     tns = ob.TNS(torch.float32, ndims=d)
     ob.set_search_radius_(tns, r)
@@ -96,6 +98,39 @@ def _run(name: str, steps: int, scale: float):
         e = ob.build_edges(tns, sid, sid)
         ob.synchronize(tns)
         print(f"{name}: n={x.shape[1]} edges={e.senders.numel()}")
+
+
+def _run_diff(ob, torch, xs, r):
+    """build_edges_diff forward + adjoint, with the library's phase times."""
+    import ctypes as C
+    tns = ob.TNS(torch.float32, ndims=3)
+    ob.set_search_radius_(tns, r)
+    c0 = torch.from_numpy(xs[0]).cuda().t()
+    sid = ob.add_point_set_(tns, c0)
+    ob.set_active_search_(tns, sid, sid)
+    lib, ctx = tns._ctx.lib, tns._ctx
+    nph = len(ob._lib.PHASES)
+    ms = (C.c_double * nph)()
+    cnt = (C.c_int64 * nph)()
+    for step, x in enumerate(xs):
+        c = torch.from_numpy(x).cuda().t().requires_grad_(True)
+        lib.oct_profile_enable(ctx.handle, 1)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
+        ob.update_point_set_(tns, sid, c.detach())
+        ob.run_(tns)
+        ev[1].record()
+        e = ob.build_edges_diff(c, tns, sid, r)
+        loss = (e.rel_displacement ** 2).sum() + 0.5 * (e.rel_dist_norm ** 2).sum()
+        ev[2].record()
+        loss.backward()
+        ev[3].record()
+        torch.cuda.synchronize()
+        lib.oct_profile_read(ctx.handle, ms, cnt, nph)
+        lib.oct_profile_enable(ctx.handle, 0)
+        ph = {ob._lib.PHASES[i]: round(ms[i], 4) for i in range(nph) if cnt[i]}
+        print(f"diff2m step {step}: edges={e.senders.numel()} build={ev[0].elapsed_time(ev[1]):.3f} ms "
+              f"forward={ev[1].elapsed_time(ev[2]):.3f} ms backward={ev[2].elapsed_time(ev[3]):.3f} ms phases={ph}")
 
 
 if __name__ == "__main__":
