@@ -118,15 +118,32 @@ __device__ __forceinline__ void edge_term_recompute(int64_t k, int32_t i, int32_
 }
 
 // Self-pair adjoint without a sort.  The neighbor relation of a self pair is
-// symmetric, so the edge (i <- j) of point i's segment has a twin (j <- i) in
-// j's segment; point i's gradient is the sum over its own segment of
-// term(k) - term(twin(k)), in segment order.  A missing twin (the edges are
-// not a self-pair COO) raises the flag and the caller uses the sorted path.
+// symmetric, so the edge k = (i <- j) of point i's segment has a twin
+// (j <- i) in j's segment.  k_find_twins finds it for every edge (one thread
+// per edge scans j's segment); a missing twin (the edges are not a self-pair
+// COO) raises the flag and the caller takes the sorted path.
+__global__ void k_find_twins(int64_t m, const int64_t* __restrict__ roff, const int32_t* __restrict__ snd,
+                             const int32_t* __restrict__ rcv, int32_t* __restrict__ twin, int* __restrict__ missing) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const int32_t i1 = rcv[k];
+    const int32_t j = snd[k] - 1;
+    const int64_t m1 = roff[j + 1];
+    int64_t tw = -1;
+    for (int64_t q = roff[j]; q < m1; ++q)
+        if (snd[q] == i1) { tw = q; break; }
+    if (tw < 0) atomicOr(missing, 1);
+    twin[k] = (int32_t)tw;
+}
+
+// Point i's gradient: the sum over its own segment, in segment order, of
+// term(k) - term(twin(k)) in double precision.
 template <class T, int D, bool RECOMPUTE>
 __global__ void k_grad_twins(int64_t n, const int64_t* __restrict__ roff, const int32_t* __restrict__ snd,
-                             const T* __restrict__ rel_disp, const T* __restrict__ rel_dist,
-                             const T* __restrict__ coords, const T* __restrict__ d_disp, const T* __restrict__ d_dist,
-                             T r, T inv_r, T* __restrict__ grad, int* __restrict__ missing) {
+                             const int32_t* __restrict__ twin, const T* __restrict__ rel_disp,
+                             const T* __restrict__ rel_dist, const T* __restrict__ coords,
+                             const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r, T inv_r,
+                             T* __restrict__ grad) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double acc[D], c[D];
@@ -135,18 +152,11 @@ __global__ void k_grad_twins(int64_t n, const int64_t* __restrict__ roff, const 
     const int64_t k0 = roff[i], k1 = roff[i + 1];
     for (int64_t k = k0; k < k1; ++k) {
         const int32_t j = snd[k] - 1;
+        const int64_t tw = twin[k];
         if (RECOMPUTE) edge_term_recompute<T, D>(k, (int32_t)i, j, coords, d_disp, d_dist, r, inv_r, c);
         else edge_term<T, D>(k, rel_disp, rel_dist, d_disp, d_dist, r, c);
 #pragma unroll
         for (int d = 0; d < D; ++d) acc[d] += c[d];
-        int64_t tw = -1;
-        const int64_t m1 = roff[j + 1];
-        for (int64_t m = roff[j]; m < m1; ++m)
-            if (snd[m] - 1 == (int32_t)i) { tw = m; break; }
-        if (tw < 0) {
-            atomicOr(missing, 1);
-            return;
-        }
         if (RECOMPUTE) edge_term_recompute<T, D>(tw, j, (int32_t)i, coords, d_disp, d_dist, r, inv_r, c);
         else edge_term<T, D>(tw, rel_disp, rel_dist, d_disp, d_dist, r, c);
 #pragma unroll
@@ -166,29 +176,37 @@ int twins_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_
     cudaError_t err;
     const T r = (T)radius;
     const T inv_r = T(1) / r;
-    if ((err = ensure(ctx.droff, (n + 1) * 8)) || (err = ensure(ctx.dstatus, 4)))
+    if ((err = ensure(ctx.droff, (n + 1) * 8)) || (err = ensure(ctx.dstatus, 8)) ||
+        (err = ensure(ctx.dvals[0], (size_t)m * 4)))
         return cuda_status(ctx, err, "allocating adjoint scratch");
     const int tb = 256;
     PhaseTimer pt_(ctx, PH_ADJOINT);
-    if ((err = cudaMemsetAsync(ctx.dstatus.p, 0, 4, s))) return cuda_status(ctx, err, "status reset");
+    // Word 1 of the status buffer (word 0 belongs to the edge fill guard).
+    int* missing_flag = ctx.dstatus.as<int>() + 1;
+    if ((err = cudaMemsetAsync(missing_flag, 0, 4, s))) return cuda_status(ctx, err, "status reset");
+    int32_t* twin = ctx.dvals[0].as<int32_t>();
     k_segment_starts<<<div_up(n + 1, tb), tb, 0, s>>>(rcv, m, n, ctx.droff.as<int64_t>());
-    if (coords)
-        k_grad_twins<T, D, true><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), snd, nullptr, nullptr,
-                                                               (const T*)coords, (const T*)d_disp, (const T*)d_dist,
-                                                               r, inv_r, (T*)grad, ctx.dstatus.as<int>());
-    else
-        k_grad_twins<T, D, false><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), snd, (const T*)rel_disp,
-                                                                (const T*)rel_dist, nullptr, (const T*)d_disp,
-                                                                (const T*)d_dist, r, inv_r, (T*)grad,
-                                                                ctx.dstatus.as<int>());
+    k_find_twins<<<div_up(m, tb), tb, 0, s>>>(m, ctx.droff.as<int64_t>(), snd, rcv, twin, missing_flag);
     ctx.kernel_launches += 2;
     int missing = 0;
-    if ((err = cudaMemcpyAsync(&missing, ctx.dstatus.p, 4, cudaMemcpyDeviceToHost, s)) ||
+    if ((err = cudaMemcpyAsync(&missing, missing_flag, 4, cudaMemcpyDeviceToHost, s)) ||
         (err = cudaStreamSynchronize(s)))
         return cuda_status(ctx, err, "adjoint");
     *ok = missing == 0;
-    return OK;
+    if (!*ok) return OK;
+    if (coords)
+        k_grad_twins<T, D, true><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), snd, twin, nullptr, nullptr,
+                                                               (const T*)coords, (const T*)d_disp, (const T*)d_dist,
+                                                               r, inv_r, (T*)grad);
+    else
+        k_grad_twins<T, D, false><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), snd, twin,
+                                                                (const T*)rel_disp, (const T*)rel_dist, nullptr,
+                                                                (const T*)d_disp, (const T*)d_dist, r, inv_r,
+                                                                (T*)grad);
+    ctx.kernel_launches += 1;
+    return cuda_status(ctx, cudaGetLastError(), "adjoint launch");
 }
+
 
 template <class T, int D>
 int backward_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_t* rcv, const void* rel_disp,

@@ -286,7 +286,7 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
     if ((err = ensure(ctx.counts, (size_t)std::max<int64_t>(nq, 1) * 4)) ||
         (err = ensure(ctx.offsets, (size_t)(nq + 1) * 8)) ||
         (err = ensure(ctx.scan_tmp, (size_t)scan_tmp_elems(nq) * 8)) || (err = ensure(ctx.total, 8)) ||
-        (err = ensure(ctx.dstatus, 4)))
+        (err = ensure(ctx.dstatus, 8)))
         return cuda_status(ctx, err, "allocating edge scratch");
     if ((err = cudaMemsetAsync(ctx.dstatus.p, 0, 4, s))) return cuda_status(ctx, err, "status reset");
     if (!ctx.total_host) {
