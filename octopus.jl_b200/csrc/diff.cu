@@ -92,75 +92,79 @@ __global__ void k_grad(int64_t n, const int64_t* __restrict__ roff, const int64_
     for (int d = 0; d < D; ++d) grad[(int64_t)D * i + d] = (T)acc[d];
 }
 
-// Edge term recomputed from the coordinates instead of the stored features:
-// rel_disp = (x_i - x_j) * inv_r and rel_dist = sqrt(d2) * inv_r with the
-// forward's exact operation order, so the values are identical.
-template <class T, int D>
-__device__ __forceinline__ void edge_term_recompute(int64_t k, int32_t i, int32_t j, const T* __restrict__ coords,
-                                                    const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r,
-                                                    T inv_r, double* out) {
-    T diff[D];
-    const T d2 = dist2<T, D>(coords + (int64_t)D * j, coords + (int64_t)D * i, diff);  // x_j - x_i
-#pragma unroll
-    for (int d = 0; d < D; ++d) out[d] = 0.0;
-    if (d_disp) {
-#pragma unroll
-        for (int d = 0; d < D; ++d) out[d] += (double)div_rn(d_disp[(int64_t)D * k + d], r);
-    }
-    if (d_dist) {
-        const T dn = mul_rn(sqrt_rn(d2), inv_r);
-        if (dn > T(1e-8)) {
-            const T inv = div_rn(d_dist[k], mul_rn(dn, r));
-#pragma unroll
-            for (int d = 0; d < D; ++d) out[d] += (double)mul_rn(mul_rn(-diff[d], inv_r), inv);
-        }
-    }
-}
-
 // Self-pair adjoint without a sort.  The neighbor relation of a self pair is
 // symmetric, so the edge k = (i <- j) of point i's segment has a twin
-// (j <- i) in j's segment.  k_find_twins finds it for every edge (one thread
-// per edge scans j's segment); a missing twin (the edges are not a self-pair
-// COO) raises the flag and the caller takes the sorted path.
-__global__ void k_find_twins(int64_t m, const int64_t* __restrict__ roff, const int32_t* __restrict__ snd,
-                             const int32_t* __restrict__ rcv, int32_t* __restrict__ twin, int* __restrict__ missing) {
+// t = (j <- i) in j's segment, found by scanning j's segment.  The twin's
+// features are those of k mirrored exactly (rel_disp[t] = -rel_disp[k] and
+// rel_dist[t] = rel_dist[k] bit for bit, from the forward's arithmetic), so
+// only its cotangents are read.  Point i's gradient is
+//   sum over its segment of term(k) - term(t),
+// one value per edge here (v[k], in edge order), summed per segment by
+// k_sum_segments.  A missing twin (the edges are not a self-pair COO) raises
+// the flag and the caller takes the sorted path.
+template <class T, int D, bool RECOMPUTE>
+__global__ void k_edge_net(int64_t m, const int64_t* __restrict__ roff, const int32_t* __restrict__ snd,
+                           const int32_t* __restrict__ rcv, const T* __restrict__ rel_disp,
+                           const T* __restrict__ rel_dist, const T* __restrict__ coords,
+                           const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r, T inv_r,
+                           double* __restrict__ v, int* __restrict__ missing) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= m) return;
     const int32_t i1 = rcv[k];
     const int32_t j = snd[k] - 1;
-    const int64_t m1 = roff[j + 1];
+    const int64_t q1 = roff[j + 1];
     int64_t tw = -1;
-    for (int64_t q = roff[j]; q < m1; ++q)
+    for (int64_t q = roff[j]; q < q1; ++q)
         if (snd[q] == i1) { tw = q; break; }
-    if (tw < 0) atomicOr(missing, 1);
-    twin[k] = (int32_t)tw;
+    if (tw < 0) {
+        atomicOr(missing, 1);
+        return;
+    }
+    // Features of edge k (receiver i = i1 - 1, sender j).
+    T rd[D], rn;
+    if (RECOMPUTE) {
+        T diff[D];
+        const T d2 = dist2<T, D>(coords + (int64_t)D * j, coords + (int64_t)D * (i1 - 1), diff);
+#pragma unroll
+        for (int d = 0; d < D; ++d) rd[d] = mul_rn(-diff[d], inv_r);
+        rn = mul_rn(sqrt_rn(d2), inv_r);
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) rd[d] = rel_disp[(int64_t)D * k + d];
+        rn = rel_dist[k];
+    }
+    double net[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) net[d] = 0.0;
+    if (d_disp) {
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+            net[d] += (double)div_rn(d_disp[(int64_t)D * k + d], r) - (double)div_rn(d_disp[(int64_t)D * tw + d], r);
+    }
+    if (d_dist && rn > T(1e-8)) {
+        const T a = div_rn(d_dist[k], mul_rn(rn, r));
+        const T b = div_rn(d_dist[tw], mul_rn(rn, r));
+        // term(t) uses rel_disp[t] = -rd, so it enters with the opposite sign.
+#pragma unroll
+        for (int d = 0; d < D; ++d) net[d] += (double)mul_rn(rd[d], a) + (double)mul_rn(rd[d], b);
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) v[(int64_t)D * k + d] = net[d];
 }
 
-// Point i's gradient: the sum over its own segment, in segment order, of
-// term(k) - term(twin(k)) in double precision.
-template <class T, int D, bool RECOMPUTE>
-__global__ void k_grad_twins(int64_t n, const int64_t* __restrict__ roff, const int32_t* __restrict__ snd,
-                             const int32_t* __restrict__ twin, const T* __restrict__ rel_disp,
-                             const T* __restrict__ rel_dist, const T* __restrict__ coords,
-                             const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r, T inv_r,
-                             T* __restrict__ grad) {
+// grad[i] = sum of v over point i's segment, in edge order.
+template <class T, int D>
+__global__ void k_sum_segments(int64_t n, const int64_t* __restrict__ roff, const double* __restrict__ v,
+                               T* __restrict__ grad) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double acc[D], c[D];
+    double acc[D];
 #pragma unroll
     for (int d = 0; d < D; ++d) acc[d] = 0.0;
-    const int64_t k0 = roff[i], k1 = roff[i + 1];
-    for (int64_t k = k0; k < k1; ++k) {
-        const int32_t j = snd[k] - 1;
-        const int64_t tw = twin[k];
-        if (RECOMPUTE) edge_term_recompute<T, D>(k, (int32_t)i, j, coords, d_disp, d_dist, r, inv_r, c);
-        else edge_term<T, D>(k, rel_disp, rel_dist, d_disp, d_dist, r, c);
+    const int64_t k1 = roff[i + 1];
+    for (int64_t k = roff[i]; k < k1; ++k) {
 #pragma unroll
-        for (int d = 0; d < D; ++d) acc[d] += c[d];
-        if (RECOMPUTE) edge_term_recompute<T, D>(tw, j, (int32_t)i, coords, d_disp, d_dist, r, inv_r, c);
-        else edge_term<T, D>(tw, rel_disp, rel_dist, d_disp, d_dist, r, c);
-#pragma unroll
-        for (int d = 0; d < D; ++d) acc[d] -= c[d];
+        for (int d = 0; d < D; ++d) acc[d] += v[(int64_t)D * k + d];
     }
 #pragma unroll
     for (int d = 0; d < D; ++d) grad[(int64_t)D * i + d] = (T)acc[d];
@@ -177,16 +181,24 @@ int twins_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_
     const T r = (T)radius;
     const T inv_r = T(1) / r;
     if ((err = ensure(ctx.droff, (n + 1) * 8)) || (err = ensure(ctx.dstatus, 8)) ||
-        (err = ensure(ctx.dvals[0], (size_t)m * 4)))
+        (err = ensure(ctx.dnet, (size_t)m * D * 8)))
         return cuda_status(ctx, err, "allocating adjoint scratch");
     const int tb = 256;
     PhaseTimer pt_(ctx, PH_ADJOINT);
     // Word 1 of the status buffer (word 0 belongs to the edge fill guard).
     int* missing_flag = ctx.dstatus.as<int>() + 1;
     if ((err = cudaMemsetAsync(missing_flag, 0, 4, s))) return cuda_status(ctx, err, "status reset");
-    int32_t* twin = ctx.dvals[0].as<int32_t>();
+    double* v = ctx.dnet.as<double>();
     k_segment_starts<<<div_up(n + 1, tb), tb, 0, s>>>(rcv, m, n, ctx.droff.as<int64_t>());
-    k_find_twins<<<div_up(m, tb), tb, 0, s>>>(m, ctx.droff.as<int64_t>(), snd, rcv, twin, missing_flag);
+    if (coords)
+        k_edge_net<T, D, true><<<div_up(m, tb), tb, 0, s>>>(m, ctx.droff.as<int64_t>(), snd, rcv, nullptr, nullptr,
+                                                             (const T*)coords, (const T*)d_disp, (const T*)d_dist, r,
+                                                             inv_r, v, missing_flag);
+    else
+        k_edge_net<T, D, false><<<div_up(m, tb), tb, 0, s>>>(m, ctx.droff.as<int64_t>(), snd, rcv,
+                                                              (const T*)rel_disp, (const T*)rel_dist, nullptr,
+                                                              (const T*)d_disp, (const T*)d_dist, r, inv_r, v,
+                                                              missing_flag);
     ctx.kernel_launches += 2;
     int missing = 0;
     if ((err = cudaMemcpyAsync(&missing, missing_flag, 4, cudaMemcpyDeviceToHost, s)) ||
@@ -194,15 +206,7 @@ int twins_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_
         return cuda_status(ctx, err, "adjoint");
     *ok = missing == 0;
     if (!*ok) return OK;
-    if (coords)
-        k_grad_twins<T, D, true><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), snd, twin, nullptr, nullptr,
-                                                               (const T*)coords, (const T*)d_disp, (const T*)d_dist,
-                                                               r, inv_r, (T*)grad);
-    else
-        k_grad_twins<T, D, false><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), snd, twin,
-                                                                (const T*)rel_disp, (const T*)rel_dist, nullptr,
-                                                                (const T*)d_disp, (const T*)d_dist, r, inv_r,
-                                                                (T*)grad);
+    k_sum_segments<T, D><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), v, (T*)grad);
     ctx.kernel_launches += 1;
     return cuda_status(ctx, cudaGetLastError(), "adjoint launch");
 }

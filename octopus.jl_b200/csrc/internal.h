@@ -133,6 +133,7 @@ struct Ctx {
     int64_t plan_edges = -1;
     // Adjoint scratch (diff.cu).
     DevBuf dkeys[2], dvals[2], dhist, dsort_tmp, droff, dsoff;
+    DevBuf dnet;         // double per edge and axis: net adjoint contribution
     // Profiler.
     int64_t kernel_launches = 0;  // every kernel this context has launched
     bool profiling = false;
