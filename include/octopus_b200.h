@@ -96,10 +96,21 @@ OCT_API int oct_tree_destroy(oct_tree* tree);
  * (ext/OctopusCUDAExt.jl:214-248) and reproduces the CPU build
  * (src/api.jl:194-250) exactly.  `coords` is read during the call only.
  * keep_morton != 0 retains the per-point Morton codes (set_refit_mode!,
- * src/api.jl:43-47).  Returns OCT_ERR_INEXACT where the reference's
- * floor(Int32, ...) throws InexactError (non-finite or out-of-range cell). */
+ * src/api.jl:43-47) and, from the second build of the same size and radius
+ * on, reuses the previous sorted order: keys are re-encoded in that order,
+ * the changed ones are sorted and merged in, and when none changed only the
+ * bounds are recomputed.  The result is identical to a full rebuild (the
+ * reference rebuilds fully on every run!, test/refit.jl:15-40).  Returns
+ * OCT_ERR_INEXACT where the reference's floor(Int32, ...) throws
+ * InexactError (non-finite or out-of-range cell). */
 OCT_API int oct_tree_build(oct_ctx* ctx, oct_tree* tree, const void* coords, int64_t n,
                            double radius, int keep_morton);
+
+/* How the last oct_tree_build ordered the points: *path = 0 full sort,
+ * 1 changed keys merged into the previous order, 2 no key changed (bounds
+ * only); *n_changed = keys changed since the previous build, or -1 when the
+ * previous order was not reusable.  No counterpart in the reference. */
+OCT_API int oct_tree_last_build(const oct_tree* tree, int* path, int64_t* n_changed);
 
 /* Batched run! for many independent point sets ("clouds") in one pass; no
  * counterpart in the reference, which builds one TNS per radius

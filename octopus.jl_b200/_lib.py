@@ -56,6 +56,7 @@ SIGNATURES = [
     ("oct_tree_build", I, [P, P, P, I64, D, I]),
     ("oct_tree_build_batch", I, [P, P, P, I64, P, P, C.c_int32]),
     ("oct_batch_edge_offsets", I, [P, P, P]),
+    ("oct_tree_last_build", I, [P, C.POINTER(I), C.POINTER(I64)]),
     ("oct_tree_n_nodes", I, [P, P, C.POINTER(I64)]),
     ("oct_tree_view_get", I, [P, P, C.POINTER(TreeView)]),
     ("oct_edges_count", I, [P, P, P, I, C.POINTER(I64)]),

@@ -157,6 +157,17 @@ class Octree:
                 pass
             self.handle = None
 
+    def last_build(self) -> tuple[int, int]:
+        """How the last run! ordered the points: (path, n_changed) with path
+        0 = full sort, 1 = changed keys merged into the previous order,
+        2 = no key changed (bounds only); n_changed = -1 when the previous
+        order was not reusable (refit mode off, first build, new size or
+        radius)."""
+        path, moved = C.c_int(), C.c_int64()
+        self._ctx.check(self._ctx.lib.oct_tree_last_build(self.handle, C.byref(path), C.byref(moved)),
+                        "last_build")
+        return int(path.value), int(moved.value)
+
     def view(self) -> _lib.TreeView:
         v = _lib.TreeView()
         self._ctx.bind_stream()

@@ -121,6 +121,24 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const T* __restrict__ coord
 }
 
 // ------------------------------------------------------------ 2. encode --
+// Morton key of one point's cell (src/cpu/bin_cpu.jl:12-31 with
+// src/morton.jl:13-60): floor((x - origin) * inv_cs) per axis, clamped to the
+// key's bits per axis, bit-interleaved with x in the lowest bit.
+template <class T, int D>
+__device__ __forceinline__ uint64_t cell_key(const T* __restrict__ x, const T* o, T inv_cs) {
+    constexpr int64_t cmax = (1LL << Dims<D>::bits) - 1;
+    uint64_t c[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const T v = mul_rn(sub_rn(x[d], o[d]), inv_cs);
+        int64_t ci = (int64_t)floor(v);
+        ci = ci < 0 ? 0 : (ci > cmax ? cmax : ci);
+        c[d] = (uint64_t)ci;
+    }
+    return (D == 3) ? ((split_by_3(c[2]) << 2) | (split_by_3(c[1]) << 1) | split_by_3(c[0]))
+                    : ((split_by_2(c[1]) << 1) | split_by_2(c[0]));
+}
+
 // bin_point + clamp + morton_encode (src/cpu/bin_cpu.jl:52-95).  The host has
 // already proven every cell index fits Int32 (the max coordinate bins last).
 template <class T, int D, class K>
@@ -140,17 +158,7 @@ __global__ void __launch_bounds__(kThreads) k_encode(const T* __restrict__ coord
         o[2] = (T)cp[2];
         inv_cs = (T)cp[3];
     }
-    constexpr int64_t cmax = (1LL << Dims<D>::bits) - 1;
-    uint64_t c[3] = {0, 0, 0};
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-        const T v = mul_rn(sub_rn(coords[D * i + d], o[d]), inv_cs);
-        int64_t ci = (int64_t)floor(v);
-        ci = ci < 0 ? 0 : (ci > cmax ? cmax : ci);
-        c[d] = (uint64_t)ci;
-    }
-    const uint64_t key = (D == 3) ? ((split_by_3(c[2]) << 2) | (split_by_3(c[1]) << 1) | split_by_3(c[0]))
-                                  : ((split_by_2(c[1]) << 1) | split_by_2(c[0]));
+    const uint64_t key = cell_key<T, D>(coords + D * i, o, inv_cs);
     keys[i] = bt.n_clouds ? (K)(((uint64_t)cloud << bt.kbits) | key) : (K)key;
     if (morton_out) morton_out[i] = key;
 }
@@ -619,11 +627,221 @@ __global__ void k_gather_edge_offsets(const int64_t* __restrict__ offsets, const
     if (c <= n_clouds) eoff[c] = offsets[coff[c]];
 }
 
+// ---------------------------------------------------- 10. time stepping --
+// Refit mode keeps the previous build's sorted keys and permutation.  Points
+// move little between steps, so most keys are unchanged: re-encoding every
+// point in the previous sorted order leaves the unchanged keys U still sorted
+// by (key, index).  The changed keys M are few; they are sorted by
+// (key, index) in shared-memory chunks, ranked across chunks, and merged with
+// U by binary search.  The merged order is exactly the stable sort of the new
+// keys (src/sort.jl:15-24), so the topology and everything after it are the
+// same as a full rebuild.  When no key changed, order and topology are kept
+// and only the bounds are recomputed.
+constexpr int kChunk = 2048;
+constexpr int64_t kMaxMerged = 65536;  // above this many changed keys a full sort is cheaper
+
+template <class K>
+__device__ __forceinline__ bool key_less(K ka, int32_t ia, K kb, int32_t ib) {
+    return ka < kb || (ka == kb && ia < ib);
+}
+
+// Number of entries of the (key, index)-sorted array (k, v)[0, len) below (key, idx).
+template <class K>
+__device__ __forceinline__ int64_t count_below(const K* __restrict__ k, const int32_t* __restrict__ v, int64_t len,
+                                               K key, int32_t idx) {
+    int64_t a = 0, b = len;
+    while (a < b) {
+        const int64_t mid = (a + b) >> 1;
+        if (key_less(k[mid], v[mid], key, idx)) a = mid + 1; else b = mid;
+    }
+    return a;
+}
+
+// Re-encodes point perm[p] at its previous sorted position p, flags a changed
+// key and counts the changes per block.  The origin comes from this build's
+// bounds reduce, with the host's arithmetic (src/cpu/bin_cpu.jl:22).
+template <class T, int D, class K>
+__global__ void __launch_bounds__(kThreads) k_resort_mark(const T* __restrict__ coords, int64_t n,
+                                                          const int32_t* __restrict__ perm, K* __restrict__ keys,
+                                                          T inv_cs, const OctHeader* __restrict__ hdr,
+                                                          uint8_t* __restrict__ changed, int32_t* __restrict__ blockcnt,
+                                                          uint64_t* __restrict__ morton_out) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int mv = 0;
+    if (p < n) {
+        T o[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int d = 0; d < D; ++d) o[d] = sub_rn((T)hdr->gmin[d], T(1e-6));
+        const int32_t i = perm[p];
+        const uint64_t key = cell_key<T, D>(coords + (int64_t)D * i, o, inv_cs);
+        mv = (K)key != keys[p];
+        keys[p] = (K)key;
+        changed[p] = (uint8_t)mv;
+        if (morton_out) morton_out[i] = key;
+    }
+    const int c = __syncthreads_count(mv);
+    if (threadIdx.x == 0) blockcnt[blockIdx.x] = c;
+}
+
+// Stable partition of the re-encoded positions: unchanged to (uk, uv) in
+// order, changed to (mk, mv) in order.  moved_before[b] counts the changed
+// positions before block b.
+template <class K>
+__global__ void __launch_bounds__(kThreads) k_resort_split(int64_t n, const K* __restrict__ keys,
+                                                           const int32_t* __restrict__ perm,
+                                                           const uint8_t* __restrict__ changed,
+                                                           const int64_t* __restrict__ moved_before,
+                                                           K* __restrict__ uk, int32_t* __restrict__ uv,
+                                                           K* __restrict__ mk, int32_t* __restrict__ mv) {
+    __shared__ int wsum[kThreads / 32];
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool c = p < n && changed[p];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned bal = __ballot_sync(0xffffffffu, c);
+    if (lane == 0) wsum[w] = __popc(bal);
+    __syncthreads();
+    int before = __popc(bal & lanemask_lt());
+    for (int j = 0; j < w; ++j) before += wsum[j];
+    if (p >= n) return;
+    const int64_t mb = moved_before[blockIdx.x] + before;
+    if (c) {
+        mk[mb] = keys[p];
+        mv[mb] = perm[p];
+    } else {
+        uk[p - mb] = keys[p];
+        uv[p - mb] = perm[p];
+    }
+}
+
+// Sorts each chunk of kChunk changed keys by (key, index) in shared memory
+// (bitonic network, one compare-exchange per thread and stage).
+template <class K>
+__global__ void __launch_bounds__(kChunk / 2) k_moved_sort(int64_t m, K* __restrict__ mk, int32_t* __restrict__ mv) {
+    __shared__ K sk[kChunk];
+    __shared__ int32_t sv[kChunk];
+    const int64_t base = (int64_t)blockIdx.x * kChunk;
+    for (int t = threadIdx.x; t < kChunk; t += blockDim.x) {
+        const int64_t j = base + t;
+        if (j < m) {
+            sk[t] = mk[j];
+            sv[t] = mv[j];
+        } else {
+            sk[t] = ~K(0);
+            sv[t] = INT32_MAX;  // above every real index: padding sorts last
+        }
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    for (int size = 2; size <= kChunk; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const int i = 2 * t - (t & (stride - 1));
+            const int j = i + stride;
+            const bool up = (i & size) == 0;
+            const K ki = sk[i], kj = sk[j];
+            const int32_t vi = sv[i], vj = sv[j];
+            if (key_less(kj, vj, ki, vi) == up) {
+                sk[i] = kj;
+                sk[j] = ki;
+                sv[i] = vj;
+                sv[j] = vi;
+            }
+            __syncthreads();
+        }
+    }
+    for (int t2 = threadIdx.x; t2 < kChunk; t2 += blockDim.x) {
+        const int64_t j = base + t2;
+        if (j < m) {
+            mk[j] = sk[t2];
+            mv[j] = sv[t2];
+        }
+    }
+}
+
+// Global rank of each changed key: its rank in its own chunk plus the number
+// of smaller keys in every other chunk.
+template <class K>
+__global__ void __launch_bounds__(kThreads) k_moved_rank(int64_t m, const K* __restrict__ ck,
+                                                         const int32_t* __restrict__ cv, K* __restrict__ sk,
+                                                         int32_t* __restrict__ sv) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const K key = ck[j];
+    const int32_t idx = cv[j];
+    const int64_t own = j / kChunk;
+    int64_t r = j - own * kChunk;
+    const int64_t nchunks = (m + kChunk - 1) / kChunk;
+    for (int64_t c = 0; c < nchunks; ++c) {
+        if (c == own) continue;
+        const int64_t b = c * kChunk;
+        r += count_below(ck + b, cv + b, m - b < kChunk ? m - b : (int64_t)kChunk, key, idx);
+    }
+    sk[r] = key;
+    sv[r] = idx;
+}
+
+// Merges U (n - m entries) and M (m entries) into the final sorted keys and
+// permutation, and gathers the sorted points (the gather of section 4).
+template <class T, int D, class K>
+__global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, int64_t m, const K* __restrict__ uk,
+                                                           const int32_t* __restrict__ uv, const K* __restrict__ mk,
+                                                           const int32_t* __restrict__ mv, const T* __restrict__ coords,
+                                                           K* __restrict__ okeys, int32_t* __restrict__ operm,
+                                                           SPt<T, D>* __restrict__ spts) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int64_t nu = n - m;
+    K key;
+    int32_t idx;
+    int64_t pos;
+    if (t < nu) {
+        key = uk[t];
+        idx = uv[t];
+        pos = t + count_below(mk, mv, m, key, idx);
+    } else {
+        const int64_t j = t - nu;
+        key = mk[j];
+        idx = mv[j];
+        pos = j + count_below(uk, uv, nu, key, idx);
+    }
+    okeys[pos] = key;
+    operm[pos] = idx;
+    SPt<T, D> sp;
+#pragma unroll
+    for (int d = 0; d < D; ++d) sp.x[d] = coords[(int64_t)D * idx + d];
+    sp.idx = idx;
+    spts[pos] = sp;
+}
+
+// Bounds-only step (no key changed): the topology is kept; reset the refit
+// arrival counters and preset the full-range nodes from this build's reduce.
+template <class T, int D>
+__global__ void __launch_bounds__(kThreads) k_refit_prepare(int64_t nn, int64_t n, TNode<T, D>* __restrict__ tnode,
+                                                            const int2* __restrict__ nrange,
+                                                            int32_t* __restrict__ arrive, OctHeader* hdr,
+                                                            int64_t n_groups, int32_t dfs_start) {
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id == 0) {
+        hdr->n_nodes = nn;
+        hdr->n_groups = n_groups;
+        hdr->dfs_start = dfs_start;
+    }
+    if (id >= nn) return;
+    arrive[id] = 0;
+    const int2 rg = nrange[id];
+    if (rg.x == 0 && (int64_t)rg.y == n - 1) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            tnode[id].lo[d] = (T)hdr->gmin[d];
+            tnode[id].hi[d] = (T)hdr->gmax[d];
+        }
+    }
+}
+
 // ------------------------------------------------------------- host side --
 namespace {
 
 template <class T, int D, class K>
-int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
+int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_t moved = -1, int prev = -1) {
     const Batch bt = t.batch();
     cudaStream_t s = ctx.stream;
     cudaError_t err;
@@ -633,42 +851,108 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
     T o[3] = {T(0), T(0), T(0)};
     for (int d = 0; d < D; ++d) o[d] = (T)t.origin[d];
 
-    // --- encode
-    if ((err = ensure(t.keys[0], (size_t)n * sizeof(K))) || (err = ensure(t.keys[1], (size_t)n * sizeof(K))) ||
-        (err = ensure(t.vals[0], (size_t)n * 4)) || (err = ensure(t.vals[1], (size_t)n * 4)))
-        return cuda_status(ctx, err, "allocating sort buffers");
-    uint64_t* morton = nullptr;
-    if (t.keep_morton) {
-        if ((err = ensure(t.morton, (size_t)n * 8))) return cuda_status(ctx, err, "allocating morton codes");
-        morton = t.morton.as<uint64_t>();
-    }
-    {
-        PhaseTimer pt_(ctx, PH_ENCODE);
-        k_encode<T, D, K><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, n, o[0], o[1], o[2], inv_cs,
-                                                                    t.keys[0].as<K>(), morton, bt);
-        ctx.kernel_launches += 1;
-    }
-
-    // --- sort (stable: ties keep ascending original index, src/sort.jl:15-24)
-    if ((err = ensure(t.hist, sort_hist_bytes(n))) || (err = ensure(t.sort_tmp, sort_scan_bytes(n))))
-        return cuda_status(ctx, err, "allocating histograms");
-    K* kb[2] = {t.keys[0].as<K>(), t.keys[1].as<K>()};
-    int32_t* vb[2] = {t.vals[0].as<int32_t>(), t.vals[1].as<int32_t>()};
-    int src;
-    {
-        PhaseTimer pt_(ctx, PH_SORT);
-        src = radix_sort_pairs<K>(kb, vb, t.hist.as<int32_t>(), t.sort_tmp.as<int64_t>(), n, t.key_bits, false, s);
-        ctx.kernel_launches += 5 * t.sort_passes;
-    }
-    const K* skeys = kb[src];
-    const int32_t* perm = t.sort_passes ? vb[src] : nullptr;
-
-    // --- sorted points
     if ((err = ensure(t.spts, (size_t)n * sizeof(SPt<T, D>)))) return cuda_status(ctx, err, "allocating points");
-    {
-        PhaseTimer pt_(ctx, PH_GATHER);
-        k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, perm, n, t.spts.as<SPt<T, D>>());
-        ctx.kernel_launches += 1;
+    OctHeader* hdr = t.hdr.as<OctHeader>();
+    const K* skeys;
+    const int32_t* perm;
+    int sorted = -1;  // buffer holding this build's sorted keys and permutation
+    if (moved < 0) {
+        // --- encode
+        if ((err = ensure(t.keys[0], (size_t)n * sizeof(K))) || (err = ensure(t.keys[1], (size_t)n * sizeof(K))) ||
+            (err = ensure(t.vals[0], (size_t)n * 4)) || (err = ensure(t.vals[1], (size_t)n * 4)))
+            return cuda_status(ctx, err, "allocating sort buffers");
+        uint64_t* morton = nullptr;
+        if (t.keep_morton) {
+            if ((err = ensure(t.morton, (size_t)n * 8))) return cuda_status(ctx, err, "allocating morton codes");
+            morton = t.morton.as<uint64_t>();
+        }
+        {
+            PhaseTimer pt_(ctx, PH_ENCODE);
+            k_encode<T, D, K><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, n, o[0], o[1], o[2], inv_cs,
+                                                                        t.keys[0].as<K>(), morton, bt);
+            ctx.kernel_launches += 1;
+        }
+
+        // --- sort (stable: ties keep ascending original index, src/sort.jl:15-24)
+        if ((err = ensure(t.hist, sort_hist_bytes(n))) || (err = ensure(t.sort_tmp, sort_scan_bytes(n))))
+            return cuda_status(ctx, err, "allocating histograms");
+        K* kb[2] = {t.keys[0].as<K>(), t.keys[1].as<K>()};
+        int32_t* vb[2] = {t.vals[0].as<int32_t>(), t.vals[1].as<int32_t>()};
+        int src;
+        {
+            PhaseTimer pt_(ctx, PH_SORT);
+            src = radix_sort_pairs<K>(kb, vb, t.hist.as<int32_t>(), t.sort_tmp.as<int64_t>(), n, t.key_bits, false,
+                                      s);
+            ctx.kernel_launches += 5 * t.sort_passes;
+        }
+        skeys = kb[src];
+        perm = t.sort_passes ? vb[src] : nullptr;
+        if (perm && !bt.n_clouds) sorted = src;
+
+        // --- sorted points
+        {
+            PhaseTimer pt_(ctx, PH_GATHER);
+            k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, perm, n, t.spts.as<SPt<T, D>>());
+            ctx.kernel_launches += 1;
+        }
+        t.last_path = 0;
+    } else {
+        // Refit mode, keys already re-encoded in the previous order (section 10).
+        K* kp = t.keys[prev].as<K>();
+        int32_t* vp = t.vals[prev].as<int32_t>();
+        skeys = kp;
+        perm = vp;
+        sorted = prev;
+        if (moved == 0) {
+            // Same keys, same order, same topology: new bounds only.
+            {
+                PhaseTimer pt_(ctx, PH_GATHER);
+                k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, vp, n, t.spts.as<SPt<T, D>>());
+                ctx.kernel_launches += 1;
+            }
+            {
+                PhaseTimer pt_(ctx, PH_REFIT);
+                const int nb = div_up(t.n_nodes, kThreads);
+                k_refit_prepare<T, D><<<nb, kThreads, 0, s>>>(t.n_nodes, n, t.tnode.as<TNode<T, D>>(),
+                                                               t.nrange.as<int2>(), t.arrive.as<int32_t>(), hdr,
+                                                               t.n_groups, t.dfs_start);
+                k_refit<T, D><<<nb, kThreads, 0, s>>>(t.capacity, n, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
+                                                       t.parent.as<int32_t>(), t.arrive.as<int32_t>(),
+                                                       t.spts.as<SPt<T, D>>(), hdr, bt);
+                ctx.kernel_launches += 2;
+            }
+            if ((err = cudaGetLastError())) return cuda_status(ctx, err, "bounds refit");
+            t.last_path = 2;
+            t.sorted_buf = sorted;
+            return OK;
+        }
+        const int nb = div_up(n, kThreads);
+        const int64_t nchunks = div_up(moved, kChunk);
+        if ((err = ensure(t.mkeys, (size_t)moved * sizeof(K))) || (err = ensure(t.mvals, (size_t)moved * 4)) ||
+            (err = ensure(t.mkeys2, (size_t)moved * sizeof(K))) || (err = ensure(t.mvals2, (size_t)moved * 4)))
+            return cuda_status(ctx, err, "allocating changed keys");
+        K* uk = t.keys[1 - prev].as<K>();
+        int32_t* uv = t.vals[1 - prev].as<int32_t>();
+        K* mk = t.mkeys.as<K>();
+        int32_t* mv = t.mvals.as<int32_t>();
+        {
+            PhaseTimer pt_(ctx, PH_SORT);
+            k_resort_split<K><<<nb, kThreads, 0, s>>>(n, kp, vp, t.rflag.as<uint8_t>(), t.roff.as<int64_t>(), uk, uv,
+                                                      mk, mv);
+            k_moved_sort<K><<<(unsigned)nchunks, kChunk / 2, 0, s>>>(moved, mk, mv);
+            ctx.kernel_launches += 2;
+            if (nchunks > 1) {
+                k_moved_rank<K><<<div_up(moved, kThreads), kThreads, 0, s>>>(moved, mk, mv, t.mkeys2.as<K>(),
+                                                                              t.mvals2.as<int32_t>());
+                mk = t.mkeys2.as<K>();
+                mv = t.mvals2.as<int32_t>();
+                ctx.kernel_launches += 1;
+            }
+            k_resort_merge<T, D, K><<<nb, kThreads, 0, s>>>(n, moved, uk, uv, mk, mv, coords, kp, vp,
+                                                             t.spts.as<SPt<T, D>>());
+            ctx.kernel_launches += 1;
+        }
+        t.last_path = 1;
     }
 
     // --- topology + refit (retried once with the exact node count on overflow)
@@ -681,7 +965,6 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
         return cuda_status(ctx, err, "allocating topology scratch");
     int64_t est = (int64_t)Dims<D>::nch * ((n + 31) / 32) + 2 * NLEV + 64;
     if (t.capacity < est) t.capacity = est;
-    OctHeader* hdr = t.hdr.as<OctHeader>();
     for (int attempt = 0; attempt < 3; ++attempt) {
         const int64_t cap = t.capacity;
         if ((err = ensure(t.tnode, (size_t)cap * sizeof(TNode<T, D>))) || (err = ensure(t.nrange, (size_t)cap * 8)) ||
@@ -744,9 +1027,31 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius) {
         t.n_nodes = t.hdr_host->n_nodes;
         t.n_groups = t.hdr_host->n_groups;
         t.dfs_start = t.hdr_host->dfs_start;
+        t.sorted_buf = sorted;
         return OK;
     }
     return set_error(ctx, ERR_OVERFLOW, "tree build: node capacity retry did not converge");
+}
+
+// Refit mode: re-encodes every point at its previous sorted position and
+// counts the changed keys into hdr->n_moved (read with the bounds).
+template <class T, int D, class K>
+int resort_mark(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int prev) {
+    cudaStream_t s = ctx.stream;
+    cudaError_t err;
+    const int nb = div_up(n, kThreads);
+    if ((err = ensure(t.rflag, (size_t)n)) || (err = ensure(t.rcnt, (size_t)nb * 4)) ||
+        (err = ensure(t.roff, (size_t)(nb + 1) * 8)) || (err = ensure(t.scan_tmp, (size_t)scan_tmp_elems(nb) * 8)) ||
+        (t.keep_morton && (err = ensure(t.morton, (size_t)n * 8))))
+        return cuda_status(ctx, err, "allocating refit-mode scratch");
+    OctHeader* hdr = t.hdr.as<OctHeader>();
+    PhaseTimer pt_(ctx, PH_ENCODE);
+    k_resort_mark<T, D, K><<<nb, kThreads, 0, s>>>(coords, n, t.vals[prev].as<int32_t>(), t.keys[prev].as<K>(),
+                                                    T(1) / radius, hdr, t.rflag.as<uint8_t>(), t.rcnt.as<int32_t>(),
+                                                    t.keep_morton ? t.morton.as<uint64_t>() : nullptr);
+    exclusive_scan_i32_i64(t.rcnt.as<int32_t>(), t.roff.as<int64_t>(), nb, &hdr->n_moved, t.scan_tmp.as<int64_t>(), s);
+    ctx.kernel_launches += 4;
+    return OK;
 }
 
 template <class T, int D>
@@ -768,6 +1073,16 @@ int build_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, double radius_d) 
         PhaseTimer pt_(ctx, PH_BOUNDS);
         k_bounds<T, D><<<nb, kThreads, 0, s>>>(coords, n, t.partials.as<double>(), hdr);
         ctx.kernel_launches += 1;
+    }
+    // Refit mode with a reusable previous order: re-encode in that order now,
+    // so the count of changed keys arrives with the bounds.
+    const int prev = t.sorted_buf;
+    t.sorted_buf = -1;
+    const bool try_resort = t.keep_morton && prev >= 0 && t.sorted_n == n && t.sorted_radius == radius_d;
+    if (try_resort) {
+        const int st = t.sorted_key_bytes == 4 ? resort_mark<T, D, uint32_t>(ctx, t, coords, n, radius, prev)
+                                               : resort_mark<T, D, uint64_t>(ctx, t, coords, n, radius, prev);
+        if (st != OK) return st;
     }
     if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
         (err = cudaStreamSynchronize(s)))
@@ -795,8 +1110,22 @@ int build_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, double radius_d) 
     t.key_bits = D * nbits_axis;
     t.key_bytes = t.key_bits <= 32 ? 4 : 8;
     t.sort_passes = (t.key_bits + 7) / 8;
-    if (t.key_bytes == 4) return run_pipeline<T, D, uint32_t>(ctx, t, coords, n, radius);
-    return run_pipeline<T, D, uint64_t>(ctx, t, coords, n, radius);
+    // Merge the changed keys into the previous order unless they are so many
+    // that a full sort is cheaper (or the key width changed).
+    int64_t moved = -1;
+    t.last_moved = try_resort ? t.hdr_host->n_moved : -1;
+    if (try_resort && t.key_bytes == t.sorted_key_bytes) {
+        const int64_t cap = std::min<int64_t>(kMaxMerged, std::max<int64_t>(kChunk, n / 8));
+        if (t.hdr_host->n_moved <= cap) moved = t.hdr_host->n_moved;
+    }
+    const int st = t.key_bytes == 4 ? run_pipeline<T, D, uint32_t>(ctx, t, coords, n, radius, moved, prev)
+                                    : run_pipeline<T, D, uint64_t>(ctx, t, coords, n, radius, moved, prev);
+    if (st == OK && t.sorted_buf >= 0) {
+        t.sorted_n = n;
+        t.sorted_radius = radius_d;
+        t.sorted_key_bytes = t.key_bytes;
+    }
+    return st;
 }
 
 template <class T, int D>
@@ -872,6 +1201,7 @@ int build_batch_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, const int64
 
 int build_tree_batch(Ctx& ctx, Tree& t, const void* coords, int64_t n, const int64_t* coff_host,
                      const double* radii_host, int32_t n_clouds) {
+    t.sorted_buf = -1;
     t.built = false;
     t.view_valid = false;
     t.n = n;
@@ -923,6 +1253,7 @@ int build_tree(Ctx& ctx, Tree& t, const void* coords, int64_t n, double radius) 
     ++t.generation;
     if (n == 0) {
         t.n_nodes = 0;
+        t.sorted_buf = -1;
         t.built = true;
         return OK;
     }

@@ -244,6 +244,13 @@ OCT_API int oct_batch_edge_offsets(oct_ctx* ctx, oct_tree* tree, int64_t* edge_o
     return oct::batch_edge_offsets(ctx->c, tree->t, edge_offsets);
 }
 
+OCT_API int oct_tree_last_build(const oct_tree* tree, int* path, int64_t* n_changed) {
+    if (!tree || !path || !n_changed) return OCT_ERR_ARGUMENT;
+    *path = tree->t.last_path;
+    *n_changed = tree->t.last_moved;
+    return OCT_OK;
+}
+
 OCT_API int oct_tree_n_nodes(oct_ctx* ctx, const oct_tree* tree, int64_t* n_nodes) {
     if (!ctx || !tree || !n_nodes) return OCT_ERR_ARGUMENT;
     *n_nodes = tree->t.built ? tree->t.n_nodes : 0;

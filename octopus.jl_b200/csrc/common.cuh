@@ -69,6 +69,7 @@ struct OctHeader {
     int64_t n_groups;
     int32_t dfs_start;  // first node of the DFS below the root's single-child chain
     int32_t pad2;
+    int64_t n_moved;    // refit mode: keys that changed since the previous build
 };
 
 // Packed pairs of floats with per-element IEEE round-to-nearest (sm_100+).

@@ -88,6 +88,19 @@ struct Tree {
     int32_t dfs_start = 0;
     DevBuf chain;                // int32[64]: full-range chain node ids and flags
 
+    // Refit mode across time steps: the previous build's sorted keys and
+    // permutation (keys[sorted_buf], vals[sorted_buf]) seed the next build.
+    int sorted_buf = -1;         // -1: no reusable order
+    int64_t sorted_n = 0;
+    double sorted_radius = 0.0;
+    int sorted_key_bytes = 0;
+    DevBuf rflag;                // uint8 per position: key changed
+    DevBuf rcnt, roff;           // int32 per block / int64 scan (+1)
+    DevBuf mkeys, mvals;         // changed keys, sorted in chunks
+    DevBuf mkeys2, mvals2;       // changed keys, fully sorted
+    int last_path = 0;           // 0 full sort, 1 merge of changed keys, 2 bounds only
+    int64_t last_moved = -1;
+
     // Batched build (many clouds in one forest); n_clouds == 0 otherwise.
     int32_t n_clouds = 0;
     int32_t kbits = 0;
