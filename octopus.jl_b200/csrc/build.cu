@@ -630,13 +630,16 @@ __global__ void k_gather_edge_offsets(const int64_t* __restrict__ offsets, const
 // ---------------------------------------------------- 10. time stepping --
 // Refit mode keeps the previous build's sorted keys and permutation.  Points
 // move little between steps, so most keys are unchanged: re-encoding every
-// point in the previous sorted order leaves the unchanged keys U still sorted
-// by (key, index).  The changed keys M are few; they are sorted by
-// (key, index) in shared-memory chunks, ranked across chunks, and merged with
-// U by binary search.  The merged order is exactly the stable sort of the new
-// keys (src/sort.jl:15-24), so the topology and everything after it are the
-// same as a full rebuild.  When no key changed, order and topology are kept
-// and only the bounds are recomputed.
+// point at its previous sorted position leaves the unchanged keys U sorted by
+// (key, index) in place.  The changed keys M are few; they are collected,
+// sorted by (key, index) in shared-memory chunks and ranked across chunks,
+// then merged with U: an unchanged key at position p lands at
+// (p - changed keys before p) + (keys of M below it), and the keys of M that
+// fall between two consecutive unchanged keys are placed by the first of
+// the two.  The merged order is exactly the stable sort of the new keys
+// (src/sort.jl:15-24), so the topology and everything after it equal a full
+// rebuild.  When no key changed, order and topology are kept and only the
+// bounds are recomputed.
 constexpr int kChunk = 2048;
 constexpr int64_t kMaxMerged = 65536;  // above this many changed keys a full sort is cheaper
 
@@ -658,69 +661,60 @@ __device__ __forceinline__ int64_t count_below(const K* __restrict__ k, const in
 }
 
 // Re-encodes point perm[p] at its previous sorted position p, flags a changed
-// key and counts the changes per block.  The origin comes from this build's
-// bounds reduce, with the host's arithmetic (src/cpu/bin_cpu.jl:22).
+// key, counts the changes per block and appends the changed (key, index)
+// pairs to (mk, mv) in any order (slots past `cap` are counted, not
+// written).  The origin comes from this build's bounds reduce, with the
+// host's arithmetic (src/cpu/bin_cpu.jl:22).
 template <class T, int D, class K>
 __global__ void __launch_bounds__(kThreads) k_resort_mark(const T* __restrict__ coords, int64_t n,
-                                                          const int32_t* __restrict__ perm, K* __restrict__ keys,
-                                                          T inv_cs, const OctHeader* __restrict__ hdr,
+                                                          const int32_t* __restrict__ perm,
+                                                          const K* __restrict__ keys, T inv_cs, OctHeader* hdr,
                                                           uint8_t* __restrict__ changed, int32_t* __restrict__ blockcnt,
+                                                          K* __restrict__ mk, int32_t* __restrict__ mv, int64_t cap,
                                                           uint64_t* __restrict__ morton_out) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int mv = 0;
+    bool c = false;
+    K nk = 0;
+    int32_t i = 0;
     if (p < n) {
         T o[3] = {T(0), T(0), T(0)};
 #pragma unroll
         for (int d = 0; d < D; ++d) o[d] = sub_rn((T)hdr->gmin[d], T(1e-6));
-        const int32_t i = perm[p];
+        i = perm[p];
         const uint64_t key = cell_key<T, D>(coords + (int64_t)D * i, o, inv_cs);
-        mv = (K)key != keys[p];
-        keys[p] = (K)key;
-        changed[p] = (uint8_t)mv;
+        nk = (K)key;
+        c = nk != keys[p];
+        changed[p] = (uint8_t)c;
         if (morton_out) morton_out[i] = key;
     }
-    const int c = __syncthreads_count(mv);
-    if (threadIdx.x == 0) blockcnt[blockIdx.x] = c;
-}
-
-// Stable partition of the re-encoded positions: unchanged to (uk, uv) in
-// order, changed to (mk, mv) in order.  moved_before[b] counts the changed
-// positions before block b.
-template <class K>
-__global__ void __launch_bounds__(kThreads) k_resort_split(int64_t n, const K* __restrict__ keys,
-                                                           const int32_t* __restrict__ perm,
-                                                           const uint8_t* __restrict__ changed,
-                                                           const int64_t* __restrict__ moved_before,
-                                                           K* __restrict__ uk, int32_t* __restrict__ uv,
-                                                           K* __restrict__ mk, int32_t* __restrict__ mv) {
-    __shared__ int wsum[kThreads / 32];
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool c = p < n && changed[p];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned bal = __ballot_sync(0xffffffffu, c);
-    if (lane == 0) wsum[w] = __popc(bal);
-    __syncthreads();
-    int before = __popc(bal & lanemask_lt());
-    for (int j = 0; j < w; ++j) before += wsum[j];
-    if (p >= n) return;
-    const int64_t mb = moved_before[blockIdx.x] + before;
-    if (c) {
-        mk[mb] = keys[p];
-        mv[mb] = perm[p];
-    } else {
-        uk[p - mb] = keys[p];
-        uv[p - mb] = perm[p];
+    if (bal) {
+        const int lane = threadIdx.x & 31;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd((unsigned long long*)&hdr->n_moved, (unsigned long long)__popc(bal));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (c) {
+            const int64_t slot = (int64_t)base + __popc(bal & lanemask_lt());
+            if (slot < cap) {
+                mk[slot] = nk;
+                mv[slot] = i;
+            }
+        }
     }
+    const int cnt = __syncthreads_count(c);
+    if (threadIdx.x == 0) blockcnt[blockIdx.x] = cnt;
 }
 
-// Sorts each chunk of kChunk changed keys by (key, index) in shared memory
-// (bitonic network, one compare-exchange per thread and stage).
+// Sorts each chunk of up to kChunk changed keys by (key, index) in shared
+// memory: a bitonic network of `width` (a power of two, blockDim.x * 2)
+// entries, one compare-exchange per thread and stage.
 template <class K>
-__global__ void __launch_bounds__(kChunk / 2) k_moved_sort(int64_t m, K* __restrict__ mk, int32_t* __restrict__ mv) {
+__global__ void __launch_bounds__(kChunk / 2) k_moved_sort(int64_t m, int width, K* __restrict__ mk,
+                                                           int32_t* __restrict__ mv) {
     __shared__ K sk[kChunk];
     __shared__ int32_t sv[kChunk];
     const int64_t base = (int64_t)blockIdx.x * kChunk;
-    for (int t = threadIdx.x; t < kChunk; t += blockDim.x) {
+    for (int t = threadIdx.x; t < width; t += blockDim.x) {
         const int64_t j = base + t;
         if (j < m) {
             sk[t] = mk[j];
@@ -732,7 +726,7 @@ __global__ void __launch_bounds__(kChunk / 2) k_moved_sort(int64_t m, K* __restr
     }
     __syncthreads();
     const int t = threadIdx.x;
-    for (int size = 2; size <= kChunk; size <<= 1) {
+    for (int size = 2; size <= width; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
             const int i = 2 * t - (t & (stride - 1));
             const int j = i + stride;
@@ -748,7 +742,7 @@ __global__ void __launch_bounds__(kChunk / 2) k_moved_sort(int64_t m, K* __restr
             __syncthreads();
         }
     }
-    for (int t2 = threadIdx.x; t2 < kChunk; t2 += blockDim.x) {
+    for (int t2 = threadIdx.x; t2 < width; t2 += blockDim.x) {
         const int64_t j = base + t2;
         if (j < m) {
             mk[j] = sk[t2];
@@ -779,30 +773,10 @@ __global__ void __launch_bounds__(kThreads) k_moved_rank(int64_t m, const K* __r
     sv[r] = idx;
 }
 
-// Merges U (n - m entries) and M (m entries) into the final sorted keys and
-// permutation, and gathers the sorted points (the gather of section 4).
 template <class T, int D, class K>
-__global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, int64_t m, const K* __restrict__ uk,
-                                                           const int32_t* __restrict__ uv, const K* __restrict__ mk,
-                                                           const int32_t* __restrict__ mv, const T* __restrict__ coords,
-                                                           K* __restrict__ okeys, int32_t* __restrict__ operm,
-                                                           SPt<T, D>* __restrict__ spts) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int64_t nu = n - m;
-    K key;
-    int32_t idx;
-    int64_t pos;
-    if (t < nu) {
-        key = uk[t];
-        idx = uv[t];
-        pos = t + count_below(mk, mv, m, key, idx);
-    } else {
-        const int64_t j = t - nu;
-        key = mk[j];
-        idx = mv[j];
-        pos = j + count_below(uk, uv, nu, key, idx);
-    }
+__device__ __forceinline__ void put_sorted(int64_t pos, K key, int32_t idx, const T* __restrict__ coords,
+                                           K* __restrict__ okeys, int32_t* __restrict__ operm,
+                                           SPt<T, D>* __restrict__ spts) {
     okeys[pos] = key;
     operm[pos] = idx;
     SPt<T, D> sp;
@@ -810,6 +784,60 @@ __global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, int64_t m,
     for (int d = 0; d < D; ++d) sp.x[d] = coords[(int64_t)D * idx + d];
     sp.idx = idx;
     spts[pos] = sp;
+}
+
+// Merges the unchanged keys (in place at their previous positions) with the
+// sorted changed keys (mk, mv)[0, m) into (okeys, operm), and gathers the
+// sorted points (the gather of section 4).  changed_before[b] counts the
+// changed positions before block b.
+template <class T, int D, class K>
+__global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, int64_t m, const K* __restrict__ keys,
+                                                           const int32_t* __restrict__ perm,
+                                                           const uint8_t* __restrict__ changed,
+                                                           const int64_t* __restrict__ changed_before,
+                                                           const K* __restrict__ mk, const int32_t* __restrict__ mv,
+                                                           const T* __restrict__ coords, K* __restrict__ okeys,
+                                                           int32_t* __restrict__ operm, SPt<T, D>* __restrict__ spts) {
+    __shared__ int wsum[kThreads / 32];
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m == n) {  // every key changed: the sorted changed keys are the result
+        if (p < n) put_sorted<T, D, K>(p, mk[p], mv[p], coords, okeys, operm, spts);
+        return;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool in = p < n;
+    const bool c = in && changed[p];
+    const bool u = in && !c;
+    const unsigned cbal = __ballot_sync(0xffffffffu, c);
+    const unsigned ubal = __ballot_sync(0xffffffffu, u);
+    if (lane == 0) wsum[w] = __popc(cbal);
+    __syncthreads();
+    int before = __popc(cbal & lanemask_lt());
+    for (int j = 0; j < w; ++j) before += wsum[j];
+    K key = 0;
+    int32_t idx = 0;
+    int64_t s = 0;
+    if (u) {
+        key = keys[p];
+        idx = perm[p];
+        s = count_below(mk, mv, m, key, idx);
+    }
+    // Changed keys below the next unchanged key: from the next unchanged lane
+    // of this warp, or found past the warp's end.
+    const unsigned later = ubal & ~((2u << lane) - 1u);
+    const int src = later ? __ffs(later) - 1 : lane;
+    int64_t sn = __shfl_sync(0xffffffffu, s, src);
+    if (!u) return;
+    if (!later) {
+        int64_t q = p - lane + 32;
+        while (q < n && changed[q]) ++q;
+        sn = q < n ? count_below(mk, mv, m, keys[q], perm[q]) : m;
+    }
+    const int64_t ui = p - (changed_before[blockIdx.x] + before);  // rank among unchanged keys
+    put_sorted<T, D, K>(ui + s, key, idx, coords, okeys, operm, spts);
+    for (int64_t j = s; j < sn; ++j) put_sorted<T, D, K>(j + ui + 1, mk[j], mv[j], coords, okeys, operm, spts);
+    if (ui == 0)
+        for (int64_t j = 0; j < s; ++j) put_sorted<T, D, K>(j, mk[j], mv[j], coords, okeys, operm, spts);
 }
 
 // Bounds-only step (no key changed): the topology is kept; reset the refit
@@ -882,8 +910,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         {
             PhaseTimer pt_(ctx, PH_SORT);
             src = radix_sort_pairs<K>(kb, vb, t.hist.as<int32_t>(), t.sort_tmp.as<int64_t>(), n, t.key_bits, false,
-                                      s);
-            ctx.kernel_launches += 5 * t.sort_passes;
+                                      s, &ctx.kernel_launches);
         }
         skeys = kb[src];
         perm = t.sort_passes ? vb[src] : nullptr;
@@ -928,19 +955,18 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         }
         const int nb = div_up(n, kThreads);
         const int64_t nchunks = div_up(moved, kChunk);
-        if ((err = ensure(t.mkeys, (size_t)moved * sizeof(K))) || (err = ensure(t.mvals, (size_t)moved * 4)) ||
-            (err = ensure(t.mkeys2, (size_t)moved * sizeof(K))) || (err = ensure(t.mvals2, (size_t)moved * 4)))
+        int width = 64;
+        while (width < moved && width < kChunk) width <<= 1;
+        if ((err = ensure(t.mkeys2, (size_t)moved * sizeof(K))) || (err = ensure(t.mvals2, (size_t)moved * 4)))
             return cuda_status(ctx, err, "allocating changed keys");
-        K* uk = t.keys[1 - prev].as<K>();
-        int32_t* uv = t.vals[1 - prev].as<int32_t>();
         K* mk = t.mkeys.as<K>();
         int32_t* mv = t.mvals.as<int32_t>();
+        K* ok = t.keys[1 - prev].as<K>();
+        int32_t* ov = t.vals[1 - prev].as<int32_t>();
         {
             PhaseTimer pt_(ctx, PH_SORT);
-            k_resort_split<K><<<nb, kThreads, 0, s>>>(n, kp, vp, t.rflag.as<uint8_t>(), t.roff.as<int64_t>(), uk, uv,
-                                                      mk, mv);
-            k_moved_sort<K><<<(unsigned)nchunks, kChunk / 2, 0, s>>>(moved, mk, mv);
-            ctx.kernel_launches += 2;
+            k_moved_sort<K><<<(unsigned)nchunks, width / 2, 0, s>>>(moved, width, mk, mv);
+            ctx.kernel_launches += 1;
             if (nchunks > 1) {
                 k_moved_rank<K><<<div_up(moved, kThreads), kThreads, 0, s>>>(moved, mk, mv, t.mkeys2.as<K>(),
                                                                               t.mvals2.as<int32_t>());
@@ -948,10 +974,14 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
                 mv = t.mvals2.as<int32_t>();
                 ctx.kernel_launches += 1;
             }
-            k_resort_merge<T, D, K><<<nb, kThreads, 0, s>>>(n, moved, uk, uv, mk, mv, coords, kp, vp,
+            k_resort_merge<T, D, K><<<nb, kThreads, 0, s>>>(n, moved, kp, vp, t.rflag.as<uint8_t>(),
+                                                             t.roff.as<int64_t>(), mk, mv, coords, ok, ov,
                                                              t.spts.as<SPt<T, D>>());
             ctx.kernel_launches += 1;
         }
+        skeys = ok;
+        perm = ov;
+        sorted = 1 - prev;
         t.last_path = 1;
     }
 
@@ -981,14 +1011,14 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         PhaseTimer pt_(ctx, PH_TOPOLOGY);
         k_mark<D, K><<<nblocks, kThreads, 0, s>>>(skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(), nblocks,
                                                   bt);
-        exclusive_scan_i32_i64(t.blockcnt.as<int32_t>(), t.blockoff.as<int64_t>(), nbc, &hdr->n_nodes,
-                               t.scan_tmp.as<int64_t>(), s);
+        ctx.kernel_launches += exclusive_scan_i32_i64(t.blockcnt.as<int32_t>(), t.blockoff.as<int64_t>(), nbc,
+                                                      &hdr->n_nodes, t.scan_tmp.as<int64_t>(), s);
         k_emit_ids<D><<<nblocks, kThreads, 0, s>>>(n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks, cap,
                                                     t.fchild.as<int32_t>(), t.nrange.as<int2>(), hdr, bt);
         k_emit_nodes<T, D, K><<<div_up(cap, kThreads), kThreads, 0, s>>>(
             skeys, n, cap, t.fchild.as<int32_t>(), t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
             t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.chain.as<int32_t>(), hdr, bt);
-        ctx.kernel_launches += 6;
+        ctx.kernel_launches += 3;
         }
         {
         PhaseTimer pt_(ctx, PH_REFIT);
@@ -1003,13 +1033,13 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
                                                                         t.gcnt.as<int32_t>(), nullptr, nullptr,
                                                                         t.chain.as<int32_t>(), t.parent.as<int32_t>(),
                                                                         hdr);
-            exclusive_scan_i32_i64(t.gcnt.as<int32_t>(), t.goff.as<int64_t>(), cap, &hdr->n_groups,
-                                   t.scan_tmp.as<int64_t>(), s);
+            ctx.kernel_launches += exclusive_scan_i32_i64(t.gcnt.as<int32_t>(), t.goff.as<int64_t>(), cap,
+                                                          &hdr->n_groups, t.scan_tmp.as<int64_t>(), s);
             k_groups<T, D, 1><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
                                                                         t.gcnt.as<int32_t>(), t.goff.as<int64_t>(),
                                                                         t.groups.as<int2>(), t.chain.as<int32_t>(),
                                                                         t.parent.as<int32_t>(), hdr);
-            ctx.kernel_launches += 5;
+            ctx.kernel_launches += 2;
             if (bt.n_clouds) {
                 k_cloud_start<T, D><<<div_up(bt.n_clouds, 128), 128, 0, s>>>(t.tnode.as<TNode<T, D>>(), bt, cap, hdr);
                 ctx.kernel_launches += 1;
@@ -1036,21 +1066,23 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
 // Refit mode: re-encodes every point at its previous sorted position and
 // counts the changed keys into hdr->n_moved (read with the bounds).
 template <class T, int D, class K>
-int resort_mark(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int prev) {
+int resort_mark(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int prev, int64_t cap) {
     cudaStream_t s = ctx.stream;
     cudaError_t err;
     const int nb = div_up(n, kThreads);
     if ((err = ensure(t.rflag, (size_t)n)) || (err = ensure(t.rcnt, (size_t)nb * 4)) ||
         (err = ensure(t.roff, (size_t)(nb + 1) * 8)) || (err = ensure(t.scan_tmp, (size_t)scan_tmp_elems(nb) * 8)) ||
+        (err = ensure(t.mkeys, (size_t)cap * sizeof(K))) || (err = ensure(t.mvals, (size_t)cap * 4)) ||
         (t.keep_morton && (err = ensure(t.morton, (size_t)n * 8))))
         return cuda_status(ctx, err, "allocating refit-mode scratch");
     OctHeader* hdr = t.hdr.as<OctHeader>();
     PhaseTimer pt_(ctx, PH_ENCODE);
     k_resort_mark<T, D, K><<<nb, kThreads, 0, s>>>(coords, n, t.vals[prev].as<int32_t>(), t.keys[prev].as<K>(),
                                                     T(1) / radius, hdr, t.rflag.as<uint8_t>(), t.rcnt.as<int32_t>(),
+                                                    t.mkeys.as<K>(), t.mvals.as<int32_t>(), cap,
                                                     t.keep_morton ? t.morton.as<uint64_t>() : nullptr);
-    exclusive_scan_i32_i64(t.rcnt.as<int32_t>(), t.roff.as<int64_t>(), nb, &hdr->n_moved, t.scan_tmp.as<int64_t>(), s);
-    ctx.kernel_launches += 4;
+    ctx.kernel_launches += 1 + exclusive_scan_i32_i64(t.rcnt.as<int32_t>(), t.roff.as<int64_t>(), nb, nullptr,
+                                                      t.scan_tmp.as<int64_t>(), s);
     return OK;
 }
 
@@ -1079,9 +1111,11 @@ int build_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, double radius_d) 
     const int prev = t.sorted_buf;
     t.sorted_buf = -1;
     const bool try_resort = t.keep_morton && prev >= 0 && t.sorted_n == n && t.sorted_radius == radius_d;
+    // Merge at most this many changed keys; more are cheaper to sort afresh.
+    const int64_t cap = std::min<int64_t>(kMaxMerged, std::max<int64_t>(kChunk, n / 8));
     if (try_resort) {
-        const int st = t.sorted_key_bytes == 4 ? resort_mark<T, D, uint32_t>(ctx, t, coords, n, radius, prev)
-                                               : resort_mark<T, D, uint64_t>(ctx, t, coords, n, radius, prev);
+        const int st = t.sorted_key_bytes == 4 ? resort_mark<T, D, uint32_t>(ctx, t, coords, n, radius, prev, cap)
+                                               : resort_mark<T, D, uint64_t>(ctx, t, coords, n, radius, prev, cap);
         if (st != OK) return st;
     }
     if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
@@ -1110,14 +1144,11 @@ int build_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, double radius_d) 
     t.key_bits = D * nbits_axis;
     t.key_bytes = t.key_bits <= 32 ? 4 : 8;
     t.sort_passes = (t.key_bits + 7) / 8;
-    // Merge the changed keys into the previous order unless they are so many
-    // that a full sort is cheaper (or the key width changed).
+    // Merge the changed keys into the previous order unless they are too many
+    // (or the key width changed).
     int64_t moved = -1;
     t.last_moved = try_resort ? t.hdr_host->n_moved : -1;
-    if (try_resort && t.key_bytes == t.sorted_key_bytes) {
-        const int64_t cap = std::min<int64_t>(kMaxMerged, std::max<int64_t>(kChunk, n / 8));
-        if (t.hdr_host->n_moved <= cap) moved = t.hdr_host->n_moved;
-    }
+    if (try_resort && t.key_bytes == t.sorted_key_bytes && t.hdr_host->n_moved <= cap) moved = t.hdr_host->n_moved;
     const int st = t.key_bytes == 4 ? run_pipeline<T, D, uint32_t>(ctx, t, coords, n, radius, moved, prev)
                                     : run_pipeline<T, D, uint64_t>(ctx, t, coords, n, radius, moved, prev);
     if (st == OK && t.sorted_buf >= 0) {

@@ -236,13 +236,13 @@ int backward_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int
     uint32_t* kb[2] = {ctx.dkeys[0].as<uint32_t>(), ctx.dkeys[1].as<uint32_t>()};
     int32_t* vb[2] = {ctx.dvals[0].as<int32_t>(), ctx.dvals[1].as<int32_t>()};
     const int src = radix_sort_pairs<uint32_t>(kb, vb, ctx.dhist.as<int32_t>(), ctx.dsort_tmp.as<int64_t>(), m, bits,
-                                               false, s);
+                                               false, s, &ctx.kernel_launches);
     const int32_t* sorted_edge = bits > 0 ? vb[src] : nullptr;
     k_sorted_starts<<<div_up(n + 1, tb), tb, 0, s>>>(kb[src], m, n, ctx.dsoff.as<int64_t>());
     k_grad<T, D><<<div_up(n, tb), tb, 0, s>>>(n, ctx.droff.as<int64_t>(), ctx.dsoff.as<int64_t>(), sorted_edge,
                                              (const T*)rel_disp, (const T*)rel_dist, (const T*)d_disp,
                                              (const T*)d_dist, r, (T*)grad);
-    ctx.kernel_launches += 4 + 5 * ((bits + 7) / 8);
+    ctx.kernel_launches += 4;
     return cuda_status(ctx, cudaGetLastError(), "adjoint launch");
 }
 

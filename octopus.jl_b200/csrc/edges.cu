@@ -34,30 +34,59 @@ constexpr int kEdgeWarps = 4;
 constexpr int kEdgeThreads = kEdgeWarps * 32;
 constexpr int kStage = 32;  // staged hits per lane, and points per leaf sub-chunk
 
-template <class T, int D, bool FILL>
+// The three passes of k_edges.
+enum EdgePass {
+    EP_COUNT = 0,   // per-query neighbor counts only
+    EP_RECORD = 1,  // counts, plus each query's hit positions (up to hit_stride of them)
+    EP_FILL = 2,    // the COO at the scanned offsets: from the records, or by a second walk
+};
+
+// Edge k of the COO: sender = target point t, receiver = query qi at px
+// (src/cpu/edges_cpu.jl:200-215: rel_displacement = (x_q - x_t) * inv(r),
+// rel_dist_norm = sqrt(d2) * inv(r), 1-based indices).
+template <class T, int D>
+__device__ __forceinline__ void write_edge(int64_t k, const SPt<T, D>& t, const T* px, int32_t qi, int32_t base,
+                                           T inv_r, int32_t* __restrict__ senders, int32_t* __restrict__ receivers,
+                                           T* __restrict__ rdisp, T* __restrict__ rdist) {
+    T diff[D];
+    const T d2 = dist2<T, D>(t.x, px, diff);
+    senders[k] = t.idx - base + 1;
+    receivers[k] = qi - base + 1;
+#pragma unroll
+    for (int d = 0; d < D; ++d) rdisp[(int64_t)D * k + d] = mul_rn(-diff[d], inv_r);
+    rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
+}
+
+// dstatus: in the fill pass, the bounds-guard word; in the record pass, the
+// count of groups whose records overflowed (those groups are walked again by
+// the fill pass).  hits[qpos * hit_stride + e] = sorted target position of
+// the e-th hit of the query at sorted position qpos; gflag[g] = 1 when group
+// g overflowed.
+template <class T, int D, int PASS>
 __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     const SPt<T, D>* __restrict__ qpts, const int2* __restrict__ qgroups, int64_t n_groups,
     const TNode<T, D>* __restrict__ tnode, int32_t start_node,
     const SPt<T, D>* __restrict__ tpts, int64_t n_tnodes, T r2, T inv_r, int exclude_self,
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ dstatus,
-    Batch bt) {
+    int32_t* __restrict__ hits, int64_t hit_stride, uint8_t* __restrict__ gflag, Batch bt) {
+    constexpr bool STAGE = PASS != EP_COUNT;
     constexpr int SD = stack_depth<D>();
     // Stack entries are the pushed node's (a, b) record; bit 31 of a marks
     // ascending-order subtrees (see below).
     __shared__ int2 stack[kEdgeWarps][SD];
     // The current leaf chunk, structure of arrays so pairs load as 8 bytes.
     __shared__ __align__(16) T sx[kEdgeWarps][D][32];
-    __shared__ int32_t sid[kEdgeWarps][32];
-    // Fill pass: each lane stages the sorted positions of its next hits; a
-    // flush writes them as runs of consecutive edges of one query segment.
-    __shared__ int32_t obuf[FILL ? kEdgeWarps : 1][32][FILL ? kStage + 1 : 1];
+    // Each lane stages the sorted positions of its next hits; a flush writes
+    // them as runs of consecutive entries of one query.
+    __shared__ __align__(16) int32_t obuf[STAGE ? kEdgeWarps : 1][32][STAGE ? kStage + 1 : 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t g = (int64_t)blockIdx.x * kEdgeWarps + w;
     if (g >= n_groups) return;  // warp-uniform
     const int2 grp = qgroups[g];
     const bool valid = lane < grp.y;
-    const SPt<T, D> q = qpts[grp.x + (valid ? lane : 0)];
+    const int64_t qpos = grp.x + (valid ? lane : 0);  // sorted position of this lane's query
+    const SPt<T, D> q = qpts[qpos];
     // A batch searches each cloud in its own tree with its own radius and
     // reports cloud-local indices.
     int32_t base = 0;
@@ -69,6 +98,91 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
         start_node = bt.cstart[c];
         base = (int32_t)bt.coff[c];
     }
+    int64_t cur = 0, cur_end = 0;
+    if (PASS == EP_FILL && valid) {
+        cur = offsets[q.idx];
+        cur_end = offsets[q.idx + 1];
+    }
+    if (PASS == EP_FILL && hits != nullptr && gflag[g] == 0) {
+        // The count pass recorded every hit of this group.  Its edges form
+        // one flat list, query ql's hits at [pre[ql], pre[ql + 1]); lane e
+        // writes flat entries e, e + 32, ... so every lane has work and the
+        // loads of consecutive entries are independent.
+        char* wsm = reinterpret_cast<char*>(&obuf[w][0][0]);
+        long long* scur = reinterpret_cast<long long*>(wsm);      // 32 x 8 B
+        T* sqx = reinterpret_cast<T*>(wsm + 256);                 // D x 32 x T
+        int32_t* sqi = reinterpret_cast<int32_t*>(wsm + 1024);    // 32 x 4 B
+        int32_t* spre = reinterpret_cast<int32_t*>(wsm + 1152);   // 33 x 4 B
+        const int nql = valid ? (int)(cur_end - cur) : 0;
+        int incl = nql;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        scur[lane] = cur;
+#pragma unroll
+        for (int d = 0; d < D; ++d) sqx[d * 32 + lane] = q.x[d];
+        sqi[lane] = q.idx;
+        spre[lane + 1] = incl;
+        if (lane == 0) spre[0] = 0;
+        __syncwarp();
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        // Four entries per lane in flight: all hit loads, then all point
+        // loads, then the writes.  The displacement of entry f goes through
+        // shared memory so that the warp stores D * 32 consecutive values
+        // of rel_displacement per batch instead of D strided ones.
+        T* sdisp = reinterpret_cast<T*>(wsm + 1536);                 // D x 32 x T
+        long long* sk = reinterpret_cast<long long*>(wsm + 1536 + D * 32 * sizeof(T));  // 32 x 8 B
+        int ql = 0;
+        for (int f0 = lane; f0 - lane < total; f0 += 4 * 32) {
+            int qv[4], ev[4];
+            int32_t pos[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int f = f0 + 32 * u;
+                if (f < total) {
+                    while (spre[ql + 1] <= f) ++ql;
+                    qv[u] = ql;
+                    ev[u] = f - spre[ql];
+                    pos[u] = hits[(grp.x + ql) * hit_stride + ev[u]];
+                }
+            }
+            SPt<T, D> tp[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (f0 + 32 * u < total) tp[u] = tpts[pos[u]];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int fb = f0 - lane + 32 * u;  // first entry of this batch (warp-uniform)
+                if (fb >= total) break;
+                const int nb = min(32, total - fb);
+                if (lane < nb) {
+                    const int q2 = qv[u];
+                    const long long k = scur[q2] + ev[u];
+                    T px[D], diff[D];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) px[d] = sqx[d * 32 + q2];
+                    const T d2 = dist2<T, D>(tp[u].x, px, diff);
+                    senders[k] = tp[u].idx - base + 1;
+                    receivers[k] = sqi[q2] - base + 1;
+                    rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) sdisp[D * lane + d] = mul_rn(-diff[d], inv_r);
+                    sk[lane] = k;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    const int v = 32 * c + lane;  // value v of the batch: entry v / D, axis v % D
+                    const int ent = v / D;
+                    if (ent < nb) rdisp[D * sk[ent] + (v - D * ent)] = sdisp[v];
+                }
+                __syncwarp();
+            }
+        }
+        return;
+    }
     T qlo[D], qhi[D];
 #pragma unroll
     for (int d = 0; d < D; ++d) {
@@ -76,17 +190,13 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
         qhi[d] = warp_max(q.x[d]);
     }
     int64_t cnt = 0;
-    int64_t cur = 0, cur_end = 0;
-    if (FILL && valid) {
-        cur = offsets[q.idx];
-        cur_end = offsets[q.idx + 1];
-    }
     const bool self_pair = exclude_self != 0;
     int ocnt = 0;
+    bool overflow = false;  // warp-uniform: a query had more hits than its record holds
 
-    // One query per round: lane e writes the query's e-th staged edge, so a
-    // round stores a run of consecutive edges of one segment.  Only the lanes
-    // passing `need` are flushed, so each query leaves in long runs.
+    // One query per round, lanes writing consecutive entries of its run.
+    // Only the lanes passing `need` are flushed, so each query leaves in long
+    // runs.
     auto flush = [&](bool need) {
         __syncwarp();
         unsigned busy = __ballot_sync(0xffffffffu, need && ocnt > 0);
@@ -95,24 +205,25 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             busy &= busy - 1;
             const int nql = __shfl_sync(0xffffffffu, ocnt, ql);
             const long long cq = __shfl_sync(0xffffffffu, (long long)cur, ql);
-            const long long ce = __shfl_sync(0xffffffffu, (long long)cur_end, ql);
-            const int32_t qi = __shfl_sync(0xffffffffu, q.idx, ql);
-            T px[D];
-#pragma unroll
-            for (int d = 0; d < D; ++d) px[d] = __shfl_sync(0xffffffffu, q.x[d], ql);
-            if (lane < nql) {
-                const int64_t k = cq + lane;
-                if (k < ce) {
-                    const SPt<T, D> t = tpts[obuf[w][ql][lane]];
-                    T diff[D];
-                    const T d2 = dist2<T, D>(t.x, px, diff);
-                    senders[k] = t.idx - base + 1;
-                    receivers[k] = qi - base + 1;
-#pragma unroll
-                    for (int d = 0; d < D; ++d) rdisp[(int64_t)D * k + d] = mul_rn(-diff[d], inv_r);
-                    rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
+            if (PASS == EP_RECORD) {
+                if (cq + nql <= hit_stride) {
+                    if (lane < nql) hits[(grp.x + ql) * hit_stride + cq + lane] = obuf[w][ql][lane];
                 } else {
-                    atomicOr(dstatus, 1);  // never taken when count and fill agree
+                    overflow = true;
+                }
+            } else {
+                const long long ce = __shfl_sync(0xffffffffu, (long long)cur_end, ql);
+                const int32_t qi = __shfl_sync(0xffffffffu, q.idx, ql);
+                T px[D];
+#pragma unroll
+                for (int d = 0; d < D; ++d) px[d] = __shfl_sync(0xffffffffu, q.x[d], ql);
+                if (lane < nql) {
+                    const int64_t k = cq + lane;
+                    if (k < ce)
+                        write_edge<T, D>(k, tpts[obuf[w][ql][lane]], px, qi, base, inv_r, senders, receivers, rdisp,
+                                         rdist);
+                    else
+                        atomicOr(dstatus, 1);  // never taken when count and fill agree
                 }
             }
         }
@@ -139,25 +250,21 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
         const int32_t nb = ent.y;
         if (nb > 0) {
             // Leaf: every (query, point) pair, points in ascending position,
-            // in sub-chunks of at most kStage points.
+            // in sub-chunks of at most kStage points; hits as a bit mask.
             for (int32_t c0 = 0; c0 < nb; c0 += kStage) {
                 const int m = min(kStage, nb - c0);
                 const int mp = (m + 1) & ~1;  // padded to whole pairs with +inf points
-                if (FILL && __any_sync(0xffffffffu, ocnt + m > kStage)) {
-                    flush(ocnt + m > kStage);
-                }
                 __syncwarp();
                 if (lane < m) {
                     const SPt<T, D> t = tpts[na + c0 + lane];
 #pragma unroll
                     for (int d = 0; d < D; ++d) sx[w][d][lane] = t.x[d];
-                    sid[w][lane] = t.idx;
                 } else if (lane < mp) {
 #pragma unroll
                     for (int d = 0; d < D; ++d) sx[w][d][lane] = T(INFINITY);
-                    sid[w][lane] = -1;
                 }
                 __syncwarp();
+                unsigned hm = 0;
                 if constexpr (std::is_same<T, float>::value) {
                     unsigned long long P[D];
 #pragma unroll
@@ -174,27 +281,30 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                             s0 = (d == 0) ? lo2(sq) : __fadd_rn(s0, lo2(sq));
                             s1 = (d == 0) ? hi2(sq) : __fadd_rn(s1, hi2(sq));
                         }
-                        const bool h0 = valid && s0 <= r2;
-                        const bool h1 = valid && s1 <= r2;
-                        if (FILL) {
-                            if (h0 && !(self_pair && sid[w][j] == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j;
-                            if (h1 && !(self_pair && sid[w][j + 1] == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j + 1;
-                        } else {
-                            cnt += (h0 ? 1 : 0) + (h1 ? 1 : 0);
-                        }
+                        hm |= ((s0 <= r2 ? 1u : 0u) | (s1 <= r2 ? 2u : 0u)) << j;
                     }
                 } else {
                     for (int j = 0; j < m; ++j) {
                         T t[D], diff[D];
 #pragma unroll
                         for (int d = 0; d < D; ++d) t[d] = sx[w][d][j];
-                        const T d2 = dist2<T, D>(t, q.x, diff);
-                        const bool hit = valid && d2 <= r2;
-                        if (FILL) {
-                            if (hit && !(self_pair && sid[w][j] == q.idx)) obuf[w][lane][ocnt++] = na + c0 + j;
-                        } else {
-                            cnt += hit ? 1 : 0;
-                        }
+                        hm |= (dist2<T, D>(t, q.x, diff) <= r2 ? 1u : 0u) << j;
+                    }
+                }
+                if (!valid) hm = 0;
+                if (self_pair) {  // query and target are the same tree
+                    const int64_t rel = qpos - (na + c0);
+                    if (rel >= 0 && rel < m) hm &= ~(1u << rel);
+                }
+                const int nh = __popc(hm);
+                cnt += nh;
+                if (STAGE) {
+                    if (__any_sync(0xffffffffu, ocnt + nh > kStage)) flush(ocnt + nh > kStage);
+                    const int32_t b0 = na + c0;
+                    while (hm) {
+                        const int j = __ffs(hm) - 1;
+                        hm &= hm - 1;
+                        obuf[w][lane][ocnt++] = b0 + j;
                     }
                 }
             }
@@ -223,8 +333,12 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             __syncwarp();
         }
     }
-    if (FILL) flush(true);
-    if (!FILL && valid) counts[q.idx] = (int32_t)(cnt - (self_pair ? 1 : 0));
+    if (STAGE) flush(true);
+    if (PASS != EP_FILL && valid) counts[q.idx] = (int32_t)cnt;
+    if (PASS == EP_RECORD && lane == 0) {
+        gflag[g] = overflow ? 1 : 0;
+        if (overflow) atomicAdd(dstatus, 1);
+    }
 }
 
 // Per-thread reference-order DFS for a handful of query points (the
@@ -278,6 +392,17 @@ __global__ void k_neighbors_of(const T* __restrict__ qcoords, int64_t nsel, cons
 
 namespace {
 
+// Per-query record size for the next count: about 1.5x the last mean degree
+// plus slack, in whole warps, and at most kRecordBudget bytes in all.
+constexpr int64_t kRecordBudget = 4LL << 30;
+constexpr int64_t kRecordMaxStride = 1024;
+
+int64_t record_stride(const Ctx& ctx, int64_t nq) {
+    int64_t sst = ctx.rec_stride_hint;
+    const int64_t fit = kRecordBudget / (4 * std::max<int64_t>(nq, 1)) / 32 * 32;
+    return std::min(sst, fit);
+}
+
 template <class T, int D>
 int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64_t* n_edges) {
     cudaError_t err;
@@ -285,35 +410,59 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
     const int64_t nq = q.n;
     if ((err = ensure(ctx.counts, (size_t)std::max<int64_t>(nq, 1) * 4)) ||
         (err = ensure(ctx.offsets, (size_t)(nq + 1) * 8)) ||
-        (err = ensure(ctx.scan_tmp, (size_t)scan_tmp_elems(nq) * 8)) || (err = ensure(ctx.total, 8)) ||
+        (err = ensure(ctx.scan_tmp, (size_t)scan_tmp_elems(nq) * 8)) || (err = ensure(ctx.total, 16)) ||
         (err = ensure(ctx.dstatus, 8)))
         return cuda_status(ctx, err, "allocating edge scratch");
-    if ((err = cudaMemsetAsync(ctx.dstatus.p, 0, 4, s))) return cuda_status(ctx, err, "status reset");
+    if ((err = cudaMemsetAsync(ctx.dstatus.p, 0, 4, s)) || (err = cudaMemsetAsync(ctx.total.p, 0, 16, s)))
+        return cuda_status(ctx, err, "status reset");
     if (!ctx.total_host) {
-        if ((err = cudaMallocHost((void**)&ctx.total_host, 8))) return cuda_status(ctx, err, "pinned total");
+        if ((err = cudaMallocHost((void**)&ctx.total_host, 16))) return cuda_status(ctx, err, "pinned total");
     }
     const T r = (T)t.radius;
     const T r2 = r * r;  // src/cpu/edges_cpu.jl:184
+    ctx.rec_stride = 0;
     if (t.n_nodes == 0) {
         if ((err = cudaMemsetAsync(ctx.counts.p, 0, (size_t)nq * 4, s))) return cuda_status(ctx, err, "zero counts");
     } else {
+        // Record each query's hits while counting, so that the fill pass
+        // need not walk the tree again.
+        const int64_t stride = record_stride(ctx, nq);
+        if (stride >= 32) {
+            if ((err = ensure(ctx.hits, (size_t)nq * stride * 4)) ||
+                (err = ensure(ctx.gflag, (size_t)std::max<int64_t>(q.n_groups, 1))))
+                return cuda_status(ctx, err, "allocating hit records");
+            ctx.rec_stride = stride;
+        }
         PhaseTimer pt_(ctx, PH_COUNT);
-        k_edges<T, D, false><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
-            q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start, t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0),
-            exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-            t.batch());
+        const int64_t ng = q.n_groups;
+        if (ctx.rec_stride)
+            k_edges<T, D, EP_RECORD><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
+                q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
+                t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
+                nullptr, nullptr, nullptr, nullptr, (int*)(ctx.total.as<int64_t>() + 1), ctx.hits.as<int32_t>(),
+                ctx.rec_stride, ctx.gflag.as<uint8_t>(), t.batch());
+        else
+            k_edges<T, D, EP_COUNT><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
+                q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
+                t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
+                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, t.batch());
         ctx.kernel_launches += 1;
     }
     {
         PhaseTimer pt_(ctx, PH_SCAN);
-        exclusive_scan_i32_i64(ctx.counts.as<int32_t>(), ctx.offsets.as<int64_t>(), nq, ctx.total.as<int64_t>(),
-                               ctx.scan_tmp.as<int64_t>(), s);
-        ctx.kernel_launches += 3;
+        ctx.kernel_launches += exclusive_scan_i32_i64(ctx.counts.as<int32_t>(), ctx.offsets.as<int64_t>(), nq,
+                                                      ctx.total.as<int64_t>(), ctx.scan_tmp.as<int64_t>(), s);
     }
-    if ((err = cudaMemcpyAsync(ctx.total_host, ctx.total.p, 8, cudaMemcpyDeviceToHost, s)) ||
+    if ((err = cudaMemcpyAsync(ctx.total_host, ctx.total.p, 16, cudaMemcpyDeviceToHost, s)) ||
         (err = cudaStreamSynchronize(s)))
         return cuda_status(ctx, err, "edge count");
-    *n_edges = *ctx.total_host;
+    *n_edges = ctx.total_host[0];
+    // Size the next count's records from this one: about 1.5x the mean
+    // degree plus slack, doubled while more than 1% of the groups overflow.
+    const int64_t ovf = ctx.total_host[1] & 0xffffffffLL;
+    int64_t hint = ((*n_edges / std::max<int64_t>(nq, 1)) * 3 / 2 + 16 + 31) / 32 * 32;
+    if (ctx.rec_stride && ovf * 100 > q.n_groups) hint = std::max(hint, 2 * ctx.rec_stride);
+    ctx.rec_stride_hint = std::min<int64_t>(std::max<int64_t>(hint, 32), kRecordMaxStride);
     return OK;
 }
 
@@ -324,10 +473,11 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
     const T r2 = r * r;
     const T inv_r = T(1) / r;  // inv(r), src/cpu/edges_cpu.jl:185
     PhaseTimer pt_(ctx, PH_FILL);
-    k_edges<T, D, true><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, ctx.stream>>>(
-        q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start, t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r,
-        exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(), senders, receivers, (T*)rel_disp, (T*)rel_dist,
-        ctx.dstatus.as<int>(), t.batch());
+    k_edges<T, D, EP_FILL><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, ctx.stream>>>(
+        q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
+        t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r, exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(),
+        senders, receivers, (T*)rel_disp, (T*)rel_dist, ctx.dstatus.as<int>(),
+        ctx.rec_stride ? ctx.hits.as<int32_t>() : nullptr, ctx.rec_stride, ctx.gflag.as<uint8_t>(), t.batch());
     ctx.kernel_launches += 1;
     return cuda_status(ctx, cudaGetLastError(), "edge fill launch");
 }
@@ -348,10 +498,10 @@ template <class T, int D>
 cudaError_t count_into_typed(const Tree& q, const Tree& t, bool exclude_self, int32_t* counts, cudaStream_t s) {
     const T r = (T)t.radius;
     const T r2 = r * r;
-    k_edges<T, D, false><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
+    k_edges<T, D, EP_COUNT><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
         q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
         t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, t.batch());
+        nullptr, nullptr, nullptr, nullptr, 0, nullptr, t.batch());
     return cudaGetLastError();
 }
 

@@ -136,7 +136,7 @@ struct Ctx {
     DevBuf counts;       // int32 per query point
     DevBuf offsets;      // int64 per query point + 1
     DevBuf scan_tmp;     // int64 tile sums
-    DevBuf total;        // int64 device total
+    DevBuf total;        // int64 device total, then the count of overflowed record groups
     DevBuf dstatus;      // int32 device error word set by kernels (bounds guards)
     int64_t* total_host = nullptr;  // pinned
     const Tree* plan_query = nullptr;
@@ -144,6 +144,12 @@ struct Ctx {
     uint64_t plan_qgen = 0, plan_tgen = 0;
     int plan_exclude = -1;
     int64_t plan_edges = -1;
+    // Hit records of the last count (edges.cu): rec_stride entries per query
+    // point, 0 when the count did not record; gflag marks groups whose
+    // records overflowed.
+    DevBuf hits, gflag;
+    int64_t rec_stride = 0;
+    int64_t rec_stride_hint = 64;
     // Adjoint scratch (diff.cu).
     DevBuf dkeys[2], dvals[2], dhist, dsort_tmp, droff, dsoff;
     DevBuf dnet;         // double per edge and axis: net adjoint contribution

@@ -72,28 +72,57 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const In* in, int64
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = (Out)(tile_off[blockIdx.x] + tot);
 }
 
+// Short inputs in one launch: each thread sums, then writes, its own run of
+// consecutive elements (reading each element before writing it, so `in` and
+// `out` may alias).
+template <class In, class Out>
+__global__ void __launch_bounds__(kSmallScanThreads) k_scan_small(const In* in, int64_t n, Out* out,
+                                                                  int64_t* __restrict__ d_total) {
+    __shared__ int64_t sm[kSmallScanThreads / 32 + 1];
+    const int64_t per = (n + kSmallScanThreads - 1) / kSmallScanThreads;
+    const int64_t b = (int64_t)threadIdx.x * per;
+    int64_t sum = 0;
+    for (int64_t i = b; i < b + per && i < n; ++i) sum += in[i];
+    int64_t tot;
+    int64_t run = block_exclusive_scan<int64_t>(sum, sm, &tot);
+    for (int64_t i = b; i < b + per && i < n; ++i) {
+        const In x = in[i];
+        out[i] = (Out)run;
+        run += x;
+    }
+    if (threadIdx.x == 0) {
+        out[n] = (Out)tot;
+        if (d_total) *d_total = tot;
+    }
+}
+
 // out[0..n] = exclusive scan of in[0..n-1]; out[n] = total (also *d_total).
 // `in` and `out` may alias: each tile stages its inputs before writing.
 template <class In, class Out>
-void exclusive_scan(const In* in, Out* out, int64_t n, int64_t* d_total, int64_t* tile_tmp, cudaStream_t s) {
+int exclusive_scan(const In* in, Out* out, int64_t n, int64_t* d_total, int64_t* tile_tmp, cudaStream_t s) {
     if (n <= 0) {
         cudaMemsetAsync(out, 0, sizeof(Out), s);
         if (d_total) cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
-        return;
+        return 0;
+    }
+    if (n <= kSmallScan) {
+        k_scan_small<In, Out><<<1, kSmallScanThreads, 0, s>>>(in, n, out, d_total);
+        return 1;
     }
     const int ntiles = div_up(n, kScanTile);
     k_scan_tile_sums<In><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp);
     k_scan_tiles<<<1, 1024, 0, s>>>(tile_tmp, ntiles, d_total);
     k_scan_final<In, Out><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp, out);
+    return 3;
 }
 
-void exclusive_scan_i32_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* d_total, int64_t* tile_tmp,
-                            cudaStream_t s) {
-    exclusive_scan<int32_t, int64_t>(in, out, n, d_total, tile_tmp, s);
+int exclusive_scan_i32_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* d_total, int64_t* tile_tmp,
+                           cudaStream_t s) {
+    return exclusive_scan<int32_t, int64_t>(in, out, n, d_total, tile_tmp, s);
 }
 
-void exclusive_scan_i32_i32(const int32_t* in, int32_t* out, int64_t n, int64_t* tile_tmp, cudaStream_t s) {
-    exclusive_scan<int32_t, int32_t>(in, out, n, nullptr, tile_tmp, s);
+int exclusive_scan_i32_i32(const int32_t* in, int32_t* out, int64_t n, int64_t* tile_tmp, cudaStream_t s) {
+    return exclusive_scan<int32_t, int32_t>(in, out, n, nullptr, tile_tmp, s);
 }
 
 }  // namespace oct

@@ -87,20 +87,21 @@ inline size_t sort_hist_bytes(int64_t n) { return (size_t)(256 * (int64_t)sort_t
 // Scan scratch (int64 tile sums) for the histogram scan.
 inline size_t sort_scan_bytes(int64_t n) { return (size_t)scan_tmp_elems(256 * (int64_t)sort_tiles(n)) * 8; }
 
-// Sorts n pairs by the low `bits` bits of the key; 5 launches per 8-bit pass.  Input in (k[0], v[0])
+// Sorts n pairs by the low `bits` bits of the key; 3 to 5 launches per 8-bit
+// pass, added to *launches.  Input in (k[0], v[0])
 // (v[0] may be null for the identity 0..n-1); returns the index (0 or 1) of
 // the buffers holding the result.  With zero passes the result is the input
 // and v[0] stays untouched (the caller treats a null value buffer as iota).
 template <class K>
 int radix_sort_pairs(K* k[2], int32_t* v[2], int32_t* hist, int64_t* scan_tmp, int64_t n, int bits,
-                     bool vals_in, cudaStream_t s) {
+                     bool vals_in, cudaStream_t s, int64_t* launches) {
     const int ntiles = sort_tiles(n);
     const int passes = (bits + 7) / 8;
     int src = 0;
     for (int p = 0; p < passes; ++p) {
         const int shift = 8 * p;
         k_hist<K><<<ntiles, kSortThreads, 0, s>>>(k[src], n, shift, hist, ntiles);
-        exclusive_scan_i32_i32(hist, hist, (int64_t)256 * ntiles, scan_tmp, s);
+        *launches += 2 + exclusive_scan_i32_i32(hist, hist, (int64_t)256 * ntiles, scan_tmp, s);
         k_scatter<K><<<ntiles, kSortThreads, 0, s>>>(k[src], (p == 0 && !vals_in) ? nullptr : v[src], k[src ^ 1],
                                                      v[src ^ 1], n, shift, hist, ntiles);
         src ^= 1;
