@@ -37,9 +37,14 @@ constexpr int kStage = 32;  // staged hits per lane, and points per leaf sub-chu
 // The three passes of k_edges.
 enum EdgePass {
     EP_COUNT = 0,   // per-query neighbor counts only
-    EP_RECORD = 1,  // counts, plus each query's hit positions (up to hit_stride of them)
-    EP_FILL = 2,    // the COO at the scanned offsets: from the records, or by a second walk
+    EP_RECORD = 1,  // counts, plus each query's hit records (up to rec_cap of them)
+    EP_FILL = 2,    // the COO at the scanned offsets by a second walk (groups whose records overflowed)
 };
+
+// A hit record: the sorted position of a leaf chunk's first point and the
+// bit mask of the chunk's points within the radius of one query.  A query's
+// records, in order, list its neighbors in the reference's order.
+constexpr int kMaxRecords = 240;  // per query: the record count is stored in one byte
 
 // Edge k of the COO: sender = target point t, receiver = query qi at px
 // (src/cpu/edges_cpu.jl:200-215: rel_displacement = (x_q - x_t) * inv(r),
@@ -57,32 +62,48 @@ __device__ __forceinline__ void write_edge(int64_t k, const SPt<T, D>& t, const 
     rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
 }
 
-// dstatus: in the fill pass, the bounds-guard word; in the record pass, the
-// count of groups whose records overflowed (those groups are walked again by
-// the fill pass).  hits[qpos * hit_stride + e] = sorted target position of
-// the e-th hit of the query at sorted position qpos; gflag[g] = 1 when group
-// g overflowed.
+// Radius and index base of the point set (cloud) holding sorted position p.
+template <class T>
+__device__ __forceinline__ void cloud_params(const Batch& bt, int64_t p, T& r2, T& inv_r, int32_t& start_node,
+                                             int32_t& base) {
+    if (bt.n_clouds) {
+        const int c = cloud_of_position(bt, p);
+        const double* cp = bt.cparam + (size_t)c * kCloudParams;
+        r2 = (T)cp[4];
+        inv_r = (T)cp[5];
+        start_node = bt.cstart[c];
+        base = (int32_t)bt.coff[c];
+    }
+}
+
+// ocount: in the record pass, ocount[0] counts the groups whose records
+// overflowed (those groups are walked again by the fill pass) and ocount[1]
+// is the largest record count of a query; in the fill pass, ocount[0] is
+// the bounds-guard word.  recs[qpos * rec_cap + r] = record r of the query at
+// sorted position qpos, rcount[qpos] = its record count, gflag[g] = 1 when a
+// query of group g had more than rec_cap records.
 template <class T, int D, int PASS>
 __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     const SPt<T, D>* __restrict__ qpts, const int2* __restrict__ qgroups, int64_t n_groups,
     const TNode<T, D>* __restrict__ tnode, int32_t start_node,
     const SPt<T, D>* __restrict__ tpts, int64_t n_tnodes, T r2, T inv_r, int exclude_self,
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
-    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ dstatus,
-    int32_t* __restrict__ hits, int64_t hit_stride, uint8_t* __restrict__ gflag, Batch bt) {
-    constexpr bool STAGE = PASS != EP_COUNT;
+    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ ocount,
+    int2* __restrict__ recs, int64_t rec_cap, uint8_t* __restrict__ rcount, uint8_t* __restrict__ gflag, Batch bt) {
+    constexpr bool STAGE = PASS == EP_FILL;
     constexpr int SD = stack_depth<D>();
     // Stack entries are the pushed node's (a, b) record; bit 31 of a marks
     // ascending-order subtrees (see below).
     __shared__ int2 stack[kEdgeWarps][SD];
     // The current leaf chunk, structure of arrays so pairs load as 8 bytes.
     __shared__ __align__(16) T sx[kEdgeWarps][D][32];
-    // Each lane stages the sorted positions of its next hits; a flush writes
-    // them as runs of consecutive entries of one query.
-    __shared__ __align__(16) int32_t obuf[STAGE ? kEdgeWarps : 1][32][STAGE ? kStage + 1 : 1];
+    // Fill pass: each lane stages the sorted positions of its next hits; a
+    // flush writes them as runs of consecutive edges of one query.
+    __shared__ int32_t obuf[STAGE ? kEdgeWarps : 1][32][STAGE ? kStage + 1 : 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t g = (int64_t)blockIdx.x * kEdgeWarps + w;
     if (g >= n_groups) return;  // warp-uniform
+    if (PASS == EP_FILL && recs != nullptr && gflag[g] == 0) return;  // expanded from its records
     const int2 grp = qgroups[g];
     const bool valid = lane < grp.y;
     const int64_t qpos = grp.x + (valid ? lane : 0);  // sorted position of this lane's query
@@ -90,99 +111,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     // A batch searches each cloud in its own tree with its own radius and
     // reports cloud-local indices.
     int32_t base = 0;
-    if (bt.n_clouds) {
-        const int c = cloud_of_position(bt, grp.x);
-        const double* cp = bt.cparam + (size_t)c * kCloudParams;
-        r2 = (T)cp[4];
-        inv_r = (T)cp[5];
-        start_node = bt.cstart[c];
-        base = (int32_t)bt.coff[c];
-    }
-    int64_t cur = 0, cur_end = 0;
-    if (PASS == EP_FILL && valid) {
-        cur = offsets[q.idx];
-        cur_end = offsets[q.idx + 1];
-    }
-    if (PASS == EP_FILL && hits != nullptr && gflag[g] == 0) {
-        // The count pass recorded every hit of this group.  Its edges form
-        // one flat list, query ql's hits at [pre[ql], pre[ql + 1]); lane e
-        // writes flat entries e, e + 32, ... so every lane has work and the
-        // loads of consecutive entries are independent.
-        char* wsm = reinterpret_cast<char*>(&obuf[w][0][0]);
-        long long* scur = reinterpret_cast<long long*>(wsm);      // 32 x 8 B
-        T* sqx = reinterpret_cast<T*>(wsm + 256);                 // D x 32 x T
-        int32_t* sqi = reinterpret_cast<int32_t*>(wsm + 1024);    // 32 x 4 B
-        int32_t* spre = reinterpret_cast<int32_t*>(wsm + 1152);   // 33 x 4 B
-        const int nql = valid ? (int)(cur_end - cur) : 0;
-        int incl = nql;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        scur[lane] = cur;
-#pragma unroll
-        for (int d = 0; d < D; ++d) sqx[d * 32 + lane] = q.x[d];
-        sqi[lane] = q.idx;
-        spre[lane + 1] = incl;
-        if (lane == 0) spre[0] = 0;
-        __syncwarp();
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        // Four entries per lane in flight: all hit loads, then all point
-        // loads, then the writes.  The displacement of entry f goes through
-        // shared memory so that the warp stores D * 32 consecutive values
-        // of rel_displacement per batch instead of D strided ones.
-        T* sdisp = reinterpret_cast<T*>(wsm + 1536);                 // D x 32 x T
-        long long* sk = reinterpret_cast<long long*>(wsm + 1536 + D * 32 * sizeof(T));  // 32 x 8 B
-        int ql = 0;
-        for (int f0 = lane; f0 - lane < total; f0 += 4 * 32) {
-            int qv[4], ev[4];
-            int32_t pos[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int f = f0 + 32 * u;
-                if (f < total) {
-                    while (spre[ql + 1] <= f) ++ql;
-                    qv[u] = ql;
-                    ev[u] = f - spre[ql];
-                    pos[u] = hits[(grp.x + ql) * hit_stride + ev[u]];
-                }
-            }
-            SPt<T, D> tp[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (f0 + 32 * u < total) tp[u] = tpts[pos[u]];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int fb = f0 - lane + 32 * u;  // first entry of this batch (warp-uniform)
-                if (fb >= total) break;
-                const int nb = min(32, total - fb);
-                if (lane < nb) {
-                    const int q2 = qv[u];
-                    const long long k = scur[q2] + ev[u];
-                    T px[D], diff[D];
-#pragma unroll
-                    for (int d = 0; d < D; ++d) px[d] = sqx[d * 32 + q2];
-                    const T d2 = dist2<T, D>(tp[u].x, px, diff);
-                    senders[k] = tp[u].idx - base + 1;
-                    receivers[k] = sqi[q2] - base + 1;
-                    rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
-#pragma unroll
-                    for (int d = 0; d < D; ++d) sdisp[D * lane + d] = mul_rn(-diff[d], inv_r);
-                    sk[lane] = k;
-                }
-                __syncwarp();
-#pragma unroll
-                for (int c = 0; c < D; ++c) {
-                    const int v = 32 * c + lane;  // value v of the batch: entry v / D, axis v % D
-                    const int ent = v / D;
-                    if (ent < nb) rdisp[D * sk[ent] + (v - D * ent)] = sdisp[v];
-                }
-                __syncwarp();
-            }
-        }
-        return;
-    }
+    cloud_params<T>(bt, grp.x, r2, inv_r, start_node, base);
     T qlo[D], qhi[D];
 #pragma unroll
     for (int d = 0; d < D; ++d) {
@@ -190,13 +119,18 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
         qhi[d] = warp_max(q.x[d]);
     }
     int64_t cnt = 0;
+    int64_t cur = 0, cur_end = 0;
+    if (PASS == EP_FILL && valid) {
+        cur = offsets[q.idx];
+        cur_end = offsets[q.idx + 1];
+    }
     const bool self_pair = exclude_self != 0;
     int ocnt = 0;
-    bool overflow = false;  // warp-uniform: a query had more hits than its record holds
+    int nrec = 0;
 
-    // One query per round, lanes writing consecutive entries of its run.
-    // Only the lanes passing `need` are flushed, so each query leaves in long
-    // runs.
+    // One query per round: lane e writes the query's e-th staged edge, so a
+    // round stores a run of consecutive edges of one segment.  Only the lanes
+    // passing `need` are flushed, so each query leaves in long runs.
     auto flush = [&](bool need) {
         __syncwarp();
         unsigned busy = __ballot_sync(0xffffffffu, need && ocnt > 0);
@@ -205,26 +139,18 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             busy &= busy - 1;
             const int nql = __shfl_sync(0xffffffffu, ocnt, ql);
             const long long cq = __shfl_sync(0xffffffffu, (long long)cur, ql);
-            if (PASS == EP_RECORD) {
-                if (cq + nql <= hit_stride) {
-                    if (lane < nql) hits[(grp.x + ql) * hit_stride + cq + lane] = obuf[w][ql][lane];
-                } else {
-                    overflow = true;
-                }
-            } else {
-                const long long ce = __shfl_sync(0xffffffffu, (long long)cur_end, ql);
-                const int32_t qi = __shfl_sync(0xffffffffu, q.idx, ql);
-                T px[D];
+            const long long ce = __shfl_sync(0xffffffffu, (long long)cur_end, ql);
+            const int32_t qi = __shfl_sync(0xffffffffu, q.idx, ql);
+            T px[D];
 #pragma unroll
-                for (int d = 0; d < D; ++d) px[d] = __shfl_sync(0xffffffffu, q.x[d], ql);
-                if (lane < nql) {
-                    const int64_t k = cq + lane;
-                    if (k < ce)
-                        write_edge<T, D>(k, tpts[obuf[w][ql][lane]], px, qi, base, inv_r, senders, receivers, rdisp,
-                                         rdist);
-                    else
-                        atomicOr(dstatus, 1);  // never taken when count and fill agree
-                }
+            for (int d = 0; d < D; ++d) px[d] = __shfl_sync(0xffffffffu, q.x[d], ql);
+            if (lane < nql) {
+                const int64_t k = cq + lane;
+                if (k < ce)
+                    write_edge<T, D>(k, tpts[obuf[w][ql][lane]], px, qi, base, inv_r, senders, receivers, rdisp,
+                                     rdist);
+                else
+                    atomicOr(ocount, 1);  // never taken when count and fill agree
             }
         }
         if (need) {
@@ -298,7 +224,12 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 }
                 const int nh = __popc(hm);
                 cnt += nh;
-                if (STAGE) {
+                if (PASS == EP_RECORD) {
+                    if (hm) {
+                        if (nrec < rec_cap) recs[qpos * rec_cap + nrec] = make_int2(na + c0, (int32_t)hm);
+                        ++nrec;
+                    }
+                } else if (STAGE) {
                     if (__any_sync(0xffffffffu, ocnt + nh > kStage)) flush(ocnt + nh > kStage);
                     const int32_t b0 = na + c0;
                     while (hm) {
@@ -335,10 +266,173 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     }
     if (STAGE) flush(true);
     if (PASS != EP_FILL && valid) counts[q.idx] = (int32_t)cnt;
-    if (PASS == EP_RECORD && lane == 0) {
-        gflag[g] = overflow ? 1 : 0;
-        if (overflow) atomicAdd(dstatus, 1);
+    if (PASS == EP_RECORD) {
+        if (valid) rcount[qpos] = (uint8_t)min(nrec, kMaxRecords);
+        const bool over = __any_sync(0xffffffffu, nrec > rec_cap);
+        int mx = nrec;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) {
+            gflag[g] = over ? 1 : 0;
+            if (over) atomicAdd(ocount, 1);
+            atomicMax(ocount + 1, mx);
+        }
     }
+}
+
+// Fill pass for groups whose records are complete: the group's edges form
+// one flat list, query ql's at [epre[ql], epre[ql + 1]).  Records are
+// expanded into shared memory (lanes over consecutive records, each record's
+// first hit at the running sum of the hit counts before it), then the batch
+// of flat edges is written with lanes on consecutive edges.
+constexpr int kExpandWarps = 4;
+constexpr int kExpandCap = 1024;  // staged positions per warp: one round of 32 full records
+
+template <class T, int D>
+struct ExpandSmem {
+    int32_t pos[kExpandCap];
+    long long cur[32];   // first COO slot of each query
+    long long key[32];   // COO slot of each entry of a write batch
+    T qx[D][32];
+    T disp[D * 32];
+    int32_t qi[32];
+    int32_t epre[33];    // flat edge index where each query starts
+    int32_t rpre[33];    // flat record index where each query starts
+};
+
+template <class T, int D>
+__global__ void __launch_bounds__(kExpandWarps * 32) k_expand(
+    const SPt<T, D>* __restrict__ qpts, const int2* __restrict__ qgroups, int64_t n_groups,
+    const SPt<T, D>* __restrict__ tpts, const int64_t* __restrict__ offsets, const int2* __restrict__ recs,
+    int64_t rec_cap, const uint8_t* __restrict__ rcount, const uint8_t* __restrict__ gflag, T inv_r,
+    int32_t* __restrict__ senders, int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist,
+    Batch bt) {
+    __shared__ ExpandSmem<T, D> sm_all[kExpandWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t g = (int64_t)blockIdx.x * kExpandWarps + w;
+    if (g >= n_groups || gflag[g]) return;  // warp-uniform
+    ExpandSmem<T, D>& sm = sm_all[w];
+    const int2 grp = qgroups[g];
+    const bool valid = lane < grp.y;
+    const SPt<T, D> q = qpts[grp.x + (valid ? lane : 0)];
+    T r2 = T(0);
+    int32_t start_node = 0, base = 0;
+    cloud_params<T>(bt, grp.x, r2, inv_r, start_node, base);
+    long long cur = 0;
+    int ne = 0, nr = 0;
+    if (valid) {
+        cur = offsets[q.idx];
+        ne = (int)(offsets[q.idx + 1] - cur);
+        nr = rcount[grp.x + lane];
+    }
+    int ie = ne, ir = nr;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int a = __shfl_up_sync(0xffffffffu, ie, o);
+        const int b = __shfl_up_sync(0xffffffffu, ir, o);
+        if (lane >= o) {
+            ie += a;
+            ir += b;
+        }
+    }
+    sm.cur[lane] = cur;
+#pragma unroll
+    for (int d = 0; d < D; ++d) sm.qx[d][lane] = q.x[d];
+    sm.qi[lane] = q.idx;
+    sm.epre[lane + 1] = ie;
+    sm.rpre[lane + 1] = ir;
+    if (lane == 0) {
+        sm.epre[0] = 0;
+        sm.rpre[0] = 0;
+    }
+    __syncwarp();
+    const int total_r = __shfl_sync(0xffffffffu, ir, 31);
+    int used = 0;      // positions staged (warp-uniform)
+    int ebase = 0;     // flat edge index of pos[0]
+    int qr = 0;        // this lane's query, for records
+    int qe = 0;        // this lane's query, for edges
+
+    // Writes flat edges [ebase, ebase + cnt) from the staged positions: four
+    // entries per lane in flight, rel_displacement through shared memory so
+    // that each store of the warp covers consecutive values.
+    auto write_batch = [&](int cnt) {
+        for (int f0 = 0; f0 < cnt; f0 += 4 * 32) {
+            int qv[4];
+            long long kv[4];
+            SPt<T, D> tp[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int f = f0 + 32 * u + lane;
+                if (f < cnt) {
+                    const int e = ebase + f;
+                    while (sm.epre[qe + 1] <= e) ++qe;
+                    qv[u] = qe;
+                    kv[u] = sm.cur[qe] + (e - sm.epre[qe]);
+                    tp[u] = tpts[sm.pos[f]];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int fb = f0 + 32 * u;
+                if (fb >= cnt) break;
+                const int nb = min(32, cnt - fb);
+                if (lane < nb) {
+                    const int q2 = qv[u];
+                    const long long k = kv[u];
+                    T px[D], diff[D];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) px[d] = sm.qx[d][q2];
+                    const T d2 = dist2<T, D>(tp[u].x, px, diff);
+                    senders[k] = tp[u].idx - base + 1;
+                    receivers[k] = sm.qi[q2] - base + 1;
+                    rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) sm.disp[D * lane + d] = mul_rn(-diff[d], inv_r);
+                    sm.key[lane] = k;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    const int v = 32 * c + lane;  // value v of the batch: entry v / D, axis v % D
+                    const int ent = v / D;
+                    if (ent < nb) rdisp[D * sm.key[ent] + (v - D * ent)] = sm.disp[v];
+                }
+                __syncwarp();
+            }
+        }
+    };
+
+    for (int r0 = 0; r0 < total_r; r0 += 32) {
+        const int rho = r0 + lane;
+        int2 rec = make_int2(0, 0);
+        if (rho < total_r) {
+            while (sm.rpre[qr + 1] <= rho) ++qr;
+            rec = recs[(grp.x + qr) * rec_cap + (rho - sm.rpre[qr])];
+        }
+        const int p = __popc((unsigned)rec.y);
+        int incl = p;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int a = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += a;
+        }
+        const int tr = __shfl_sync(0xffffffffu, incl, 31);
+        if (used + tr > kExpandCap) {
+            write_batch(used);
+            ebase += used;
+            used = 0;
+        }
+        int at = used + incl - p;
+        unsigned m = (unsigned)rec.y;
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            sm.pos[at++] = rec.x + j;
+        }
+        used += tr;
+        __syncwarp();
+    }
+    write_batch(used);
 }
 
 // Per-thread reference-order DFS for a handful of query points (the
@@ -392,15 +486,14 @@ __global__ void k_neighbors_of(const T* __restrict__ qcoords, int64_t nsel, cons
 
 namespace {
 
-// Per-query record size for the next count: about 1.5x the last mean degree
-// plus slack, in whole warps, and at most kRecordBudget bytes in all.
+// Hit records per query for the next count: 32 to start, then 1.25x the
+// largest record count of the last count (at most kMaxRecords), within
+// kRecordBudget bytes in all.
 constexpr int64_t kRecordBudget = 4LL << 30;
-constexpr int64_t kRecordMaxStride = 1024;
 
-int64_t record_stride(const Ctx& ctx, int64_t nq) {
-    int64_t sst = ctx.rec_stride_hint;
-    const int64_t fit = kRecordBudget / (4 * std::max<int64_t>(nq, 1)) / 32 * 32;
-    return std::min(sst, fit);
+int64_t record_cap(const Ctx& ctx, int64_t nq) {
+    const int64_t fit = kRecordBudget / (8 * std::max<int64_t>(nq, 1));
+    return std::min<int64_t>(ctx.rec_cap_hint, fit);
 }
 
 template <class T, int D>
@@ -420,32 +513,32 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
     }
     const T r = (T)t.radius;
     const T r2 = r * r;  // src/cpu/edges_cpu.jl:184
-    ctx.rec_stride = 0;
+    ctx.rec_cap = 0;
     if (t.n_nodes == 0) {
         if ((err = cudaMemsetAsync(ctx.counts.p, 0, (size_t)nq * 4, s))) return cuda_status(ctx, err, "zero counts");
     } else {
         // Record each query's hits while counting, so that the fill pass
         // need not walk the tree again.
-        const int64_t stride = record_stride(ctx, nq);
-        if (stride >= 32) {
-            if ((err = ensure(ctx.hits, (size_t)nq * stride * 4)) ||
+        const int64_t cap = record_cap(ctx, nq);
+        if (cap >= 8) {
+            if ((err = ensure(ctx.recs, (size_t)nq * cap * 8)) || (err = ensure(ctx.rcount, (size_t)nq)) ||
                 (err = ensure(ctx.gflag, (size_t)std::max<int64_t>(q.n_groups, 1))))
                 return cuda_status(ctx, err, "allocating hit records");
-            ctx.rec_stride = stride;
+            ctx.rec_cap = cap;
         }
         PhaseTimer pt_(ctx, PH_COUNT);
         const int64_t ng = q.n_groups;
-        if (ctx.rec_stride)
+        if (ctx.rec_cap)
             k_edges<T, D, EP_RECORD><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
-                nullptr, nullptr, nullptr, nullptr, (int*)(ctx.total.as<int64_t>() + 1), ctx.hits.as<int32_t>(),
-                ctx.rec_stride, ctx.gflag.as<uint8_t>(), t.batch());
+                nullptr, nullptr, nullptr, nullptr, (int*)(ctx.total.as<int64_t>() + 1), ctx.recs.as<int2>(),
+                ctx.rec_cap, ctx.rcount.as<uint8_t>(), ctx.gflag.as<uint8_t>(), t.batch());
         else
             k_edges<T, D, EP_COUNT><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
-                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, t.batch());
+                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch());
         ctx.kernel_launches += 1;
     }
     {
@@ -457,12 +550,14 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
         (err = cudaStreamSynchronize(s)))
         return cuda_status(ctx, err, "edge count");
     *n_edges = ctx.total_host[0];
-    // Size the next count's records from this one: about 1.5x the mean
-    // degree plus slack, doubled while more than 1% of the groups overflow.
-    const int64_t ovf = ctx.total_host[1] & 0xffffffffLL;
-    int64_t hint = ((*n_edges / std::max<int64_t>(nq, 1)) * 3 / 2 + 16 + 31) / 32 * 32;
-    if (ctx.rec_stride && ovf * 100 > q.n_groups) hint = std::max(hint, 2 * ctx.rec_stride);
-    ctx.rec_stride_hint = std::min<int64_t>(std::max<int64_t>(hint, 32), kRecordMaxStride);
+    ctx.rec_overflow = 0;
+    if (ctx.rec_cap) {
+        // Size the next count's records for this one's largest query.
+        const int32_t* w = reinterpret_cast<const int32_t*>(ctx.total_host + 1);
+        ctx.rec_overflow = w[0];
+        const int64_t need = ((int64_t)w[1] * 5 / 4 + 7) / 8 * 8;
+        ctx.rec_cap_hint = std::min<int64_t>(std::max<int64_t>(need, 16), kMaxRecords);
+    }
     return OK;
 }
 
@@ -472,13 +567,25 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
     const T r = (T)t.radius;
     const T r2 = r * r;
     const T inv_r = T(1) / r;  // inv(r), src/cpu/edges_cpu.jl:185
+    cudaStream_t s = ctx.stream;
     PhaseTimer pt_(ctx, PH_FILL);
-    k_edges<T, D, EP_FILL><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, ctx.stream>>>(
-        q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
-        t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r, exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(),
-        senders, receivers, (T*)rel_disp, (T*)rel_dist, ctx.dstatus.as<int>(),
-        ctx.rec_stride ? ctx.hits.as<int32_t>() : nullptr, ctx.rec_stride, ctx.gflag.as<uint8_t>(), t.batch());
-    ctx.kernel_launches += 1;
+    const int64_t ng = q.n_groups;
+    if (ctx.rec_cap) {
+        k_expand<T, D><<<div_up(ng, kExpandWarps), kExpandWarps * 32, 0, s>>>(
+            q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
+            ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint8_t>(), ctx.gflag.as<uint8_t>(), inv_r, senders,
+            receivers, (T*)rel_disp, (T*)rel_dist, t.batch());
+        ctx.kernel_launches += 1;
+    }
+    if (!ctx.rec_cap || ctx.rec_overflow) {
+        // Groups without complete records walk the tree again.
+        k_edges<T, D, EP_FILL><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
+            q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
+            t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r, exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(),
+            senders, receivers, (T*)rel_disp, (T*)rel_dist, ctx.dstatus.as<int>(),
+            ctx.rec_cap ? ctx.recs.as<int2>() : nullptr, ctx.rec_cap, nullptr, ctx.gflag.as<uint8_t>(), t.batch());
+        ctx.kernel_launches += 1;
+    }
     return cuda_status(ctx, cudaGetLastError(), "edge fill launch");
 }
 
@@ -501,7 +608,7 @@ cudaError_t count_into_typed(const Tree& q, const Tree& t, bool exclude_self, in
     k_edges<T, D, EP_COUNT><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
         q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
         t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, nullptr, 0, nullptr, t.batch());
+        nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch());
     return cudaGetLastError();
 }
 

@@ -144,12 +144,13 @@ struct Ctx {
     uint64_t plan_qgen = 0, plan_tgen = 0;
     int plan_exclude = -1;
     int64_t plan_edges = -1;
-    // Hit records of the last count (edges.cu): rec_stride entries per query
-    // point, 0 when the count did not record; gflag marks groups whose
-    // records overflowed.
-    DevBuf hits, gflag;
-    int64_t rec_stride = 0;
-    int64_t rec_stride_hint = 64;
+    // Hit records of the last count (edges.cu): rec_cap records per query
+    // point (0 when the count did not record), rcount per query, gflag per
+    // query group whose records overflowed (rec_overflow of them).
+    DevBuf recs, rcount, gflag;
+    int64_t rec_cap = 0;
+    int64_t rec_cap_hint = 32;
+    int64_t rec_overflow = 0;
     // Adjoint scratch (diff.cu).
     DevBuf dkeys[2], dvals[2], dhist, dsort_tmp, droff, dsoff;
     DevBuf dnet;         // double per edge and axis: net adjoint contribution
