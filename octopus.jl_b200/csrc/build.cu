@@ -166,7 +166,8 @@ __global__ void __launch_bounds__(kThreads) k_encode(const T* __restrict__ coord
 // ------------------------------------------------------------ 4. gather --
 template <class T, int D>
 __global__ void __launch_bounds__(kThreads) k_gather(const T* __restrict__ coords, const int32_t* __restrict__ perm,
-                                                     int64_t n, SPt<T, D>* __restrict__ spts) {
+                                                     int64_t n, SPt<T, D>* __restrict__ spts,
+                                                     int32_t* __restrict__ iperm) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int32_t j = perm ? perm[k] : (int32_t)k;
@@ -175,6 +176,7 @@ __global__ void __launch_bounds__(kThreads) k_gather(const T* __restrict__ coord
     for (int d = 0; d < D; ++d) p.x[d] = coords[(int64_t)D * j + d];
     p.idx = j;
     spts[k] = p;
+    iperm[j] = (int32_t)k;
 }
 
 // ---------------------------------------------------------- 5. topology --
@@ -776,7 +778,8 @@ __global__ void __launch_bounds__(kThreads) k_moved_rank(int64_t m, const K* __r
 template <class T, int D, class K>
 __device__ __forceinline__ void put_sorted(int64_t pos, K key, int32_t idx, const T* __restrict__ coords,
                                            K* __restrict__ okeys, int32_t* __restrict__ operm,
-                                           SPt<T, D>* __restrict__ spts) {
+                                           SPt<T, D>* __restrict__ spts, int32_t* __restrict__ iperm) {
+    iperm[idx] = (int32_t)pos;
     okeys[pos] = key;
     operm[pos] = idx;
     SPt<T, D> sp;
@@ -797,11 +800,12 @@ __global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, int64_t m,
                                                            const int64_t* __restrict__ changed_before,
                                                            const K* __restrict__ mk, const int32_t* __restrict__ mv,
                                                            const T* __restrict__ coords, K* __restrict__ okeys,
-                                                           int32_t* __restrict__ operm, SPt<T, D>* __restrict__ spts) {
+                                                           int32_t* __restrict__ operm, SPt<T, D>* __restrict__ spts,
+                                                           int32_t* __restrict__ iperm) {
     __shared__ int wsum[kThreads / 32];
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m == n) {  // every key changed: the sorted changed keys are the result
-        if (p < n) put_sorted<T, D, K>(p, mk[p], mv[p], coords, okeys, operm, spts);
+        if (p < n) put_sorted<T, D, K>(p, mk[p], mv[p], coords, okeys, operm, spts, iperm);
         return;
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -834,10 +838,10 @@ __global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, int64_t m,
         sn = q < n ? count_below(mk, mv, m, keys[q], perm[q]) : m;
     }
     const int64_t ui = p - (changed_before[blockIdx.x] + before);  // rank among unchanged keys
-    put_sorted<T, D, K>(ui + s, key, idx, coords, okeys, operm, spts);
-    for (int64_t j = s; j < sn; ++j) put_sorted<T, D, K>(j + ui + 1, mk[j], mv[j], coords, okeys, operm, spts);
+    put_sorted<T, D, K>(ui + s, key, idx, coords, okeys, operm, spts, iperm);
+    for (int64_t j = s; j < sn; ++j) put_sorted<T, D, K>(j + ui + 1, mk[j], mv[j], coords, okeys, operm, spts, iperm);
     if (ui == 0)
-        for (int64_t j = 0; j < s; ++j) put_sorted<T, D, K>(j, mk[j], mv[j], coords, okeys, operm, spts);
+        for (int64_t j = 0; j < s; ++j) put_sorted<T, D, K>(j, mk[j], mv[j], coords, okeys, operm, spts, iperm);
 }
 
 // Bounds-only step (no key changed): the topology is kept; reset the refit
@@ -879,7 +883,8 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
     T o[3] = {T(0), T(0), T(0)};
     for (int d = 0; d < D; ++d) o[d] = (T)t.origin[d];
 
-    if ((err = ensure(t.spts, (size_t)n * sizeof(SPt<T, D>)))) return cuda_status(ctx, err, "allocating points");
+    if ((err = ensure(t.spts, (size_t)n * sizeof(SPt<T, D>))) || (err = ensure(t.iperm, (size_t)n * 4)))
+        return cuda_status(ctx, err, "allocating points");
     OctHeader* hdr = t.hdr.as<OctHeader>();
     const K* skeys;
     const int32_t* perm;
@@ -919,7 +924,8 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         // --- sorted points
         {
             PhaseTimer pt_(ctx, PH_GATHER);
-            k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, perm, n, t.spts.as<SPt<T, D>>());
+            k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, perm, n, t.spts.as<SPt<T, D>>(),
+                                                                    t.iperm.as<int32_t>());
             ctx.kernel_launches += 1;
         }
         t.last_path = 0;
@@ -934,7 +940,8 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             // Same keys, same order, same topology: new bounds only.
             {
                 PhaseTimer pt_(ctx, PH_GATHER);
-                k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, vp, n, t.spts.as<SPt<T, D>>());
+                k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, vp, n, t.spts.as<SPt<T, D>>(),
+                                                                    t.iperm.as<int32_t>());
                 ctx.kernel_launches += 1;
             }
             {
@@ -976,7 +983,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             }
             k_resort_merge<T, D, K><<<nb, kThreads, 0, s>>>(n, moved, kp, vp, t.rflag.as<uint8_t>(),
                                                              t.roff.as<int64_t>(), mk, mv, coords, ok, ov,
-                                                             t.spts.as<SPt<T, D>>());
+                                                             t.spts.as<SPt<T, D>>(), t.iperm.as<int32_t>());
             ctx.kernel_launches += 1;
         }
         skeys = ok;

@@ -93,7 +93,8 @@ void release_tree(oct::Tree& t) {
         release(*b);
     for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.sort_tmp, &t.spts, &t.tnode, &t.nrange,
                     &t.parent, &t.fchild, &t.arrive, &t.groups, &t.gcnt, &t.goff, &t.chain, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
-                    &t.morton, &t.v_first, &t.v_last, &t.v_children, &t.v_bmin, &t.v_bmax, &t.v_perm})
+                    &t.morton, &t.v_first, &t.v_last, &t.v_children, &t.v_bmin, &t.v_bmax, &t.v_perm, &t.iperm,
+                    &t.rflag, &t.rcnt, &t.roff, &t.mkeys, &t.mvals, &t.mkeys2, &t.mvals2})
         release(*b);
     if (t.hdr_host) cudaFreeHost(t.hdr_host);
     t.hdr_host = nullptr;

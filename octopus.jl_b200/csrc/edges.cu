@@ -45,6 +45,7 @@ enum EdgePass {
 // bit mask of the chunk's points within the radius of one query.  A query's
 // records, in order, list its neighbors in the reference's order.
 constexpr int kMaxRecords = 240;  // per query: the record count is stored in one byte
+constexpr uint8_t kOverflowMark = 255;  // record count of the queries of an overflowed group
 
 // Edge k of the COO: sender = target point t, receiver = query qi at px
 // (src/cpu/edges_cpu.jl:200-215: rel_displacement = (x_q - x_t) * inv(r),
@@ -267,8 +268,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     if (STAGE) flush(true);
     if (PASS != EP_FILL && valid) counts[q.idx] = (int32_t)cnt;
     if (PASS == EP_RECORD) {
-        if (valid) rcount[qpos] = (uint8_t)min(nrec, kMaxRecords);
         const bool over = __any_sync(0xffffffffu, nrec > rec_cap);
+        if (valid) rcount[qpos] = over ? kOverflowMark : (uint8_t)nrec;
         int mx = nrec;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -280,11 +281,14 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     }
 }
 
-// Fill pass for groups whose records are complete: the group's edges form
-// one flat list, query ql's at [epre[ql], epre[ql + 1]).  Records are
-// expanded into shared memory (lanes over consecutive records, each record's
-// first hit at the running sum of the hit counts before it), then the batch
-// of flat edges is written with lanes on consecutive edges.
+// Fill pass from the records, in original index order: warp v writes the
+// edges of queries 32v .. 32v+31, which the COO stores contiguously, so its
+// stores cover whole sectors.  The warp's edges form one flat list, query ql's
+// at [epre[ql], epre[ql + 1]).  Records are expanded into shared memory
+// (lanes over consecutive records, each record's first hit at the running sum
+// of the hit counts before it), then each batch of flat edges is written with
+// lanes on consecutive edges.  Queries of an overflowed group (record count
+// kOverflowMark) are left to the walking fill.
 constexpr int kExpandWarps = 4;
 constexpr int kExpandCap = 1024;  // staged positions per warp: one round of 32 full records
 
@@ -295,58 +299,66 @@ struct ExpandSmem {
     long long key[32];   // COO slot of each entry of a write batch
     T qx[D][32];
     T disp[D * 32];
-    int32_t qi[32];
+    T inv_r[32];
+    int32_t qpos[32];    // sorted position of each query
+    int32_t qi[32];      // 1-based receiver index of each query
+    int32_t base[32];    // index base of each query's point set
     int32_t epre[33];    // flat edge index where each query starts
     int32_t rpre[33];    // flat record index where each query starts
 };
 
 template <class T, int D>
 __global__ void __launch_bounds__(kExpandWarps * 32) k_expand(
-    const SPt<T, D>* __restrict__ qpts, const int2* __restrict__ qgroups, int64_t n_groups,
+    int64_t nq, const int32_t* __restrict__ iperm, const SPt<T, D>* __restrict__ qpts,
     const SPt<T, D>* __restrict__ tpts, const int64_t* __restrict__ offsets, const int2* __restrict__ recs,
-    int64_t rec_cap, const uint8_t* __restrict__ rcount, const uint8_t* __restrict__ gflag, T inv_r,
-    int32_t* __restrict__ senders, int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist,
-    Batch bt) {
+    int64_t rec_cap, const uint8_t* __restrict__ rcount, T inv_r, int32_t* __restrict__ senders,
+    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, Batch bt) {
     __shared__ ExpandSmem<T, D> sm_all[kExpandWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t g = (int64_t)blockIdx.x * kExpandWarps + w;
-    if (g >= n_groups || gflag[g]) return;  // warp-uniform
+    const int64_t i0 = ((int64_t)blockIdx.x * kExpandWarps + w) * 32;
+    if (i0 >= nq) return;  // warp-uniform
     ExpandSmem<T, D>& sm = sm_all[w];
-    const int2 grp = qgroups[g];
-    const bool valid = lane < grp.y;
-    const SPt<T, D> q = qpts[grp.x + (valid ? lane : 0)];
-    T r2 = T(0);
-    int32_t start_node = 0, base = 0;
-    cloud_params<T>(bt, grp.x, r2, inv_r, start_node, base);
+    const int64_t i = i0 + lane;
+    const bool valid = i < nq;
+    const int32_t qp = valid ? iperm[i] : 0;
+    int nr = valid ? rcount[qp] : 0;
     long long cur = 0;
-    int ne = 0, nr = 0;
-    if (valid) {
-        cur = offsets[q.idx];
-        ne = (int)(offsets[q.idx + 1] - cur);
-        nr = rcount[grp.x + lane];
+    int ne = 0;
+    if (valid && nr != kOverflowMark) {
+        cur = offsets[i];
+        ne = (int)(offsets[i + 1] - cur);
+    } else {
+        nr = 0;
     }
-    int ie = ne, ir = nr;
+    const SPt<T, D> q = qpts[qp];
+    T r2 = T(0), ir = inv_r;
+    int32_t start_node = 0, base = 0;
+    cloud_params<T>(bt, qp, r2, ir, start_node, base);
+    int ie = ne, irc = nr;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const int a = __shfl_up_sync(0xffffffffu, ie, o);
-        const int b = __shfl_up_sync(0xffffffffu, ir, o);
+        const int b = __shfl_up_sync(0xffffffffu, irc, o);
         if (lane >= o) {
             ie += a;
-            ir += b;
+            irc += b;
         }
     }
     sm.cur[lane] = cur;
 #pragma unroll
     for (int d = 0; d < D; ++d) sm.qx[d][lane] = q.x[d];
-    sm.qi[lane] = q.idx;
+    sm.inv_r[lane] = ir;
+    sm.qpos[lane] = qp;
+    sm.qi[lane] = q.idx - base + 1;
+    sm.base[lane] = base;
     sm.epre[lane + 1] = ie;
-    sm.rpre[lane + 1] = ir;
+    sm.rpre[lane + 1] = irc;
     if (lane == 0) {
         sm.epre[0] = 0;
         sm.rpre[0] = 0;
     }
     __syncwarp();
-    const int total_r = __shfl_sync(0xffffffffu, ir, 31);
+    const int total_r = __shfl_sync(0xffffffffu, irc, 31);
     int used = 0;      // positions staged (warp-uniform)
     int ebase = 0;     // flat edge index of pos[0]
     int qr = 0;        // this lane's query, for records
@@ -379,15 +391,16 @@ __global__ void __launch_bounds__(kExpandWarps * 32) k_expand(
                 if (lane < nb) {
                     const int q2 = qv[u];
                     const long long k = kv[u];
+                    const T iv = sm.inv_r[q2];
                     T px[D], diff[D];
 #pragma unroll
                     for (int d = 0; d < D; ++d) px[d] = sm.qx[d][q2];
                     const T d2 = dist2<T, D>(tp[u].x, px, diff);
-                    senders[k] = tp[u].idx - base + 1;
-                    receivers[k] = sm.qi[q2] - base + 1;
-                    rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
+                    senders[k] = tp[u].idx - sm.base[q2] + 1;
+                    receivers[k] = sm.qi[q2];
+                    rdist[k] = mul_rn(sqrt_rn(d2), iv);
 #pragma unroll
-                    for (int d = 0; d < D; ++d) sm.disp[D * lane + d] = mul_rn(-diff[d], inv_r);
+                    for (int d = 0; d < D; ++d) sm.disp[D * lane + d] = mul_rn(-diff[d], iv);
                     sm.key[lane] = k;
                 }
                 __syncwarp();
@@ -407,7 +420,7 @@ __global__ void __launch_bounds__(kExpandWarps * 32) k_expand(
         int2 rec = make_int2(0, 0);
         if (rho < total_r) {
             while (sm.rpre[qr + 1] <= rho) ++qr;
-            rec = recs[(grp.x + qr) * rec_cap + (rho - sm.rpre[qr])];
+            rec = recs[(int64_t)sm.qpos[qr] * rec_cap + (rho - sm.rpre[qr])];
         }
         const int p = __popc((unsigned)rec.y);
         int incl = p;
@@ -571,10 +584,10 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
     PhaseTimer pt_(ctx, PH_FILL);
     const int64_t ng = q.n_groups;
     if (ctx.rec_cap) {
-        k_expand<T, D><<<div_up(ng, kExpandWarps), kExpandWarps * 32, 0, s>>>(
-            q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
-            ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint8_t>(), ctx.gflag.as<uint8_t>(), inv_r, senders,
-            receivers, (T*)rel_disp, (T*)rel_dist, t.batch());
+        k_expand<T, D><<<div_up(q.n, 32 * kExpandWarps), kExpandWarps * 32, 0, s>>>(
+            q.n, q.iperm.as<int32_t>(), q.spts.as<SPt<T, D>>(), t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
+            ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint8_t>(), inv_r, senders, receivers, (T*)rel_disp,
+            (T*)rel_dist, t.batch());
         ctx.kernel_launches += 1;
     }
     if (!ctx.rec_cap || ctx.rec_overflow) {

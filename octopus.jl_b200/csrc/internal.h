@@ -69,6 +69,7 @@ struct Tree {
     DevBuf hist;                 // radix digit histograms (+1 total slot)
     DevBuf sort_tmp;             // int64 tile sums of the histogram scan
     DevBuf spts;                 // SPt<T,D>[n] in Morton order
+    DevBuf iperm;                // int32 [n]: sorted position of each original point
     DevBuf tnode;                // TNode<T,D>[capacity]
     DevBuf nrange;               // int2 {first,last} 0-based per node
     DevBuf parent;               // int32 per node (-1 for the root)
