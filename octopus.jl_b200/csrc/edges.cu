@@ -283,8 +283,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
 
 // Fill pass from the records, in original index order: warp v writes the
 // edges of queries 32v .. 32v+31, which the COO stores contiguously, so its
-// stores cover whole sectors.  The warp's edges form one flat list, query ql's
-// at [epre[ql], epre[ql + 1]).  Records are expanded into shared memory
+// stores cover whole sectors.  The warp's edges form one flat list, query
+// ql's first at flat index epre(ql), COO slot kq[ql] + flat index.  Records are expanded into shared memory
 // (lanes over consecutive records, each record's first hit at the running sum
 // of the hit counts before it), then each batch of flat edges is written with
 // lanes on consecutive edges.  Queries of an overflowed group (record count
@@ -295,7 +295,8 @@ constexpr int kExpandCap = 1024;  // staged positions per warp: one round of 32 
 template <class T, int D>
 struct ExpandSmem {
     int32_t pos[kExpandCap];
-    long long cur[32];   // first COO slot of each query
+    uint8_t who[kExpandCap];  // query (lane) of each staged position
+    long long kq[32];    // COO slot of each query's flat edge 0: first slot - epre
     long long key[32];   // COO slot of each entry of a write batch
     T qx[D][32];
     T disp[D * 32];
@@ -303,12 +304,11 @@ struct ExpandSmem {
     int32_t qpos[32];    // sorted position of each query
     int32_t qi[32];      // 1-based receiver index of each query
     int32_t base[32];    // index base of each query's point set
-    int32_t epre[33];    // flat edge index where each query starts
     int32_t rpre[33];    // flat record index where each query starts
 };
 
 template <class T, int D>
-__global__ void __launch_bounds__(kExpandWarps * 32) k_expand(
+__global__ void __launch_bounds__(kExpandWarps * 32, 8) k_expand(
     int64_t nq, const int32_t* __restrict__ iperm, const SPt<T, D>* __restrict__ qpts,
     const SPt<T, D>* __restrict__ tpts, const int64_t* __restrict__ offsets, const int2* __restrict__ recs,
     int64_t rec_cap, const uint8_t* __restrict__ rcount, T inv_r, int32_t* __restrict__ senders,
@@ -344,25 +344,20 @@ __global__ void __launch_bounds__(kExpandWarps * 32) k_expand(
             irc += b;
         }
     }
-    sm.cur[lane] = cur;
+    sm.kq[lane] = cur - (ie - ne);
 #pragma unroll
     for (int d = 0; d < D; ++d) sm.qx[d][lane] = q.x[d];
     sm.inv_r[lane] = ir;
     sm.qpos[lane] = qp;
     sm.qi[lane] = q.idx - base + 1;
     sm.base[lane] = base;
-    sm.epre[lane + 1] = ie;
     sm.rpre[lane + 1] = irc;
-    if (lane == 0) {
-        sm.epre[0] = 0;
-        sm.rpre[0] = 0;
-    }
+    if (lane == 0) sm.rpre[0] = 0;
     __syncwarp();
     const int total_r = __shfl_sync(0xffffffffu, irc, 31);
     int used = 0;      // positions staged (warp-uniform)
     int ebase = 0;     // flat edge index of pos[0]
     int qr = 0;        // this lane's query, for records
-    int qe = 0;        // this lane's query, for edges
 
     // Writes flat edges [ebase, ebase + cnt) from the staged positions: four
     // entries per lane in flight, rel_displacement through shared memory so
@@ -376,10 +371,9 @@ __global__ void __launch_bounds__(kExpandWarps * 32) k_expand(
             for (int u = 0; u < 4; ++u) {
                 const int f = f0 + 32 * u + lane;
                 if (f < cnt) {
-                    const int e = ebase + f;
-                    while (sm.epre[qe + 1] <= e) ++qe;
+                    const int qe = sm.who[f];
                     qv[u] = qe;
-                    kv[u] = sm.cur[qe] + (e - sm.epre[qe]);
+                    kv[u] = sm.kq[qe] + (ebase + f);
                     tp[u] = tpts[sm.pos[f]];
                 }
             }
@@ -440,6 +434,7 @@ __global__ void __launch_bounds__(kExpandWarps * 32) k_expand(
         while (m) {
             const int j = __ffs(m) - 1;
             m &= m - 1;
+            sm.who[at] = (uint8_t)qr;
             sm.pos[at++] = rec.x + j;
         }
         used += tr;
