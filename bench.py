@@ -38,11 +38,29 @@ JITTER = 0.1 * H
 SIGMA = 0.005 * H
 METRIC = "edges/s build+query+COO @1M pts; batched & fwd+bwd vs plain, exact edges"
 WORKLOAD = "sph_lattice_timestep_1M"
-# DRAM bytes per edge of the fill launch, from an ncu capture of the same
-# kernel on the 70^3-point lattice (same density, radius and leaf structure):
-# dram__bytes_read.sum + dram__bytes_write.sum = 369.2 MB for 9,623,512 edges.
-# The traffic is per edge, so it scales to the 1M-point launch by edge count.
-FILL_DRAM_BYTES_PER_EDGE = 38.4
+# DRAM bytes per edge of the fill launch (k_expand), from an ncu capture of
+# the same kernel on the 70^3-point lattice (same density, radius and leaf
+# structure): dram__bytes_read.sum + dram__bytes_write.sum = 55.3 + 176.7 MB
+# for 9,623,512 edges.  The traffic is per edge, so it scales to the
+# 1M-point launch by edge count.
+FILL_DRAM_BYTES_PER_EDGE = 24.1
+
+
+def phase_bytes(n, e, n_nodes, path):
+    """Algorithmic HBM bytes per step of the HBM-bound build phases and of
+    the edge write, for float32 3D and the kernels that run in `path`
+    (0 full sort: k_encode + 3 radix passes + k_gather; 1 refit-mode merge:
+    k_resort_mark + k_resort_merge, which also gathers)."""
+    b = {"bounds": 12 * n}                          # coordinates read once
+    if path == 1:
+        b["encode"] = (4 + 12 + 4 + 1 + 8) * n        # perm, gathered coords, old key in; flag, Morton code out
+        b["sort"] = (4 + 4 + 1 + 12 + 4 + 4 + 16 + 4) * n  # key, perm, flag, coords in; key, perm, point, inverse out
+    else:
+        b["encode"] = (12 + 4 + 8) * n                # coords in; key and Morton code out
+        b["sort"] = 3 * (4 + 4 + 4 + 4 + 4) * n + (4 + 12 + 16 + 4) * n  # 3 passes + gather
+    b["refit"] = 16 * n + 2 * 32 * n_nodes          # sorted points in; node records read and written
+    b["fill"] = (12 + 4 * 3) * e + 8 * n            # (12 + 4D) E + 8N
+    return b
 
 
 def config_dict(extra=None):
@@ -278,6 +296,10 @@ def run_ours(args, rank, world, local):
     fill_bytes = (12 + 4 * 3) * e_per_step + 8 * N  # (12 + 4D) E + 8N
     achieved = fill_bytes / (fill_ms / 1e3) / 1e9
     dominant = max(phases, key=phases.get) if phases else None
+    path, _ = tns.trees[sid - 1].last_build()
+    pb = phase_bytes(N, e_per_step, tns.trees[sid - 1].n_nodes, path)
+    phase_hbm = {k: {"bytes": v, "gbs": v / (phases[k] / 1e3) / 1e9, "frac": v / (phases[k] / 1e3) / 1e9 / peak}
+                 for k, v in pb.items() if phases.get(k)}
 
     result = None
     if rank == 0:
@@ -301,13 +323,15 @@ def run_ours(args, rank, world, local):
                     "h2d_bytes_per_step": N * 12, "d2h_bytes_per_step": int(24 * e2e_edges / K),
                     "ms_per_step": e2e_ms_max / K},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_src, "kernel": "fill (k_edges<FILL>)",
+                         "frac": achieved / peak, "peak_source": peak_src, "kernel": "fill (k_expand)",
                          "traffic": (args.fill_traffic if args.fill_traffic is not None
                                      else FILL_DRAM_BYTES_PER_EDGE * e_per_step),
                          "traffic_source": "ncu dram bytes/edge of the fill kernel on the 343k-point "
                                            "lattice, scaled by edges per launch",
                          "algorithmic_bytes_per_launch": fill_bytes},
             "phases_ms_per_step": phases,
+            "phase_hbm": phase_hbm,
+            "build_path": {0: "full sort", 1: "changed keys merged", 2: "bounds only"}[path],
             "phase_records": phase_calls,
             "dominant_phase": dominant,
             "gpu_launches": int(launches),

@@ -154,6 +154,17 @@ OCT_API int oct_edges_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* 
                            int exclude_self, int32_t* senders, int32_t* receivers,
                            void* rel_displacement, void* rel_dist_norm, int64_t capacity);
 
+/* materialize_all_neighbors! for the pair of the last oct_edges_count:
+ * CSR neighbor lists, offsets (n_query + 1 Int32, offsets[0] = 0, row i of
+ * query point i+1 at flat[offsets[i] .. offsets[i+1]-1]) and flat (1-based
+ * target indices, the self pair excluded when exclude_self != 0), each row
+ * in the reference's traversal order -- the senders column of build_edges'
+ * COO.  Replaces materialize_cpu! (src/cpu/query_cpu.jl:149-192); the
+ * reference raises on a CUDA TNS (src/api.jl:350).  OCT_ERR_OVERFLOW when
+ * the total does not fit the Int32 offsets. */
+OCT_API int oct_csr_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
+                         int32_t* offsets, int32_t* flat, int64_t capacity);
+
 /* Neighbors of n_queries points (device coords, (ndims, n_queries)) in the
  * target tree, in the reference's traversal order and without the self
  * filter: the host for_each_neighbor / get_neighborlist accessors

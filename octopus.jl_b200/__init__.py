@@ -6,7 +6,7 @@ reference's public functions (src/Octopus.jl:31-44) over that library.
 """
 from .api import (  # noqa: F401
     ArgumentError, DimensionMismatch, InexactError, OctopusError,
-    TNS, PointSet, Octree, EdgeBuffer, EdgesTuple, DeviceView,
+    TNS, PointSet, Octree, EdgeBuffer, NeighborBuffer, EdgesTuple, DeviceView,
     set_search_radius_, set_refit_mode_, add_point_set_, resize_point_set_,
     update_point_set_, set_active_search_, run_, build_edges_, build_edges,
     for_each_neighbor, get_neighborlist, materialize_all_neighbors_,
@@ -17,6 +17,6 @@ from . import _lib  # noqa: F401
 __all__ = [
     "TNS", "set_search_radius_", "set_refit_mode_", "add_point_set_", "resize_point_set_",
     "update_point_set_", "set_active_search_", "run_", "for_each_neighbor", "get_neighborlist",
-    "materialize_all_neighbors_", "build_edges", "build_edges_", "EdgeBuffer", "build_edges_diff",
+    "materialize_all_neighbors_", "NeighborBuffer", "build_edges", "build_edges_", "EdgeBuffer", "build_edges_diff",
     "device_view", "ArgumentError", "DimensionMismatch", "InexactError", "OctopusError",
 ]

@@ -61,6 +61,7 @@ SIGNATURES = [
     ("oct_tree_view_get", I, [P, P, C.POINTER(TreeView)]),
     ("oct_edges_count", I, [P, P, P, I, C.POINTER(I64)]),
     ("oct_edges_fill", I, [P, P, P, I, P, P, P, P, I64]),
+    ("oct_csr_fill", I, [P, P, P, I, P, P, I64]),
     ("oct_neighbors", I, [P, P, P, I64, P, P, I64]),
     ("oct_edges_diff_backward", I, [P, I, I, I64, I64, P, P, P, P, P, P, D, P]),
     ("oct_edges_diff_backward_recompute", I, [P, I, I, I64, I64, P, P, P, P, P, D, P]),

@@ -211,6 +211,18 @@ class EdgeBuffer:
         self.materialized = False
 
 
+class NeighborBuffer:
+    """src/types.jl:44-54: CSR neighbor lists of one active pair: ``flat``
+    (1-based target indices) and ``offsets`` (n_query + 1 Int32, starting at
+    0); row i of query point i+1 is ``flat[offsets[i]:offsets[i+1]]``."""
+
+    def __init__(self, device: int):
+        dev = f"cuda:{device}"
+        self.flat = torch.empty(0, dtype=torch.int32, device=dev)
+        self.offsets = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.materialized = False
+
+
 EdgesTuple = namedtuple("EdgesTuple", ["senders", "receivers", "rel_displacement", "rel_dist_norm"])
 DeviceView = namedtuple("DeviceView", ["coords_q", "coords_t", "bounds_min", "bounds_max", "node_first",
                                        "node_last", "node_children", "perm", "n_nodes", "radius",
@@ -235,6 +247,7 @@ class TNS:
         self.active_pairs: list[tuple[int, int]] = []
         self.trees: list[Octree] = []
         self.edge_buffers: list[EdgeBuffer] = []
+        self.neighbor_buffers: list[NeighborBuffer] = []
         self.dirty: list[bool] = []
         self._ctx: _Context | None = None
 
@@ -333,7 +346,9 @@ def set_active_search_(tns: TNS, q: int, t: int) -> TNS:
     if pair in tns.active_pairs:
         return tns
     tns.active_pairs.append(pair)
-    tns.edge_buffers.append(EdgeBuffer(tns.T, tns.ndims, tns.device if tns.device is not None else 0))
+    dev = tns.device if tns.device is not None else 0
+    tns.edge_buffers.append(EdgeBuffer(tns.T, tns.ndims, dev))
+    tns.neighbor_buffers.append(NeighborBuffer(dev))
     return tns
 
 
@@ -364,6 +379,8 @@ def run_(tns: TNS) -> TNS:
         _build_set(tns, sid)
         tns.dirty[sid] = False
     for buf in tns.edge_buffers:
+        buf.materialized = False
+    for buf in tns.neighbor_buffers:
         buf.materialized = False
     return tns
 
@@ -397,20 +414,17 @@ def _resize_buffer(buf: EdgeBuffer, T, ndims, n_edges, device):
     buf.n_edges = n_edges
 
 
-def build_edges_(tns: TNS, qid: int, tid: int) -> EdgeBuffer:
-    """src/api.jl:304-320 with the CUDA path of ext/OctopusCUDAExt.jl:345-415."""
-    pidx = _pair_index(tns, qid, tid)
-    buf = tns.edge_buffers[pidx]
+def _count_pair(tns: TNS, qid: int, tid: int, what: str):
+    """Pass A for the pair (qid, tid): returns (ctx, qtree, ttree, exclude_self,
+    n_edges), or None when the pair has no edges by construction (an empty
+    query set, or a target never built: ext/OctopusCUDAExt.jl:353-367,
+    test/backend_errors_cpu.jl:40-57)."""
     if tns.dev != "cuda":
-        raise OctopusError("build_edges!: TNS not initialized; add a point set first")
-    qs, ts = tns.point_sets[qid - 1], tns.point_sets[tid - 1]
+        raise OctopusError(f"{what}: TNS not initialized; add a point set first")
+    qs = tns.point_sets[qid - 1]
     qtree, ttree = tns.trees[qid - 1], tns.trees[tid - 1]
     if qs.n == 0 or not ttree.built or ttree.n_nodes == 0:
-        # An empty query set, or a target never built (n_nodes == 0):
-        # zero edges (ext/OctopusCUDAExt.jl:353-367, test/backend_errors_cpu.jl:40-57).
-        _resize_buffer(buf, tns.T, tns.ndims, 0, tns.device)
-        buf.materialized = True
-        return buf
+        return None
     if not qtree.built:
         # The query set was added after the last run!; its Morton order is
         # needed to group the queries, so build it now.
@@ -419,8 +433,20 @@ def build_edges_(tns: TNS, qid: int, tid: int) -> EdgeBuffer:
     ctx.bind_stream()
     excl = 1 if qid == tid else 0
     ne = C.c_int64()
-    ctx.check(ctx.lib.oct_edges_count(ctx.handle, qtree.handle, ttree.handle, excl, C.byref(ne)), "build_edges!")
-    n_edges = int(ne.value)
+    ctx.check(ctx.lib.oct_edges_count(ctx.handle, qtree.handle, ttree.handle, excl, C.byref(ne)), what)
+    return ctx, qtree, ttree, excl, int(ne.value)
+
+
+def build_edges_(tns: TNS, qid: int, tid: int) -> EdgeBuffer:
+    """src/api.jl:304-320 with the CUDA path of ext/OctopusCUDAExt.jl:345-415."""
+    pidx = _pair_index(tns, qid, tid)
+    buf = tns.edge_buffers[pidx]
+    got = _count_pair(tns, qid, tid, "build_edges!")
+    if got is None:
+        _resize_buffer(buf, tns.T, tns.ndims, 0, tns.device)
+        buf.materialized = True
+        return buf
+    ctx, qtree, ttree, excl, n_edges = got
     if n_edges > 2**31 - 1:
         raise OctopusError(f"build_edges!: {n_edges} edges exceed the Int32 edge count of EdgeBuffer")
     _resize_buffer(buf, tns.T, tns.ndims, n_edges, tns.device)
@@ -488,9 +514,32 @@ def get_neighborlist(tns: TNS, qid: int, tid: int, i: int) -> np.ndarray:
     return js.astype(np.int32)
 
 
-def materialize_all_neighbors_(tns: TNS):
-    """src/api.jl:349-362: CPU-only in the reference; on a CUDA TNS it raises."""
-    raise OctopusError("materialize_all_neighbors! on GPU is not wired yet; use for_each_neighbor_device")
+def materialize_all_neighbors_(tns: TNS) -> TNS:
+    """src/api.jl:349-362 / materialize_cpu! (src/cpu/query_cpu.jl:149-192):
+    CSR neighbor lists for every active pair, in each pair's NeighborBuffer.
+    The reference wires this for a CPU TNS only; here it runs on the GPU:
+    the same count pass as build_edges, then the senders column alone."""
+    if tns.dev != "cuda":
+        raise OctopusError("materialize_all_neighbors!: TNS not initialized; add a point set first")
+    for pidx, (qid, tid) in enumerate(tns.active_pairs):
+        buf = tns.neighbor_buffers[pidx]
+        dev = f"cuda:{tns.device}"
+        nq = tns.point_sets[qid - 1].n
+        got = _count_pair(tns, qid, tid, "materialize_all_neighbors!")
+        if got is None:
+            buf.flat = torch.empty(0, dtype=torch.int32, device=dev)
+            buf.offsets = torch.zeros(nq + 1, dtype=torch.int32, device=dev)
+            buf.materialized = True
+            continue
+        ctx, qtree, ttree, excl, n = got
+        if n > 2**31 - 1:
+            raise OctopusError(f"materialize_all_neighbors!: {n} neighbors exceed the Int32 offsets")
+        buf.flat = torch.empty(n, dtype=torch.int32, device=dev)
+        buf.offsets = torch.empty(nq + 1, dtype=torch.int32, device=dev)
+        ctx.check(ctx.lib.oct_csr_fill(ctx.handle, qtree.handle, ttree.handle, excl, _ptr(buf.offsets),
+                                       _ptr(buf.flat), n), "materialize_all_neighbors!")
+        buf.materialized = True
+    return tns
 
 
 def device_view(tns: TNS, qid: int, tid: int) -> DeviceView:

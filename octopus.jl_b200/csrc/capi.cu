@@ -320,6 +320,18 @@ OCT_API int oct_edges_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* 
                            rel_dist_norm, capacity);
 }
 
+OCT_API int oct_csr_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
+                         int32_t* offsets, int32_t* flat, int64_t capacity) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    int st = check_pair(ctx, query, target);
+    if (st != OCT_OK) return st;
+    if (!offsets || (capacity > 0 && !flat))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "neighbor list output buffer is NULL");
+    DeviceGuard g(ctx->c.device);
+    return oct::csr_fill(ctx->c, query->t, target->t, exclude_self != 0, offsets, flat, capacity);
+}
+
 OCT_API int oct_neighbors(oct_ctx* ctx, const oct_tree* target, const void* query_coords, int64_t n_queries,
                           int32_t* out_counts, int32_t* out_indices, int64_t cap_per_query) {
     if (!ctx || !target) return OCT_ERR_ARGUMENT;

@@ -54,9 +54,10 @@ template <class T, int D>
 __device__ __forceinline__ void write_edge(int64_t k, const SPt<T, D>& t, const T* px, int32_t qi, int32_t base,
                                            T inv_r, int32_t* __restrict__ senders, int32_t* __restrict__ receivers,
                                            T* __restrict__ rdisp, T* __restrict__ rdist) {
+    senders[k] = t.idx - base + 1;
+    if (rdisp == nullptr) return;  // neighbor lists (CSR values) only
     T diff[D];
     const T d2 = dist2<T, D>(t.x, px, diff);
-    senders[k] = t.idx - base + 1;
     receivers[k] = qi - base + 1;
 #pragma unroll
     for (int d = 0; d < D; ++d) rdisp[(int64_t)D * k + d] = mul_rn(-diff[d], inv_r);
@@ -355,6 +356,7 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 8) k_expand(
     if (lane == 0) sm.rpre[0] = 0;
     __syncwarp();
     const int total_r = __shfl_sync(0xffffffffu, irc, 31);
+    const bool feat = rdisp != nullptr;  // false: neighbor lists (CSR values) only
     int used = 0;      // positions staged (warp-uniform)
     int ebase = 0;     // flat edge index of pos[0]
     int qr = 0;        // this lane's query, for records
@@ -385,26 +387,30 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 8) k_expand(
                 if (lane < nb) {
                     const int q2 = qv[u];
                     const long long k = kv[u];
-                    const T iv = sm.inv_r[q2];
-                    T px[D], diff[D];
-#pragma unroll
-                    for (int d = 0; d < D; ++d) px[d] = sm.qx[d][q2];
-                    const T d2 = dist2<T, D>(tp[u].x, px, diff);
                     senders[k] = tp[u].idx - sm.base[q2] + 1;
-                    receivers[k] = sm.qi[q2];
-                    rdist[k] = mul_rn(sqrt_rn(d2), iv);
+                    if (feat) {
+                        const T iv = sm.inv_r[q2];
+                        T px[D], diff[D];
 #pragma unroll
-                    for (int d = 0; d < D; ++d) sm.disp[D * lane + d] = mul_rn(-diff[d], iv);
-                    sm.key[lane] = k;
-                }
-                __syncwarp();
+                        for (int d = 0; d < D; ++d) px[d] = sm.qx[d][q2];
+                        const T d2 = dist2<T, D>(tp[u].x, px, diff);
+                        receivers[k] = sm.qi[q2];
+                        rdist[k] = mul_rn(sqrt_rn(d2), iv);
 #pragma unroll
-                for (int c = 0; c < D; ++c) {
-                    const int v = 32 * c + lane;  // value v of the batch: entry v / D, axis v % D
-                    const int ent = v / D;
-                    if (ent < nb) rdisp[D * sm.key[ent] + (v - D * ent)] = sm.disp[v];
+                        for (int d = 0; d < D; ++d) sm.disp[D * lane + d] = mul_rn(-diff[d], iv);
+                        sm.key[lane] = k;
+                    }
                 }
-                __syncwarp();
+                if (feat) {
+                    __syncwarp();
+#pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        const int v = 32 * c + lane;  // value v of the batch: entry v / D, axis v % D
+                        const int ent = v / D;
+                        if (ent < nb) rdisp[D * sm.key[ent] + (v - D * ent)] = sm.disp[v];
+                    }
+                    __syncwarp();
+                }
             }
         }
     };
@@ -669,6 +675,33 @@ int edges_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
                             : fill_typed<float, 2>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist);
     return t.ndims == 3 ? fill_typed<double, 3>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist)
                         : fill_typed<double, 2>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist);
+}
+
+namespace {
+__global__ void k_offsets_i32(const int64_t* __restrict__ in, int64_t n, int32_t* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (int32_t)in[i];
+}
+}  // namespace
+
+int csr_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* offsets, int32_t* flat,
+             int64_t capacity) {
+    if (ctx.plan_query != &q || ctx.plan_target != &t || ctx.plan_qgen != q.generation ||
+        ctx.plan_tgen != t.generation || ctx.plan_exclude != (exclude_self ? 1 : 0))
+        return set_error(ctx, ERR_STATE, "oct_csr_fill: no matching oct_edges_count for this pair and build");
+    if (ctx.plan_edges > INT32_MAX)
+        return set_error(ctx, ERR_OVERFLOW, "oct_csr_fill: more than 2^31 - 1 neighbors overflow the Int32 offsets");
+    if (capacity < ctx.plan_edges)
+        return set_error(ctx, ERR_CAPACITY, "oct_csr_fill: flat capacity is smaller than the neighbor count");
+    if (q.n == 0) return cuda_status(ctx, cudaMemsetAsync(offsets, 0, 4, ctx.stream), "csr offsets");
+    k_offsets_i32<<<div_up(q.n + 1, 256), 256, 0, ctx.stream>>>(ctx.offsets.as<int64_t>(), q.n + 1, offsets);
+    ctx.kernel_launches += 1;
+    if (ctx.plan_edges == 0 || t.n_nodes == 0) return cuda_status(ctx, cudaGetLastError(), "csr offsets");
+    if (t.dtype == 0)
+        return t.ndims == 3 ? fill_typed<float, 3>(ctx, q, t, exclude_self, flat, nullptr, nullptr, nullptr)
+                            : fill_typed<float, 2>(ctx, q, t, exclude_self, flat, nullptr, nullptr, nullptr);
+    return t.ndims == 3 ? fill_typed<double, 3>(ctx, q, t, exclude_self, flat, nullptr, nullptr, nullptr)
+                        : fill_typed<double, 2>(ctx, q, t, exclude_self, flat, nullptr, nullptr, nullptr);
 }
 
 int neighbors_of(Ctx& ctx, const Tree& t, const void* qcoords, int64_t nsel, int32_t* out_counts, int32_t* out_idx,

@@ -177,6 +177,8 @@ int edges_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
 int neighbors_of(Ctx& ctx, const Tree& t, const void* qcoords, int64_t nsel, int32_t* out_counts,
                  int32_t* out_idx, int64_t cap);
 cudaError_t count_into(const Tree& q, const Tree& t, bool exclude_self, int32_t* counts, cudaStream_t s);
+int csr_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* offsets, int32_t* flat,
+             int64_t capacity);
 
 // Adjoint (diff.cu).
 int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,

@@ -59,7 +59,7 @@ def test_device_view_requires_cuda_tns(ob):
         ob.device_view(ob.TNS(), 1, 1)
 
 
-def test_materialize_all_neighbors_not_on_gpu(ob):
+def test_materialize_all_neighbors_needs_point_sets(ob):
     with pytest.raises(ob.OctopusError):
         ob.materialize_all_neighbors_(ob.TNS())
 
