@@ -165,6 +165,18 @@ OCT_API int oct_edges_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* 
 OCT_API int oct_csr_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
                          int32_t* offsets, int32_t* flat, int64_t capacity);
 
+/* apply_zsort: permute a user array by the tree's Morton order.  `in` and
+ * `out` are distinct device arrays of n rows of row_bytes bytes each (a
+ * (F, n) column-major matrix has rows of F elements; a vector, of one).
+ * direction 0: out[:, i] = in[:, perm[i]] (apply_zsort,
+ * src/cpu/zsort_cpu.jl:11-32, ext/OctopusCUDAExt.jl:422-432);
+ * direction 1: out[:, perm[i]] = in[:, i] (the pullback of its rrule,
+ * ext/OctopusChainRulesCoreExt.jl:65-94).  n must equal the tree's point
+ * count (OCT_ERR_DIMENSION), and the tree must be built (OCT_ERR_STATE,
+ * prepare_zsort's error, src/api.jl:380-386). */
+OCT_API int oct_zsort_apply(oct_ctx* ctx, const oct_tree* tree, const void* in, void* out, int64_t n,
+                            int64_t row_bytes, int direction);
+
 /* Neighbors of n_queries points (device coords, (ndims, n_queries)) in the
  * target tree, in the reference's traversal order and without the self
  * filter: the host for_each_neighbor / get_neighborlist accessors

@@ -62,6 +62,7 @@ SIGNATURES = [
     ("oct_edges_count", I, [P, P, P, I, C.POINTER(I64)]),
     ("oct_edges_fill", I, [P, P, P, I, P, P, P, P, I64]),
     ("oct_csr_fill", I, [P, P, P, I, P, P, I64]),
+    ("oct_zsort_apply", I, [P, P, P, P, I64, I64, I]),
     ("oct_neighbors", I, [P, P, P, I64, P, P, I64]),
     ("oct_edges_diff_backward", I, [P, I, I, I64, I64, P, P, P, P, P, P, D, P]),
     ("oct_edges_diff_backward_recompute", I, [P, I, I, I64, I64, P, P, P, P, P, D, P]),

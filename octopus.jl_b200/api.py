@@ -615,6 +615,87 @@ BatchedEdges = namedtuple("BatchedEdges", ["senders", "receivers", "rel_displace
                                            "edge_offsets"])
 
 
+def prepare_zsort(tns: TNS) -> TNS:
+    """src/api.jl:380-386: checks that every point set's permutation is
+    available (run! since its last change); mutates nothing."""
+    for sid, ps in enumerate(tns.point_sets):
+        tree = tns.trees[sid]
+        if tns.dirty[sid] or not tree.built:
+            raise OctopusError(f"prepare_zsort: call run! first so the permutation for set {sid + 1} is available")
+    return tns
+
+
+def _zsort_rows(tns: TNS, set_id: int, x: torch.Tensor, direction: int) -> torch.Tensor:
+    """One oct_zsort_apply call on a 1-D (N,) or 2-D (F, N) tensor, returning
+    a new tensor of the same shape (2-D results are column-major, like the
+    coordinate matrices of this API)."""
+    if x.dim() > 2:
+        raise ArgumentError(f"apply_zsort supports 1-D or 2-D arrays only; got {x.dim()}-D")
+    if not x.is_cuda:
+        raise ArgumentError("apply_zsort: the array must be a CUDA tensor: this backend runs on the GPU only")
+    n = tns.point_sets[set_id - 1].n
+    if x.shape[-1] != n:
+        raise DimensionMismatch(f"perm length {n} does not match last axis {x.shape[-1]}")
+    if x.dim() == 1:
+        xin = x.contiguous()
+        out = torch.empty_like(xin)
+        row = xin.element_size()
+    else:
+        xin = x.t().contiguous()  # (N, F): each point's F values contiguous
+        out = torch.empty((x.shape[1], x.shape[0]), dtype=x.dtype, device=x.device).t()
+        row = x.shape[0] * xin.element_size()
+    if n == 0 or row == 0:
+        return out
+    ctx = tns._ctx
+    ctx.bind_stream()
+    ctx.check(ctx.lib.oct_zsort_apply(ctx.handle, tns.trees[set_id - 1].handle, _ptr(xin), _ptr(out), n, row,
+                                      direction), "apply_zsort")
+    return out
+
+
+class _ZSort(torch.autograd.Function):
+    """apply_zsort with the reference's rrule (ext/OctopusChainRulesCoreExt.jl:65-94):
+    the pullback scatters the cotangent back, grad[:, perm] = dy."""
+
+    @staticmethod
+    def forward(ctx, x, tns, set_id):
+        ctx.tns, ctx.set_id = tns, set_id
+        ctx.shape = x.shape
+        return _zsort_rows(tns, set_id, x, 0)
+
+    @staticmethod
+    def backward(ctx, dy):
+        if dy is None:
+            return None, None, None
+        g = _zsort_rows(ctx.tns, ctx.set_id, dy, 1)
+        return g, None, None
+
+
+def apply_zsort(tns: TNS, set_id: int, user_array: torch.Tensor) -> torch.Tensor:
+    """src/api.jl:388-409: a new array whose entries (1-D) or columns (2-D,
+    (F, N)) follow point set ``set_id``'s z-order: out[:, i] =
+    user_array[:, perm[i]].  ``user_array`` is read, never written.
+    Differentiable (the rrule's scatter is the backward)."""
+    if tns.dev != "cuda":
+        raise OctopusError("apply_zsort: TNS not initialized; add a point set first")
+    prepare_zsort(tns)
+    return _ZSort.apply(user_array, tns, int(set_id))
+
+
+def prepare_zsort_(tns: TNS) -> TNS:
+    """Deprecated v0.1 spelling of :func:`prepare_zsort` (src/api.jl:411-412)."""
+    import warnings
+    warnings.warn("prepare_zsort! is deprecated, use prepare_zsort", DeprecationWarning, stacklevel=2)
+    return prepare_zsort(tns)
+
+
+def apply_zsort_(tns: TNS, set_id: int, user_array: torch.Tensor) -> torch.Tensor:
+    """Deprecated v0.1 spelling of :func:`apply_zsort` (src/api.jl:411-412)."""
+    import warnings
+    warnings.warn("apply_zsort! is deprecated, use apply_zsort", DeprecationWarning, stacklevel=2)
+    return apply_zsort(tns, set_id, user_array)
+
+
 class BatchedSearch:
     """Many independent point clouds searched in one pass (no counterpart in
     the reference, which needs one TNS per radius, src/api.jl:24-29).

@@ -958,6 +958,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             if ((err = cudaGetLastError())) return cuda_status(ctx, err, "bounds refit");
             t.last_path = 2;
             t.sorted_buf = sorted;
+            t.perm_dev = vp;
             return OK;
         }
         const int nb = div_up(n, kThreads);
@@ -1065,6 +1066,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         t.n_groups = t.hdr_host->n_groups;
         t.dfs_start = t.hdr_host->dfs_start;
         t.sorted_buf = sorted;
+        t.perm_dev = perm;
         return OK;
     }
     return set_error(ctx, ERR_OVERFLOW, "tree build: node capacity retry did not converge");

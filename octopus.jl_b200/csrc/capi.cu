@@ -332,6 +332,14 @@ OCT_API int oct_csr_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* ta
     return oct::csr_fill(ctx->c, query->t, target->t, exclude_self != 0, offsets, flat, capacity);
 }
 
+OCT_API int oct_zsort_apply(oct_ctx* ctx, const oct_tree* tree, const void* in, void* out, int64_t n,
+                            int64_t row_bytes, int direction) {
+    if (!ctx || !tree) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    DeviceGuard g(ctx->c.device);
+    return oct::zsort_apply(ctx->c, tree->t, in, out, n, row_bytes, direction);
+}
+
 OCT_API int oct_neighbors(oct_ctx* ctx, const oct_tree* target, const void* query_coords, int64_t n_queries,
                           int32_t* out_counts, int32_t* out_indices, int64_t cap_per_query) {
     if (!ctx || !target) return OCT_ERR_ARGUMENT;

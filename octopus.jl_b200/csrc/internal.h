@@ -70,6 +70,7 @@ struct Tree {
     DevBuf sort_tmp;             // int64 tile sums of the histogram scan
     DevBuf spts;                 // SPt<T,D>[n] in Morton order
     DevBuf iperm;                // int32 [n]: sorted position of each original point
+    const int32_t* perm_dev = nullptr;  // original index of each sorted position (null: identity)
     DevBuf tnode;                // TNode<T,D>[capacity]
     DevBuf nrange;               // int2 {first,last} 0-based per node
     DevBuf parent;               // int32 per node (-1 for the root)
@@ -179,6 +180,9 @@ int neighbors_of(Ctx& ctx, const Tree& t, const void* qcoords, int64_t nsel, int
 cudaError_t count_into(const Tree& q, const Tree& t, bool exclude_self, int32_t* counts, cudaStream_t s);
 int csr_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* offsets, int32_t* flat,
              int64_t capacity);
+
+// Permutation of user arrays by a built tree (zsort.cu).
+int zsort_apply(Ctx& ctx, const Tree& t, const void* in, void* out, int64_t n, int64_t row_bytes, int direction);
 
 // Adjoint (diff.cu).
 int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,

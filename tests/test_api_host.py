@@ -76,3 +76,10 @@ def test_colmajor_layout(ob):
     assert torch.equal(y, x)
     z = torch.rand(5, 3).t()
     assert ob.colmajor(z).data_ptr() == z.data_ptr()
+
+
+def test_apply_zsort_needs_point_sets(ob):
+    import torch
+    with pytest.raises(ob.OctopusError):
+        ob.apply_zsort(ob.TNS(), 1, torch.zeros(3))
+    assert ob.prepare_zsort(ob.TNS()) is not None  # no sets: nothing to check
