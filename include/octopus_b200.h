@@ -201,6 +201,18 @@ OCT_API int oct_edges_diff_backward(oct_ctx* ctx, int ndims, int dtype, int64_t 
                                     const void* rel_dist_norm, const void* d_rel_displacement,
                                     const void* d_rel_dist_norm, double radius, void* grad_coords);
 
+/* Adjoint of build_edges for a cross pair (query set != target set): the
+ * cotangent term of edge k (receiver i <- sender j, as in
+ * oct_edges_diff_backward) is added to grad_query[:, i] and subtracted
+ * from grad_target[:, j].  The reference's rrule covers the self pair only
+ * and names this extension (ext/OctopusChainRulesCoreExt.jl:134-135);
+ * deterministic, no floating-point atomics. */
+OCT_API int oct_edges_diff_backward_pair(oct_ctx* ctx, int ndims, int dtype, int64_t n_query, int64_t n_target,
+                                         int64_t n_edges, const int32_t* senders, const int32_t* receivers,
+                                         const void* rel_displacement, const void* rel_dist_norm,
+                                         const void* d_rel_displacement, const void* d_rel_dist_norm, double radius,
+                                         void* grad_query, void* grad_target);
+
 /* The same pullback without the stored features: rel_displacement and
  * rel_dist_norm are recomputed from `coords` ((ndims, n_points), the
  * coordinates the edges were built from) with the forward's exact arithmetic,

@@ -610,6 +610,51 @@ def build_edges_diff(coords: torch.Tensor, tns: TNS, set_id: int, radius, recomp
     return EdgesTuple(*_EdgesDiff.apply(coords, tns, set_id, radius, recompute))
 
 
+class _EdgesDiffPair(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords_q, coords_t, tns, qid, tid, radius):
+        e = build_edges(tns, qid, tid)
+        snd, rcv = e.senders.clone(), e.receivers.clone()
+        disp = e.rel_displacement.t().contiguous().t()
+        dist = e.rel_dist_norm.t().contiguous().t()
+        ctx.tns = tns
+        ctx.radius = float(radius)
+        ctx.shapes = (coords_q.shape, coords_t.shape)
+        ctx.save_for_backward(snd, rcv, disp, dist)
+        ctx.mark_non_differentiable(snd, rcv)
+        return snd, rcv, disp, dist
+
+    @staticmethod
+    def backward(ctx, g_snd, g_rcv, g_disp, g_dist):
+        tns = ctx.tns
+        (d, nq), (_, nt) = ctx.shapes
+        T = tns.T
+        dev = f"cuda:{tns.device}"
+        gq = torch.empty((nq, d), dtype=T, device=dev)
+        gt = torch.empty((nt, d), dtype=T, device=dev)
+        dd = None if g_disp is None else g_disp.t().contiguous()
+        dn = None if g_dist is None else g_dist.reshape(-1).contiguous()
+        snd, rcv, disp, dist = ctx.saved_tensors
+        lc = tns._ctx
+        lc.bind_stream()
+        lc.check(lc.lib.oct_edges_diff_backward_pair(
+            lc.handle, d, _dtype_code(T), nq, nt, snd.numel(), _ptr(snd), _ptr(rcv), _ptr(disp.t()), _ptr(dist),
+            _ptr(dd), _ptr(dn), ctx.radius, _ptr(gq), _ptr(gt)), "build_edges_diff pullback")
+        return gq.t(), gt.t(), None, None, None, None
+
+
+def build_edges_diff_pair(coords_q: torch.Tensor, coords_t: torch.Tensor, tns: TNS, qid: int, tid: int,
+                          radius) -> EdgesTuple:
+    """Differentiable build_edges for a cross pair (qid != tid): gradients
+    flow to both ``coords_q`` (receivers) and ``coords_t`` (senders).  The
+    reference's rrule is self-pair only and names this extension
+    (ext/OctopusChainRulesCoreExt.jl:134-135); the per-edge term is its
+    rrule's (ext/OctopusChainRulesCoreExt.jl:150-189)."""
+    if int(qid) == int(tid):
+        raise ArgumentError("build_edges_diff_pair is for qid != tid; use build_edges_diff for a self pair")
+    return EdgesTuple(*_EdgesDiffPair.apply(coords_q, coords_t, tns, int(qid), int(tid), radius))
+
+
 # ----------------------------------------------------------- batched clouds --
 BatchedEdges = namedtuple("BatchedEdges", ["senders", "receivers", "rel_displacement", "rel_dist_norm",
                                            "edge_offsets"])

@@ -371,6 +371,28 @@ OCT_API int oct_edges_diff_backward(oct_ctx* ctx, int ndims, int dtype, int64_t 
                               rel_dist_norm, d_rel_displacement, d_rel_dist_norm, radius, grad_coords, nullptr);
 }
 
+OCT_API int oct_edges_diff_backward_pair(oct_ctx* ctx, int ndims, int dtype, int64_t n_query, int64_t n_target,
+                                         int64_t n_edges, const int32_t* senders, const int32_t* receivers,
+                                         const void* rel_displacement, const void* rel_dist_norm,
+                                         const void* d_rel_displacement, const void* d_rel_dist_norm, double radius,
+                                         void* grad_query, void* grad_target) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (bad_dims(ndims) || bad_dtype(dtype)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "bad ndims/dtype");
+    if (n_query < 0 || n_target < 0 || n_edges < 0 || n_edges > 2147483647LL || n_query > 2147483647LL ||
+        n_target > 2147483647LL)
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "sizes must fit Int32");
+    if (!(radius > 0.0)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "radius must be positive");
+    if ((n_query > 0 && !grad_query) || (n_target > 0 && !grad_target))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "gradient output is NULL");
+    if (n_edges > 0 && (!senders || !receivers || !rel_displacement || !rel_dist_norm))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge array is NULL");
+    DeviceGuard g(ctx->c.device);
+    return oct::diff_backward_pair(ctx->c, ndims, dtype, n_query, n_target, n_edges, senders, receivers,
+                                   rel_displacement, rel_dist_norm, d_rel_displacement, d_rel_dist_norm, radius,
+                                   grad_query, grad_target);
+}
+
 OCT_API int oct_edges_diff_backward_recompute(oct_ctx* ctx, int ndims, int dtype, int64_t n_points,
                                               int64_t n_edges, const int32_t* senders, const int32_t* receivers,
                                               const void* coords, const void* d_rel_displacement,

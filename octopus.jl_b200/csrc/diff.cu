@@ -1,4 +1,4 @@
-// Adjoint of build_edges_diff for a self pair (ext/OctopusChainRulesCoreExt.jl:137-192,
+// Adjoint of build_edges_diff (ext/OctopusChainRulesCoreExt.jl:137-192,
 // ext/OctopusCUDAChainRulesCoreExt.jl:56-99), without floating-point atomics.
 //
 // Per edge k = (receiver i <- sender j) the cotangent contributes
@@ -90,6 +90,30 @@ __global__ void k_grad(int64_t n, const int64_t* __restrict__ roff, const int64_
     }
 #pragma unroll
     for (int d = 0; d < D; ++d) grad[(int64_t)D * i + d] = (T)acc[d];
+}
+
+// One side of a cross pair's gradient: grad[i] = sign * sum of the terms of
+// the edges listed for point i, in list order (edge order, or the
+// sender-sorted order when `sorted_edge` is given).
+template <class T, int D>
+__global__ void k_grad_part(int64_t n, const int64_t* __restrict__ off, const int32_t* __restrict__ sorted_edge,
+                            const T* __restrict__ rel_disp, const T* __restrict__ rel_dist,
+                            const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r, double sign,
+                            T* __restrict__ grad) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) acc[d] = 0.0;
+    double c[D];
+    for (int64_t m = off[i]; m < off[i + 1]; ++m) {
+        const int64_t k = sorted_edge ? sorted_edge[m] : m;
+        edge_term<T, D>(k, rel_disp, rel_dist, d_disp, d_dist, r, c);
+#pragma unroll
+        for (int d = 0; d < D; ++d) acc[d] += c[d];
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) grad[(int64_t)D * i + d] = (T)(sign * acc[d]);
 }
 
 // Self-pair adjoint without a sort.  The neighbor relation of a self pair is
@@ -247,6 +271,71 @@ int backward_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int
 }
 
 }  // namespace
+
+namespace {
+
+template <class T, int D>
+int backward_pair_typed(Ctx& ctx, int64_t nq, int64_t nt, int64_t m, const int32_t* snd, const int32_t* rcv,
+                        const void* rel_disp, const void* rel_dist, const void* d_disp, const void* d_dist,
+                        double radius, void* grad_q, void* grad_t) {
+    cudaStream_t s = ctx.stream;
+    cudaError_t err;
+    const T r = (T)radius;
+    if (m == 0 || (!d_disp && !d_dist)) {
+        if ((err = cudaMemsetAsync(grad_q, 0, sizeof(T) * D * nq, s)) ||
+            (err = cudaMemsetAsync(grad_t, 0, sizeof(T) * D * nt, s)))
+            return cuda_status(ctx, err, "zero gradient");
+        return OK;
+    }
+    if ((err = ensure(ctx.dkeys[0], m * 4)) || (err = ensure(ctx.dkeys[1], m * 4)) ||
+        (err = ensure(ctx.dvals[0], m * 4)) || (err = ensure(ctx.dvals[1], m * 4)) ||
+        (err = ensure(ctx.dhist, sort_hist_bytes(m))) || (err = ensure(ctx.dsort_tmp, sort_scan_bytes(m))) ||
+        (err = ensure(ctx.droff, (nq + 1) * 8)) || (err = ensure(ctx.dsoff, (nt + 1) * 8)))
+        return cuda_status(ctx, err, "allocating adjoint scratch");
+    const int tb = 256;
+    PhaseTimer pt_(ctx, PH_ADJOINT);
+    k_segment_starts<<<div_up(nq + 1, tb), tb, 0, s>>>(rcv, m, nq, ctx.droff.as<int64_t>());
+    k_sender_keys<<<div_up(m, tb), tb, 0, s>>>(snd, m, ctx.dkeys[0].as<uint32_t>());
+    int bits = 0;
+    while (bits < 32 && ((uint64_t)(nt - 1) >> bits) != 0) ++bits;
+    uint32_t* kb[2] = {ctx.dkeys[0].as<uint32_t>(), ctx.dkeys[1].as<uint32_t>()};
+    int32_t* vb[2] = {ctx.dvals[0].as<int32_t>(), ctx.dvals[1].as<int32_t>()};
+    const int src = radix_sort_pairs<uint32_t>(kb, vb, ctx.dhist.as<int32_t>(), ctx.dsort_tmp.as<int64_t>(), m, bits,
+                                               false, s, &ctx.kernel_launches);
+    const int32_t* sorted_edge = bits > 0 ? vb[src] : nullptr;
+    k_sorted_starts<<<div_up(nt + 1, tb), tb, 0, s>>>(kb[src], m, nt, ctx.dsoff.as<int64_t>());
+    k_grad_part<T, D><<<div_up(nq, tb), tb, 0, s>>>(nq, ctx.droff.as<int64_t>(), nullptr, (const T*)rel_disp,
+                                                    (const T*)rel_dist, (const T*)d_disp, (const T*)d_dist, r, 1.0,
+                                                    (T*)grad_q);
+    k_grad_part<T, D><<<div_up(nt, tb), tb, 0, s>>>(nt, ctx.dsoff.as<int64_t>(), sorted_edge, (const T*)rel_disp,
+                                                    (const T*)rel_dist, (const T*)d_disp, (const T*)d_dist, r, -1.0,
+                                                    (T*)grad_t);
+    ctx.kernel_launches += 5;
+    return cuda_status(ctx, cudaGetLastError(), "adjoint launch");
+}
+
+}  // namespace
+
+int diff_backward_pair(Ctx& ctx, int ndims, int dtype, int64_t nq, int64_t nt, int64_t m, const int32_t* snd,
+                       const int32_t* rcv, const void* rel_disp, const void* rel_dist, const void* d_disp,
+                       const void* d_dist, double radius, void* grad_q, void* grad_t) {
+    if (nq == 0 && nt == 0) return OK;
+    if (nq == 0 || nt == 0) {
+        // No edges can exist; the non-empty side's gradient is zero.
+        const size_t es = dtype == 0 ? 4 : 8;
+        cudaError_t err = cudaMemsetAsync(nq ? grad_q : grad_t, 0, es * ndims * (nq ? nq : nt), ctx.stream);
+        return cuda_status(ctx, err, "zero gradient");
+    }
+    if (dtype == 0)
+        return ndims == 3 ? backward_pair_typed<float, 3>(ctx, nq, nt, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist,
+                                                          radius, grad_q, grad_t)
+                          : backward_pair_typed<float, 2>(ctx, nq, nt, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist,
+                                                          radius, grad_q, grad_t);
+    return ndims == 3 ? backward_pair_typed<double, 3>(ctx, nq, nt, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist,
+                                                       radius, grad_q, grad_t)
+                      : backward_pair_typed<double, 2>(ctx, nq, nt, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist,
+                                                       radius, grad_q, grad_t);
+}
 
 int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n, int64_t m, const int32_t* snd, const int32_t* rcv,
                   const void* rel_disp, const void* rel_dist, const void* d_disp, const void* d_dist, double radius,

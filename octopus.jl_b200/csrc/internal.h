@@ -189,6 +189,9 @@ int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n_points, int64_t n_ed
                   const int32_t* senders, const int32_t* receivers, const void* rel_disp,
                   const void* rel_dist, const void* d_disp, const void* d_dist, double radius,
                   void* grad, const void* coords);
+int diff_backward_pair(Ctx& ctx, int ndims, int dtype, int64_t nq, int64_t nt, int64_t m, const int32_t* snd,
+                       const int32_t* rcv, const void* rel_disp, const void* rel_dist, const void* d_disp,
+                       const void* d_dist, double radius, void* grad_q, void* grad_t);
 
 int set_error(Ctx& ctx, int status, const std::string& msg);
 int cuda_status(Ctx& ctx, cudaError_t e, const char* where);

@@ -135,3 +135,80 @@ def test_general_coo_uses_sorted_adjoint(ob, oracle_mod, dtype):
                                   rn.cpu().numpy(), gd.cpu().numpy(), gn.cpu().numpy(), r)
     tol = 1e-12 if dtype == np.float64 else 2e-5
     assert np.abs(grad.cpu().numpy() - go).max() <= tol * np.abs(go).max()
+
+
+def _pair_rrule_f64(nq, nt, s, q, rd, rn, gd, gn, r):
+    """The rrule's per-edge term (ext/OctopusChainRulesCoreExt.jl:150-189)
+    added to the receiver and subtracted from the sender, in float64."""
+    rd = rd.astype(np.float64)
+    rn = rn.astype(np.float64)
+    term = gd.astype(np.float64) / r
+    mask = rn > 1e-8
+    term[mask] += rd[mask] * (gn.astype(np.float64)[mask] / (rn[mask] * r))[:, None]
+    g_q = np.zeros((nq, rd.shape[1]))
+    g_t = np.zeros((nt, rd.shape[1]))
+    np.add.at(g_q, q, term)
+    np.subtract.at(g_t, s, term)
+    return g_q, g_t
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_cross_pair_adjoint(ob, dtype):
+    """Query set A, target set B: gradients reach both coordinate sets."""
+    T = torch.float32 if dtype == np.float32 else torch.float64
+    a = uniform(2500, 3, 8201, dtype=dtype)
+    b = uniform(3500, 3, 8202, dtype=dtype)
+    r = dtype(0.09)
+    tns = ob.TNS(T, ndims=3)
+    ob.set_search_radius_(tns, r)
+    ca = torch.from_numpy(a).cuda().t().requires_grad_(True)
+    cb = torch.from_numpy(b).cuda().t().requires_grad_(True)
+    ia = ob.add_point_set_(tns, ca.detach())
+    ib = ob.add_point_set_(tns, cb.detach())
+    ob.set_active_search_(tns, ia, ib)
+    ob.run_(tns)
+    e = ob.build_edges_diff_pair(ca, cb, tns, ia, ib, r)
+    ((e.rel_displacement ** 2).sum() + 0.5 * (e.rel_dist_norm ** 2).sum()).backward()
+    s = e.senders.cpu().numpy().astype(np.int64) - 1
+    q = e.receivers.cpu().numpy().astype(np.int64) - 1
+    rd = e.rel_displacement.detach().t().cpu().numpy()
+    rn = e.rel_dist_norm.detach().reshape(-1).cpu().numpy()
+    gq, gt = _pair_rrule_f64(len(a), len(b), s, q, rd, rn, 2 * rd, rn, float(r))
+    tol = 1e-12 if dtype == np.float64 else 2e-5
+    assert np.abs(ca.grad.t().cpu().numpy() - gq).max() <= tol * np.abs(gq).max()
+    assert np.abs(cb.grad.t().cpu().numpy() - gt).max() <= tol * np.abs(gt).max()
+    with pytest.raises(ob.ArgumentError):
+        ob.build_edges_diff_pair(ca, ca, tns, ia, ia, r)
+
+
+def test_cross_pair_adjoint_fp64_central_differences(ob):
+    a = uniform(300, 3, 8203, dtype=np.float64)
+    b = uniform(350, 3, 8204, dtype=np.float64)
+    r = 0.25
+    tns = ob.TNS(torch.float64, ndims=3)
+    ob.set_search_radius_(tns, r)
+    ca = torch.from_numpy(a).cuda().t().requires_grad_(True)
+    cb = torch.from_numpy(b).cuda().t().requires_grad_(True)
+    ia = ob.add_point_set_(tns, ca.detach())
+    ib = ob.add_point_set_(tns, cb.detach())
+    ob.set_active_search_(tns, ia, ib)
+    ob.run_(tns)
+    e = ob.build_edges_diff_pair(ca, cb, tns, ia, ib, r)
+    ((e.rel_displacement ** 2).sum() + 0.5 * (e.rel_dist_norm ** 2).sum()).backward()
+    s = e.senders.cpu().numpy() - 1
+    q = e.receivers.cpu().numpy() - 1
+
+    def f(xa, xb):
+        dd = (xa[q] - xb[s]) / r
+        return 1.5 * (dd * dd).sum()
+
+    rng = np.random.default_rng(1)
+    eps = 1e-4
+    for which, x, g in ((0, a, ca.grad.t().cpu().numpy()), (1, b, cb.grad.t().cpu().numpy())):
+        for k in rng.choice(x.size, 30, replace=False):
+            def fk(delta):
+                xx = x.copy()
+                xx.flat[k] += delta
+                return f(xx, b) if which == 0 else f(a, xx)
+            fd = (-fk(2 * eps) + 8 * fk(eps) - 8 * fk(-eps) + fk(-2 * eps)) / (12 * eps)
+            assert abs(g.flat[k] - fd) <= 1e-5 * max(1.0, abs(fd))
