@@ -504,9 +504,56 @@ def cpu_baseline(args, budget_s=None):
         steps += 1
         if secs >= budget_s:
             break
-    return {"value": edges / secs, "unit": "edges/s", "cores": nthreads, "kind": "port",
-            "sample": f"{steps} full 1M-point time steps (build + count + scan + fill), "
-                      f"{secs:.1f} s of CPU work"}
+    out = {"value": edges / secs, "unit": "edges/s", "cores": nthreads, "kind": "port",
+           "sample": f"{steps} full 1M-point time steps (build + count + scan + fill), "
+                     f"{secs:.1f} s of CPU work"}
+    out["other_configs"] = cpu_other_configs(oracle, nthreads)
+    return out
+
+
+def cpu_other_configs(oracle, nthreads):
+    """The CPU port on the other configurations, one full run each (the
+    nonuniform 2D case is left out: its 1.5 G-edge COO needs ~37 GB of host
+    memory)."""
+    wl = _workloads()
+    res = {}
+
+    def timed(fn):
+        t0 = time.perf_counter()
+        e = fn()
+        return e, time.perf_counter() - t0
+
+    x = wl.uniform(100_000, 3, 2024)
+    e, t = timed(lambda: len(oracle.build_edges(oracle.build_tree(x, np.float32(0.04), nthreads=nthreads), x,
+                                                exclude_self=True, nthreads=nthreads)["senders"]))
+    res["uniform_100k_r0.04"] = {"edges": e, "s": t, "edges_per_s": e / t}
+    rng = np.random.default_rng(4)
+    sizes = np.exp(rng.uniform(np.log(500), np.log(20000), 512)).astype(np.int64)
+    radii = rng.uniform(0.03, 0.08, 512)
+    clouds = [rng.random((int(n), 3)).astype(np.float32) for n in sizes]
+
+    def per_cloud():
+        m = 0
+        for c, r in zip(clouds, radii):
+            rr = np.float32(r)
+            m += len(oracle.build_edges(oracle.build_tree(c, rr, nthreads=nthreads), c, exclude_self=True,
+                                        nthreads=nthreads)["senders"])
+        return m
+
+    e, t = timed(per_cloud)
+    res["batched_512_clouds_per_cloud_loop"] = {"edges": e, "s": t, "edges_per_s": e / t}
+    x = wl.uniform(2_000_000, 3, 2025)
+
+    def diff():
+        tr = oracle.build_tree(x, np.float32(0.012), nthreads=nthreads)
+        oe = oracle.build_edges(tr, x, exclude_self=True, nthreads=nthreads)
+        rd, rn = oe["rel_displacement"], oe["rel_dist_norm"]
+        oracle.diff_backward(len(x), oe["senders"], oe["receivers"], rd, rn, 2 * rd, rn, np.float32(0.012))
+        return len(oe["senders"])
+
+    e, t = timed(diff)
+    res["diff_2M_r0.012_fwd_bwd"] = {"edges": e, "s": t, "edges_per_s": e / t}
+    return res
 
 
 # ------------------------------------------------------ reference arm -----
