@@ -33,6 +33,7 @@ namespace oct {
 constexpr int kEdgeWarps = 4;
 constexpr int kEdgeThreads = kEdgeWarps * 32;
 constexpr int kStage = 32;  // staged hits per lane, and points per leaf sub-chunk
+constexpr int kMaxSeg = 16;  // leaves sharing one chunk
 
 // The three passes of k_edges.
 enum EdgePass {
@@ -97,8 +98,13 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     // Stack entries are the pushed node's (a, b) record; bit 31 of a marks
     // ascending-order subtrees (see below).
     __shared__ int2 stack[kEdgeWarps][SD];
-    // The current leaf chunk, structure of arrays so pairs load as 8 bytes.
+    // The current leaf chunk, structure of arrays so pairs load as 8 bytes,
+    // its leaf segments (first position, first slot; entry nseg holds the
+    // point count), and per query lane the chunk slot of its own point
+    // ((chunk number << 5) | slot).
     __shared__ __align__(16) T sx[kEdgeWarps][D][32];
+    __shared__ int2 sseg[kEdgeWarps][kMaxSeg + 1];
+    __shared__ int sself[kEdgeWarps][32];
     // Fill pass: each lane stages the sorted positions of its next hits; a
     // flush writes them as runs of consecutive edges of one query.
     __shared__ int32_t obuf[STAGE ? kEdgeWarps : 1][32][STAGE ? kStage + 1 : 1];
@@ -129,6 +135,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     const bool self_pair = exclude_self != 0;
     int ocnt = 0;
     int nrec = 0;
+    int chunk = 0;  // leaf chunks processed by this warp (warp-uniform)
+    sself[w][lane] = -1;
 
     // One query per round: lane e writes the query's e-th staged edge, so a
     // round stores a run of consecutive edges of one segment.  Only the lanes
@@ -177,16 +185,41 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
         const int32_t na = ent.x & 0x7fffffff;
         const int32_t nb = ent.y;
         if (nb > 0) {
-            // Leaf: every (query, point) pair, points in ascending position,
-            // in sub-chunks of at most kStage points; hits as a bit mask.
+            // Leaves: every (query, point) pair, points in ascending position
+            // within a leaf, hits as a bit mask.  Leaves popped one after
+            // another (the next stack entries, so the DFS order is kept)
+            // share one chunk of at most kStage points as consecutive
+            // segments; a leaf of more than kStage points is cut into chunks.
             for (int32_t c0 = 0; c0 < nb; c0 += kStage) {
-                const int m = min(kStage, nb - c0);
-                const int mp = (m + 1) & ~1;  // padded to whole pairs with +inf points
+                __syncwarp();  // every lane is done with the previous chunk's segment table
+                int total = min(kStage, nb - c0);
+                int nseg = 1;
+                if (lane == 0) sseg[w][0] = make_int2(na + c0, 0);
+                if (nb <= kStage) {
+                    while (sp > 0 && nseg < kMaxSeg) {
+                        const int2 nx = stack[w][sp - 1];
+                        if (nx.y <= 0 || total + nx.y > kStage) break;
+                        --sp;
+                        if (lane == 0) sseg[w][nseg] = make_int2(nx.x & 0x7fffffff, total);
+                        total += nx.y;
+                        ++nseg;
+                    }
+                }
+                if (lane == 0) sseg[w][nseg] = make_int2(0, total);
+                const int mp = (total + 1) & ~1;  // padded to whole pairs with +inf points
+                ++chunk;
                 __syncwarp();
-                if (lane < m) {
-                    const SPt<T, D> t = tpts[na + c0 + lane];
+                if (lane < total) {
+                    int k = 0;
+                    while (sseg[w][k + 1].y <= lane) ++k;
+                    const int32_t pos = sseg[w][k].x + (lane - sseg[w][k].y);
+                    const SPt<T, D> t = tpts[pos];
 #pragma unroll
                     for (int d = 0; d < D; ++d) sx[w][d][lane] = t.x[d];
+                    if (self_pair) {  // query and target are the same tree: the group's own points
+                        const int64_t sl = pos - grp.x;
+                        if (sl >= 0 && sl < grp.y) sself[w][sl] = (chunk << 5) | lane;
+                    }
                 } else if (lane < mp) {
 #pragma unroll
                     for (int d = 0; d < D; ++d) sx[w][d][lane] = T(INFINITY);
@@ -212,7 +245,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                         hm |= ((s0 <= r2 ? 1u : 0u) | (s1 <= r2 ? 2u : 0u)) << j;
                     }
                 } else {
-                    for (int j = 0; j < m; ++j) {
+                    for (int j = 0; j < total; ++j) {
                         T t[D], diff[D];
 #pragma unroll
                         for (int d = 0; d < D; ++d) t[d] = sx[w][d][j];
@@ -220,24 +253,34 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                     }
                 }
                 if (!valid) hm = 0;
-                if (self_pair) {  // query and target are the same tree
-                    const int64_t rel = qpos - (na + c0);
-                    if (rel >= 0 && rel < m) hm &= ~(1u << rel);
+                if (self_pair) {
+                    const int v = sself[w][lane];
+                    if ((v >> 5) == chunk) hm &= ~(1u << (v & 31));
                 }
                 const int nh = __popc(hm);
                 cnt += nh;
                 if (PASS == EP_RECORD) {
-                    if (hm) {
-                        if (nrec < rec_cap) recs[qpos * rec_cap + nrec] = make_int2(na + c0, (int32_t)hm);
-                        ++nrec;
+                    // One record per leaf segment with hits, in pop order.
+                    for (int k = 0; k < nseg; ++k) {
+                        const int2 sg = sseg[w][k];
+                        const int len = sseg[w][k + 1].y - sg.y;
+                        const unsigned sub = (hm >> sg.y) & (len >= 32 ? 0xffffffffu : ((1u << len) - 1u));
+                        if (sub) {
+                            if (nrec < rec_cap) recs[qpos * rec_cap + nrec] = make_int2(sg.x, (int32_t)sub);
+                            ++nrec;
+                        }
                     }
                 } else if (STAGE) {
                     if (__any_sync(0xffffffffu, ocnt + nh > kStage)) flush(ocnt + nh > kStage);
-                    const int32_t b0 = na + c0;
-                    while (hm) {
-                        const int j = __ffs(hm) - 1;
-                        hm &= hm - 1;
-                        obuf[w][lane][ocnt++] = b0 + j;
+                    for (int k = 0; k < nseg; ++k) {
+                        const int2 sg = sseg[w][k];
+                        const int len = sseg[w][k + 1].y - sg.y;
+                        unsigned sub = (hm >> sg.y) & (len >= 32 ? 0xffffffffu : ((1u << len) - 1u));
+                        while (sub) {
+                            const int j = __ffs(sub) - 1;
+                            sub &= sub - 1;
+                            obuf[w][lane][ocnt++] = sg.x + j;
+                        }
                     }
                 }
             }
