@@ -137,6 +137,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     int nrec = 0;
     int chunk = 0;  // leaf chunks processed by this warp (warp-uniform)
     sself[w][lane] = -1;
+    const int cap = (int)rec_cap;
+    int2* myrec = PASS == EP_RECORD ? recs + qpos * rec_cap : nullptr;  // this query's records
 
     // One query per round: lane e writes the query's e-th staged edge, so a
     // round stores a run of consecutive edges of one segment.  Only the lanes
@@ -206,7 +208,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                     }
                 }
                 if (lane == 0) sseg[w][nseg] = make_int2(0, total);
-                const int mp = (total + 1) & ~1;  // padded to whole pairs with +inf points
+                const int mp = (total + 3) & ~3;  // padded to whole pairs of pairs with +inf points
                 ++chunk;
                 __syncwarp();
                 if (lane < total) {
@@ -230,19 +232,25 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                     unsigned long long P[D];
 #pragma unroll
                     for (int d = 0; d < D; ++d) P[d] = pack2(q.x[d], q.x[d]);
-                    for (int j = 0; j < mp; j += 2) {
-                        // Two targets at once: packed differences and squares,
-                        // scalar sums ((dx*dx + dy*dy) + dz*dz) per element.
-                        float s0 = 0.f, s1 = 0.f;
+                    for (int j = 0; j < mp; j += 4) {
+                        // Four targets per step, two per packed operation:
+                        // packed differences and squares, scalar sums
+                        // ((dx*dx + dy*dy) + dz*dz) per element.
+                        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
                         for (int d = 0; d < D; ++d) {
-                            const unsigned long long dd =
-                                sub2_rn(*reinterpret_cast<const unsigned long long*>(&sx[w][d][j]), P[d]);
-                            const unsigned long long sq = mul2_rn(dd, dd);
-                            s0 = (d == 0) ? lo2(sq) : __fadd_rn(s0, lo2(sq));
-                            s1 = (d == 0) ? hi2(sq) : __fadd_rn(s1, hi2(sq));
+                            const unsigned long long* px = reinterpret_cast<const unsigned long long*>(&sx[w][d][j]);
+                            const unsigned long long da = sub2_rn(px[0], P[d]);
+                            const unsigned long long db = sub2_rn(px[1], P[d]);
+                            const unsigned long long qa = mul2_rn(da, da);
+                            const unsigned long long qb = mul2_rn(db, db);
+                            s0 = (d == 0) ? lo2(qa) : __fadd_rn(s0, lo2(qa));
+                            s1 = (d == 0) ? hi2(qa) : __fadd_rn(s1, hi2(qa));
+                            s2 = (d == 0) ? lo2(qb) : __fadd_rn(s2, lo2(qb));
+                            s3 = (d == 0) ? hi2(qb) : __fadd_rn(s3, hi2(qb));
                         }
-                        hm |= ((s0 <= r2 ? 1u : 0u) | (s1 <= r2 ? 2u : 0u)) << j;
+                        hm |= ((s0 <= r2 ? 1u : 0u) | (s1 <= r2 ? 2u : 0u) | (s2 <= r2 ? 4u : 0u) |
+                               (s3 <= r2 ? 8u : 0u)) << j;
                     }
                 } else {
                     for (int j = 0; j < total; ++j) {
@@ -261,13 +269,13 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 cnt += nh;
                 if (PASS == EP_RECORD) {
                     // One record per leaf segment with hits, in pop order.
-                    for (int k = 0; k < nseg; ++k) {
-                        const int2 sg = sseg[w][k];
-                        const int len = sseg[w][k + 1].y - sg.y;
-                        const unsigned sub = (hm >> sg.y) & (len >= 32 ? 0xffffffffu : ((1u << len) - 1u));
-                        if (sub) {
-                            if (nrec < rec_cap) recs[qpos * rec_cap + nrec] = make_int2(sg.x, (int32_t)sub);
-                            ++nrec;
+                    if (__any_sync(0xffffffffu, hm != 0)) {
+                        for (int k = 0; k < nseg; ++k) {
+                            const int2 sg = sseg[w][k];
+                            const int len = sseg[w][k + 1].y - sg.y;
+                            const unsigned sub = (hm >> sg.y) & (0xffffffffu >> (32 - len));
+                            if (sub != 0u && nrec < cap) myrec[nrec] = make_int2(sg.x, (int32_t)sub);
+                            nrec += sub != 0u;
                         }
                     }
                 } else if (STAGE) {
@@ -312,7 +320,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     if (STAGE) flush(true);
     if (PASS != EP_FILL && valid) counts[q.idx] = (int32_t)cnt;
     if (PASS == EP_RECORD) {
-        const bool over = __any_sync(0xffffffffu, nrec > rec_cap);
+        const bool over = __any_sync(0xffffffffu, nrec > cap);
         if (valid) rcount[qpos] = over ? kOverflowMark : (uint8_t)nrec;
         int mx = nrec;
 #pragma unroll
@@ -320,7 +328,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
         if (lane == 0) {
             gflag[g] = over ? 1 : 0;
             if (over) atomicAdd(ocount, 1);
-            atomicMax(ocount + 1, mx);
+            // The maximum settles after a few groups: most groups only read it.
+            if (mx > __ldcg(ocount + 1)) atomicMax(ocount + 1, mx);
         }
     }
 }
