@@ -53,10 +53,10 @@ def phase_bytes(n, e, n_nodes, path):
     k_resort_mark + k_resort_merge, which also gathers)."""
     b = {"bounds": 12 * n}                          # coordinates read once
     if path == 1:
-        b["encode"] = (4 + 12 + 4 + 1 + 8) * n        # perm, gathered coords, old key in; flag, Morton code out
+        b["encode"] = (4 + 12 + 4 + 1) * n            # perm, gathered coords, old key in; changed flag out
         b["sort"] = (4 + 4 + 1 + 12 + 4 + 4 + 16 + 4) * n  # key, perm, flag, coords in; key, perm, point, inverse out
     else:
-        b["encode"] = (12 + 4 + 8) * n                # coords in; key and Morton code out
+        b["encode"] = (12 + 4) * n                    # coords in; key out
         b["sort"] = 3 * (4 + 4 + 4 + 4 + 4) * n + (4 + 12 + 16 + 4) * n  # 3 passes + gather
     b["refit"] = 16 * n + 2 * 32 * n_nodes          # sorted points in; node records read and written
     b["fill"] = (12 + 4 * 3) * e + 8 * n            # (12 + 4D) E + 8N

@@ -144,7 +144,7 @@ __device__ __forceinline__ uint64_t cell_key(const T* __restrict__ x, const T* o
 template <class T, int D, class K>
 __global__ void __launch_bounds__(kThreads) k_encode(const T* __restrict__ coords, int64_t n, T o0, T o1, T o2,
                                                      T inv_cs, K* __restrict__ keys,
-                                                     uint64_t* __restrict__ morton_out, Batch bt) {
+                                                     Batch bt) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     T o[3] = {o0, o1, o2};
@@ -160,7 +160,6 @@ __global__ void __launch_bounds__(kThreads) k_encode(const T* __restrict__ coord
     }
     const uint64_t key = cell_key<T, D>(coords + D * i, o, inv_cs);
     keys[i] = bt.n_clouds ? (K)(((uint64_t)cloud << bt.kbits) | key) : (K)key;
-    if (morton_out) morton_out[i] = key;
 }
 
 // ------------------------------------------------------------ 4. gather --
@@ -556,6 +555,15 @@ __global__ void k_view_perm(const SPt<T, D>* __restrict__ spts, int64_t n, int32
     if (k < n) vp[k] = spts[k].idx + 1;
 }
 
+// The retained per-point Morton codes of refit mode (src/api.jl:234-238),
+// scattered from the sorted keys on demand: morton[perm[k]] = key[k].
+template <class T, int D, class K>
+__global__ void k_view_morton(const SPt<T, D>* __restrict__ spts, const K* __restrict__ skeys, int64_t n,
+                              uint64_t* __restrict__ morton) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) morton[spts[k].idx] = (uint64_t)skeys[k];
+}
+
 // --------------------------------------------------------- 9. batches ----
 // Per-cloud min/max (Julia order) and non-finite flag, one block per cloud:
 // out[c*8 + 0..2] = min, [3..5] = max, [6] = non-finite.
@@ -672,8 +680,7 @@ __global__ void __launch_bounds__(kThreads) k_resort_mark(const T* __restrict__ 
                                                           const int32_t* __restrict__ perm,
                                                           const K* __restrict__ keys, T inv_cs, OctHeader* hdr,
                                                           uint8_t* __restrict__ changed, int32_t* __restrict__ blockcnt,
-                                                          K* __restrict__ mk, int32_t* __restrict__ mv, int64_t cap,
-                                                          uint64_t* __restrict__ morton_out) {
+                                                          K* __restrict__ mk, int32_t* __restrict__ mv, int64_t cap) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool c = false;
     K nk = 0;
@@ -687,7 +694,6 @@ __global__ void __launch_bounds__(kThreads) k_resort_mark(const T* __restrict__ 
         nk = (K)key;
         c = nk != keys[p];
         changed[p] = (uint8_t)c;
-        if (morton_out) morton_out[i] = key;
     }
     const unsigned bal = __ballot_sync(0xffffffffu, c);
     if (bal) {
@@ -894,15 +900,10 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         if ((err = ensure(t.keys[0], (size_t)n * sizeof(K))) || (err = ensure(t.keys[1], (size_t)n * sizeof(K))) ||
             (err = ensure(t.vals[0], (size_t)n * 4)) || (err = ensure(t.vals[1], (size_t)n * 4)))
             return cuda_status(ctx, err, "allocating sort buffers");
-        uint64_t* morton = nullptr;
-        if (t.keep_morton) {
-            if ((err = ensure(t.morton, (size_t)n * 8))) return cuda_status(ctx, err, "allocating morton codes");
-            morton = t.morton.as<uint64_t>();
-        }
         {
             PhaseTimer pt_(ctx, PH_ENCODE);
             k_encode<T, D, K><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, n, o[0], o[1], o[2], inv_cs,
-                                                                        t.keys[0].as<K>(), morton, bt);
+                                                                        t.keys[0].as<K>(), bt);
             ctx.kernel_launches += 1;
         }
 
@@ -959,6 +960,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             t.last_path = 2;
             t.sorted_buf = sorted;
             t.perm_dev = vp;
+            t.skeys_dev = skeys;
             return OK;
         }
         const int nb = div_up(n, kThreads);
@@ -1067,6 +1069,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         t.dfs_start = t.hdr_host->dfs_start;
         t.sorted_buf = sorted;
         t.perm_dev = perm;
+        t.skeys_dev = skeys;
         return OK;
     }
     return set_error(ctx, ERR_OVERFLOW, "tree build: node capacity retry did not converge");
@@ -1081,15 +1084,13 @@ int resort_mark(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int pre
     const int nb = div_up(n, kThreads);
     if ((err = ensure(t.rflag, (size_t)n)) || (err = ensure(t.rcnt, (size_t)nb * 4)) ||
         (err = ensure(t.roff, (size_t)(nb + 1) * 8)) || (err = ensure(t.scan_tmp, (size_t)scan_tmp_elems(nb) * 8)) ||
-        (err = ensure(t.mkeys, (size_t)cap * sizeof(K))) || (err = ensure(t.mvals, (size_t)cap * 4)) ||
-        (t.keep_morton && (err = ensure(t.morton, (size_t)n * 8))))
+        (err = ensure(t.mkeys, (size_t)cap * sizeof(K))) || (err = ensure(t.mvals, (size_t)cap * 4)))
         return cuda_status(ctx, err, "allocating refit-mode scratch");
     OctHeader* hdr = t.hdr.as<OctHeader>();
     PhaseTimer pt_(ctx, PH_ENCODE);
     k_resort_mark<T, D, K><<<nb, kThreads, 0, s>>>(coords, n, t.vals[prev].as<int32_t>(), t.keys[prev].as<K>(),
                                                     T(1) / radius, hdr, t.rflag.as<uint8_t>(), t.rcnt.as<int32_t>(),
-                                                    t.mkeys.as<K>(), t.mvals.as<int32_t>(), cap,
-                                                    t.keep_morton ? t.morton.as<uint64_t>() : nullptr);
+                                                    t.mkeys.as<K>(), t.mvals.as<int32_t>(), cap);
     ctx.kernel_launches += 1 + exclusive_scan_i32_i64(t.rcnt.as<int32_t>(), t.roff.as<int64_t>(), nb, nullptr,
                                                       t.scan_tmp.as<int64_t>(), s);
     return OK;
@@ -1325,6 +1326,15 @@ int view_typed(Ctx& ctx, Tree& t) {
     if (t.n > 0)
         k_view_perm<T, D><<<div_up(t.n, kThreads), kThreads, 0, ctx.stream>>>(t.spts.as<SPt<T, D>>(), t.n,
                                                                                t.v_perm.as<int32_t>());
+    if (t.keep_morton && t.n > 0 && !t.n_clouds) {
+        if ((err = ensure(t.morton, (size_t)t.n * 8))) return cuda_status(ctx, err, "allocating morton codes");
+        if (t.key_bytes == 4)
+            k_view_morton<T, D, uint32_t><<<div_up(t.n, kThreads), kThreads, 0, ctx.stream>>>(
+                t.spts.as<SPt<T, D>>(), (const uint32_t*)t.skeys_dev, t.n, t.morton.as<uint64_t>());
+        else
+            k_view_morton<T, D, uint64_t><<<div_up(t.n, kThreads), kThreads, 0, ctx.stream>>>(
+                t.spts.as<SPt<T, D>>(), (const uint64_t*)t.skeys_dev, t.n, t.morton.as<uint64_t>());
+    }
     if ((err = cudaStreamSynchronize(ctx.stream))) return cuda_status(ctx, err, "materializing views");
     t.view_valid = true;
     return OK;

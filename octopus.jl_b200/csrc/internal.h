@@ -71,6 +71,7 @@ struct Tree {
     DevBuf spts;                 // SPt<T,D>[n] in Morton order
     DevBuf iperm;                // int32 [n]: sorted position of each original point
     const int32_t* perm_dev = nullptr;  // original index of each sorted position (null: identity)
+    const void* skeys_dev = nullptr;    // sorted keys of the last build (key_bytes wide)
     DevBuf tnode;                // TNode<T,D>[capacity]
     DevBuf nrange;               // int2 {first,last} 0-based per node
     DevBuf parent;               // int32 per node (-1 for the root)
@@ -82,7 +83,7 @@ struct Tree {
     DevBuf scan_tmp;             // int64 tile sums for scans
     DevBuf partials;             // double per-block bounds partials
     DevBuf hdr;                  // OctHeader
-    DevBuf morton;               // uint64 per original point (refit mode)
+    DevBuf morton;               // uint64 per original point (refit mode), filled with the views
     DevBuf groups;               // int2 {first position, count <= 32}: query groups
     DevBuf gcnt;                 // int32 per node: groups formed under it
     DevBuf goff;                 // int64 exclusive scan of gcnt (+1)
