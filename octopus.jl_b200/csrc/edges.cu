@@ -42,9 +42,10 @@ enum EdgePass {
     EP_FILL = 2,    // the COO at the scanned offsets by a second walk (groups whose records overflowed)
 };
 
-// A hit record: the sorted position of a leaf chunk's first point and the
-// bit mask of the chunk's points within the radius of one query.  A query's
-// records, in order, list its neighbors in the reference's order.
+// A hit record: the sorted position of a leaf's first point (of a leaf's
+// 32-point part, for a larger leaf) and the bit mask of its points within the
+// radius of one query.  A query's records, in order, list its neighbors in
+// the reference's order.
 constexpr int kMaxRecords = 240;  // per query: the record count is stored in one byte
 constexpr uint8_t kOverflowMark = 255;  // record count of the queries of an overflowed group
 
