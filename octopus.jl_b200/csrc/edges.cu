@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
 // lanes on consecutive edges.  Queries of an overflowed group (record count
 // kOverflowMark) are left to the walking fill.
 constexpr int kExpandWarps = 4;
-constexpr int kExpandCap = 1024;  // staged positions per warp: one round of 32 full records
+constexpr int kExpandCap = 512;  // staged positions per warp (at least 32: one record)
 
 template <class T, int D>
 struct ExpandSmem {
@@ -482,22 +482,34 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 8) k_expand(
             const int a = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += a;
         }
-        const int tr = __shfl_sync(0xffffffffu, incl, 31);
-        if (used + tr > kExpandCap) {
-            write_batch(used);
-            ebase += used;
-            used = 0;
+        // Stage the round's records in parts that fit the free positions,
+        // writing the staged edges out whenever the next record does not fit.
+        int lo = 0, base_incl = 0;  // lanes below `lo` are staged (warp-uniform)
+        while (lo < 32) {
+            const bool fits = lane >= lo && incl - base_incl <= kExpandCap - used;
+            const int hi = lo + __popc(__ballot_sync(0xffffffffu, fits));
+            if (hi == lo) {
+                write_batch(used);
+                ebase += used;
+                used = 0;
+                continue;
+            }
+            if (fits) {
+                int at = used + (incl - p - base_incl);
+                unsigned m = (unsigned)rec.y;
+                while (m) {
+                    const int j = __ffs(m) - 1;
+                    m &= m - 1;
+                    sm.who[at] = (uint8_t)qr;
+                    sm.pos[at++] = rec.x + j;
+                }
+            }
+            const int hi_incl = __shfl_sync(0xffffffffu, incl, hi - 1);
+            used += hi_incl - base_incl;
+            base_incl = hi_incl;
+            lo = hi;
+            __syncwarp();
         }
-        int at = used + incl - p;
-        unsigned m = (unsigned)rec.y;
-        while (m) {
-            const int j = __ffs(m) - 1;
-            m &= m - 1;
-            sm.who[at] = (uint8_t)qr;
-            sm.pos[at++] = rec.x + j;
-        }
-        used += tr;
-        __syncwarp();
     }
     write_batch(used);
 }
