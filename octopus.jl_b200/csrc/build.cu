@@ -310,7 +310,8 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
                                                          const int32_t* __restrict__ first_child_in,
                                                          TNode<T, D>* __restrict__ tnode, int2* __restrict__ nrange,
                                                          int32_t* __restrict__ parent, int32_t* __restrict__ arrive,
-                                                         int32_t* __restrict__ chain, const OctHeader* hdr, Batch bt) {
+                                                         int32_t* __restrict__ chain, const int64_t* __restrict__ blockoff,
+                                                         int nblocks, const OctHeader* hdr, Batch bt) {
     constexpr int BITS = Dims<D>::bits;
     constexpr int NCH = Dims<D>::nch;
     const int64_t nn = hdr->n_nodes;
@@ -356,28 +357,20 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
         nd.a = (int32_t)k;
         nd.b = (int32_t)(e - k);
     } else {
+        // The children are the consecutive level-(L+1) ids from first_child
+        // whose ranges start inside [k, e) (nrange[c].x, written by the id
+        // pass, is their first position); each one's slot is its key's digit.
         const int shd = D * BITS - D * (L + 1);
-        const int d0 = slot_digit<D, K>(skeys[k], shd, bt);
-        const int d1 = slot_digit<D, K>(skeys[e - 1], shd, bt);
-        unsigned slots = 1u << d0;
-        if (d1 != d0) {
-            // lb(v) = first position in [k, e) whose digit >= v; digit v is
-            // occupied iff lb(v) < lb(v + 1).
-            int64_t prev = k;
-            for (int v = d0 + 1; v <= d1; ++v) {
-                int64_t a = prev, b = e;
-                while (a < b) {
-                    const int64_t mid = (a + b) >> 1;
-                    if (slot_digit<D, K>(skeys[mid], shd, bt) >= v) b = mid; else a = mid + 1;
-                }
-                if (a < e && slot_digit<D, K>(skeys[a], shd, bt) == v) slots |= 1u << v;
-                prev = a;
-            }
+        const int64_t lend = L + 2 <= BITS ? blockoff[(int64_t)(L + 2) * nblocks] : nn;  // first id past level L+1
+        unsigned slots = 0u;
+        for (int64_t c = first_child; c < lend && c < (int64_t)first_child + NCH; ++c) {
+            const int64_t cs = nrange[c].x;
+            if (cs >= e) break;
+            slots |= 1u << slot_digit<D, K>(skeys[cs], shd, bt);
+            parent[c] = (int32_t)id;
         }
         nd.a = first_child;
         nd.b = -(int32_t)slots;
-        const int nc = __popc(slots);
-        for (int j = 0; j < nc; ++j) parent[first_child + j] = (int32_t)id;
     }
     if (k == s0 && e == s1) {
         // A node covering its whole point set has that set's bounds.
@@ -1027,7 +1020,8 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
                                                     t.fchild.as<int32_t>(), t.nrange.as<int2>(), hdr, bt);
         k_emit_nodes<T, D, K><<<div_up(cap, kThreads), kThreads, 0, s>>>(
             skeys, n, cap, t.fchild.as<int32_t>(), t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
-            t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.chain.as<int32_t>(), hdr, bt);
+            t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.chain.as<int32_t>(), t.blockoff.as<int64_t>(), nblocks,
+            hdr, bt);
         ctx.kernel_launches += 3;
         }
         {
