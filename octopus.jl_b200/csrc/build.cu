@@ -21,6 +21,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda/atomic>
+
 #include "internal.h"
 #include "scan.cuh"
 #include "sort.cuh"
@@ -434,10 +436,11 @@ __global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n,
         if (rg.x == s0 && (int64_t)rg.y == s1 - 1) break;  // bounds preset from the set's reduce
         const int32_t pa = tnode[p].a, pb = tnode[p].b;
         const int nc = __popc((unsigned)(-pb));
-        __threadfence();
-        const int old = atomicAdd(&arrive[p], 1);
+        // Release this node's bounds and, for the last arrival, acquire its
+        // siblings' (one acquire-release read-modify-write, no full fences).
+        const int old = cuda::atomic_ref<int32_t, cuda::thread_scope_device>(arrive[p]).fetch_add(
+            1, cuda::memory_order_acq_rel);
         if (old != nc - 1) break;
-        __threadfence();
 #pragma unroll
         for (int d = 0; d < D; ++d) { lo[d] = T(INFINITY); hi[d] = T(-INFINITY); }
         for (int c = 0; c < nc; ++c) {
