@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include <cuda/atomic>
@@ -46,14 +47,41 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const T* __restrict__ coord
 #pragma unroll
     for (int d = 0; d < D; ++d) { lo[d] = T(INFINITY); hi[d] = T(-INFINITY); }
     int bad = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-            const T x = coords[D * i + d];
-            if (!isfinite(x)) bad = 1;
-            lo[d] = jl_min(lo[d], x);
-            hi[d] = jl_max(hi[d], x);
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nthr = (int64_t)gridDim.x * blockDim.x;
+    auto take = [&](int d, T x) {
+        if (!isfinite(x)) bad = 1;
+        lo[d] = jl_min(lo[d], x);
+        hi[d] = jl_max(hi[d], x);
+    };
+    int64_t done = 0;  // points folded by the vector loop
+    if constexpr (std::is_same<T, float>::value && D == 3) {
+        if (((uintptr_t)coords & 15) == 0) {
+            // Four points = 12 floats = three float4 (axes x y z x | y z x y | z x y z),
+            // two groups of four points in flight per thread.
+            const float4* v = reinterpret_cast<const float4*>(coords);
+            const int64_t groups = n / 4;
+            for (int64_t g = tid; g < groups; g += 2 * nthr) {
+                const int64_t g2 = g + nthr;
+                const float4 a = v[3 * g], b = v[3 * g + 1], c = v[3 * g + 2];
+                float4 a2 = a, b2 = b, c2 = c;
+                if (g2 < groups) {
+                    a2 = v[3 * g2];
+                    b2 = v[3 * g2 + 1];
+                    c2 = v[3 * g2 + 2];
+                }
+                take(0, a.x); take(1, a.y); take(2, a.z); take(0, a.w);
+                take(1, b.x); take(2, b.y); take(0, b.z); take(1, b.w);
+                take(2, c.x); take(0, c.y); take(1, c.z); take(2, c.w);
+                take(0, a2.x); take(1, a2.y); take(2, a2.z); take(0, a2.w);
+                take(1, b2.x); take(2, b2.y); take(0, b2.z); take(1, b2.w);
+                take(2, c2.x); take(0, c2.y); take(1, c2.z); take(2, c2.w);
+            }
+            done = groups * 4;
         }
+    }
+    for (int64_t i = done + tid; i < n; i += nthr) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) take(d, coords[D * i + d]);
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
