@@ -191,7 +191,9 @@ def run_ours(args, rank, world, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     W, K = args.warmup, args.steps
-    host = snapshots_np(PER, W + K, 12345 + rank)
+    # W warm-up steps, K timed steps, then K more steps of the same trajectory
+    # with the library's phase timers on (the timed steps run without them).
+    host = snapshots_np(PER, W + 2 * K, 12345 + rank)
     snaps = [torch.from_numpy(x).to(dev).t() for x in host]  # (3, N) column-major views
     N = host[0].shape[0]
 
@@ -216,8 +218,6 @@ def run_ours(args, rank, world, local):
     nph = len(ob._lib.PHASES)
     ms_buf = (C.c_double * nph)()
     cnt_buf = (C.c_int64 * nph)()
-    lib.oct_profile_read(ctx.handle, ms_buf, cnt_buf, nph)  # clear
-    lib.oct_profile_enable(ctx.handle, 1)
     launches0 = lib.oct_profile_kernel_launches(ctx.handle)
     clocks = ClockSampler(local)
     clocks.start()
@@ -235,13 +235,19 @@ def run_ours(args, rank, world, local):
     clk = clocks.stop()
     ms = t0.elapsed_time(t1)
     launches = lib.oct_profile_kernel_launches(ctx.handle) - launches0
+    # phase breakdown: the next K steps with the per-phase event timers on
+    lib.oct_profile_read(ctx.handle, ms_buf, cnt_buf, nph)  # clear
+    lib.oct_profile_enable(ctx.handle, 1)
+    for k in range(K):
+        step(snaps[W + K + k])
+    torch.cuda.synchronize()
     lib.oct_profile_read(ctx.handle, ms_buf, cnt_buf, nph)
     lib.oct_profile_enable(ctx.handle, 0)
     phases = {ob._lib.PHASES[i]: round(ms_buf[i] / K, 5) for i in range(nph) if cnt_buf[i]}
     phase_calls = {ob._lib.PHASES[i]: int(cnt_buf[i]) for i in range(nph) if cnt_buf[i]}
 
     # --- end to end through host buffers (pinned), same steps
-    hpin = [torch.from_numpy(x).pin_memory() for x in host]
+    hpin = [torch.from_numpy(x).pin_memory() for x in host[:W + K]]
     dcoords = torch.empty((N, 3), dtype=torch.float32, device=dev)
     e_last = edges // K
     cap = int(e_last * 1.2) + 1024

@@ -1081,7 +1081,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             }
         }
         if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
-            (err = cudaStreamSynchronize(s)))
+            (err = wait_stream(s)))
             return cuda_status(ctx, err, "tree build");
         if (t.hdr_host->status & DF_NODE_OVERFLOW) {
             t.capacity = t.hdr_host->n_nodes + t.hdr_host->n_nodes / 8 + 64;
@@ -1154,7 +1154,7 @@ int build_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, double radius_d) 
         if (st != OK) return st;
     }
     if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
-        (err = cudaStreamSynchronize(s)))
+        (err = wait_stream(s)))
         return cuda_status(ctx, err, "bounds reduce");
     if (t.hdr_host->nan_flag)
         return set_error(ctx, ERR_INEXACT, "InexactError: floor(Int32, NaN/Inf) in bin_point (non-finite coordinate)");
@@ -1217,7 +1217,7 @@ int build_batch_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, const int64
     }
     std::vector<double> cb((size_t)nc * 8);
     if ((err = cudaMemcpyAsync(cb.data(), t.b_cbounds.p, cb.size() * 8, cudaMemcpyDeviceToHost, s)) ||
-        (err = cudaStreamSynchronize(s)))
+        (err = wait_stream(s)))
         return cuda_status(ctx, err, "cloud bounds");
     // Per cloud, in T, exactly what a TNS of that cloud alone computes
     // (src/cpu/bin_cpu.jl:22,35,60; src/cpu/edges_cpu.jl:184-185).
@@ -1305,7 +1305,7 @@ int batch_edge_offsets(Ctx& ctx, Tree& t, int64_t* out_host) {
                                                                         nc, t.b_eoff.as<int64_t>());
     ctx.kernel_launches += 1;
     if ((err = cudaMemcpyAsync(out_host, t.b_eoff.p, (size_t)(nc + 1) * 8, cudaMemcpyDeviceToHost, ctx.stream)) ||
-        (err = cudaStreamSynchronize(ctx.stream)))
+        (err = wait_stream(ctx.stream)))
         return cuda_status(ctx, err, "batch edge offsets");
     return OK;
 }

@@ -226,7 +226,7 @@ int twins_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_
     ctx.kernel_launches += 2;
     int missing = 0;
     if ((err = cudaMemcpyAsync(&missing, missing_flag, 4, cudaMemcpyDeviceToHost, s)) ||
-        (err = cudaStreamSynchronize(s)))
+        (err = wait_stream(s)))
         return cuda_status(ctx, err, "adjoint");
     *ok = missing == 0;
     if (!*ok) return OK;

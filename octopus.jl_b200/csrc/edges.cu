@@ -626,7 +626,7 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
                                                       ctx.total.as<int64_t>(), ctx.scan_tmp.as<int64_t>(), s);
     }
     if ((err = cudaMemcpyAsync(ctx.total_host, ctx.total.p, 16, cudaMemcpyDeviceToHost, s)) ||
-        (err = cudaStreamSynchronize(s)))
+        (err = wait_stream(s)))
         return cuda_status(ctx, err, "edge count");
     *n_edges = ctx.total_host[0];
     ctx.rec_overflow = 0;

@@ -1,6 +1,7 @@
 // Library-internal objects shared by the build, edge and C-ABI translation units.
 #pragma once
 
+#include <chrono>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -164,6 +165,19 @@ struct Ctx {
     std::vector<cudaEvent_t> event_pool;
     cudaEvent_t get_event();
 };
+
+// Waits for the work queued on `s` by polling it: the library's host round
+// trips (bounds, node count, edge count) sit between short kernels, where a
+// blocking synchronize would add the host thread's wake-up latency each
+// time.  After 200 ms of polling it blocks instead.
+inline cudaError_t wait_stream(cudaStream_t s) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t e = cudaStreamQuery(s);
+        if (e != cudaErrorNotReady) return e;
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(200)) return cudaStreamSynchronize(s);
+    }
+}
 
 // Build pipeline (build.cu).  Returns a Status.
 int build_tree(Ctx& ctx, Tree& t, const void* coords, int64_t n, double radius);
