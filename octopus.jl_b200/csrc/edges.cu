@@ -33,6 +33,8 @@ namespace oct {
 constexpr int kEdgeWarps = 4;
 constexpr int kEdgeThreads = kEdgeWarps * 32;
 constexpr int kStage = 32;  // staged hits per lane, and points per leaf sub-chunk
+constexpr int kMultiPop = 4;     // internal nodes expanded together
+constexpr int kMultiLimit = 64;  // stack depth up to which they are
 constexpr int kMaxSeg = 16;  // leaves sharing one chunk
 
 // The three passes of k_edges.
@@ -95,10 +97,15 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ ocount,
     int2* __restrict__ recs, int64_t rec_cap, uint8_t* __restrict__ rcount, uint8_t* __restrict__ gflag, Batch bt) {
     constexpr bool STAGE = PASS == EP_FILL;
-    constexpr int SD = stack_depth<D>();
+    // The usual DFS bound, plus the room the multi-node expansions may take.
+    constexpr int SD = stack_depth<D>() + kMultiLimit + 8;
     // Stack entries are the pushed node's (a, b) record; bit 31 of a marks
     // ascending-order subtrees (see below).
     __shared__ int2 stack[kEdgeWarps][SD];
+    // The internal nodes expanded together: their stack entries and the
+    // first lane of each one's children.
+    __shared__ int2 snode[kEdgeWarps][kMultiPop];
+    __shared__ int soff[kEdgeWarps][kMultiPop + 1];
     // The current leaf chunk, structure of arrays so pairs load as 8 bytes,
     // its leaf segments (first position, first slot; entry nseg holds the
     // point count), and per query lane the chunk slot of its own point
@@ -294,27 +301,61 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 }
             }
         } else {
+            // Internal nodes.  The popped node and up to kMultiPop - 1 further
+            // internal entries at the stack top (the nodes the DFS expands
+            // next) have their children box-tested together, one lane per
+            // child; each node's passing children are pushed as a block, the
+            // first node's on top, so the visiting order is unchanged.  Only
+            // while the stack stays at most kMultiLimit deep: beyond it the
+            // usual single expansions bound the depth.
             // The reference scans an internal node whose first child slot is
             // empty as one leaf, in ascending position order
             // (src/cpu/iterator_cpu.jl:87-101).  Below such a node the
             // children are therefore visited in ascending slot order.
-            const unsigned slots = (unsigned)(-nb);
-            const bool casc = asc || !(slots & 1u);
-            const int nc = __popc(slots);
+            int nnodes = 1, totc = __popc((unsigned)(-nb));
+            if (lane == 0) {
+                snode[w][0] = ent;
+                soff[w][0] = 0;
+            }
+            while (nnodes < kMultiPop && sp > 0) {
+                const int2 nx = stack[w][sp - 1];
+                if (nx.y > 0) break;
+                const int c = __popc((unsigned)(-nx.y));
+                if (totc + c > 32 || sp - 1 + totc + c > kMultiLimit) break;
+                --sp;
+                if (lane == 0) {
+                    snode[w][nnodes] = nx;
+                    soff[w][nnodes] = totc;
+                }
+                totc += c;
+                ++nnodes;
+            }
+            if (lane == 0) soff[w][nnodes] = totc;
+            __syncwarp();
+            int j = 0;
+            if (lane < totc)
+                while (soff[w][j + 1] <= lane) ++j;
+            const int2 nd = snode[w][j];
+            const unsigned slots = (unsigned)(-nd.y);
+            const bool casc = nd.x < 0 || !(slots & 1u);
+            const int o = soff[w][j], o2 = soff[w][j + 1];
             bool pass = false;
             int2 rec = make_int2(0, 0);
-            if (lane < nc) {
-                const TNode<T, D> c = tnode[na + lane];
+            if (lane < totc) {
+                const TNode<T, D> c = tnode[(nd.x & 0x7fffffff) + (lane - o)];
                 pass = box_gap2<T, D>(qlo, qhi, c.lo, c.hi) <= r2;
                 rec = make_int2(c.a | (casc ? (int32_t)0x80000000 : 0), c.b);
             }
             const unsigned m = __ballot_sync(0xffffffffu, pass);
-            const int np = __popc(m);
             if (pass) {
-                const int rk = __popc(m & lanemask_lt());
-                stack[w][casc ? sp + np - 1 - rk : sp + rk] = rec;
+                const unsigned upto = o2 >= 32 ? 0xffffffffu : ((1u << o2) - 1u);  // lanes of nodes <= j
+                const unsigned mine = m & upto & ~((1u << o) - 1u);
+                const int deeper = __popc(m & ~upto);  // passing children of the later nodes, below
+                const int np = __popc(mine);
+                const int rk = __popc(mine & lanemask_lt());
+                stack[w][sp + deeper + (casc ? np - 1 - rk : rk)] = rec;
             }
-            sp += np;
+            sp += __popc(m);
             __syncwarp();
         }
     }
