@@ -676,6 +676,9 @@ __global__ void k_gather_edge_offsets(const int64_t* __restrict__ offsets, const
 // bounds are recomputed.
 constexpr int kChunk = 2048;
 constexpr int64_t kMaxMerged = 65536;  // above this many changed keys a full sort is cheaper
+inline int64_t merge_cap(int64_t n) { return std::min<int64_t>(kMaxMerged, std::max<int64_t>(kChunk, n / 8)); }
+constexpr int64_t kSpeculate = -2;  // run_pipeline: merge with the count of changed keys still on the device
+constexpr int kRetry = -1;          // run_pipeline: the speculative merge did not apply
 
 template <class K>
 __device__ __forceinline__ bool key_less(K ka, int32_t ia, K kb, int32_t ib) {
@@ -716,6 +719,7 @@ __global__ void __launch_bounds__(kThreads) k_resort_mark(const T* __restrict__ 
         i = perm[p];
         const uint64_t key = cell_key<T, D>(coords + (int64_t)D * i, o, inv_cs);
         nk = (K)key;
+        if ((uint64_t)nk != key) atomicOr(&hdr->status, (int)DF_KEY_WIDTH);
         c = nk != keys[p];
         changed[p] = (uint8_t)c;
     }
@@ -738,13 +742,19 @@ __global__ void __launch_bounds__(kThreads) k_resort_mark(const T* __restrict__ 
 }
 
 // Sorts each chunk of up to kChunk changed keys by (key, index) in shared
-// memory: a bitonic network of `width` (a power of two, blockDim.x * 2)
-// entries, one compare-exchange per thread and stage.
+// memory: a bitonic network of `width` entries (a power of two, the chunk
+// size rounded up), width / 2 compare-exchanges per stage shared by the
+// block's threads.  The count m is read on the device (*m_ptr); nothing is sorted
+// when m exceeds cap.
 template <class K>
-__global__ void __launch_bounds__(kChunk / 2) k_moved_sort(int64_t m, int width, K* __restrict__ mk,
-                                                           int32_t* __restrict__ mv) {
+__global__ void __launch_bounds__(kChunk / 2) k_moved_sort(const int64_t* __restrict__ m_ptr, int64_t cap,
+                                                           K* __restrict__ mk, int32_t* __restrict__ mv) {
     __shared__ K sk[kChunk];
     __shared__ int32_t sv[kChunk];
+    const int64_t m = *m_ptr;
+    if (m > cap || (int64_t)blockIdx.x * kChunk >= m) return;  // block-uniform
+    int width = 64;
+    while (width < m && width < kChunk) width <<= 1;
     const int64_t base = (int64_t)blockIdx.x * kChunk;
     for (int t = threadIdx.x; t < width; t += blockDim.x) {
         const int64_t j = base + t;
@@ -757,19 +767,20 @@ __global__ void __launch_bounds__(kChunk / 2) k_moved_sort(int64_t m, int width,
         }
     }
     __syncthreads();
-    const int t = threadIdx.x;
     for (int size = 2; size <= width; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            const int i = 2 * t - (t & (stride - 1));
-            const int j = i + stride;
-            const bool up = (i & size) == 0;
-            const K ki = sk[i], kj = sk[j];
-            const int32_t vi = sv[i], vj = sv[j];
-            if (key_less(kj, vj, ki, vi) == up) {
-                sk[i] = kj;
-                sk[j] = ki;
-                sv[i] = vj;
-                sv[j] = vi;
+            for (int t = threadIdx.x; t < width / 2; t += blockDim.x) {
+                const int i = 2 * t - (t & (stride - 1));
+                const int j = i + stride;
+                const bool up = (i & size) == 0;
+                const K ki = sk[i], kj = sk[j];
+                const int32_t vi = sv[i], vj = sv[j];
+                if (key_less(kj, vj, ki, vi) == up) {
+                    sk[i] = kj;
+                    sk[j] = ki;
+                    sv[i] = vj;
+                    sv[j] = vi;
+                }
             }
             __syncthreads();
         }
@@ -786,11 +797,12 @@ __global__ void __launch_bounds__(kChunk / 2) k_moved_sort(int64_t m, int width,
 // Global rank of each changed key: its rank in its own chunk plus the number
 // of smaller keys in every other chunk.
 template <class K>
-__global__ void __launch_bounds__(kThreads) k_moved_rank(int64_t m, const K* __restrict__ ck,
-                                                         const int32_t* __restrict__ cv, K* __restrict__ sk,
-                                                         int32_t* __restrict__ sv) {
+__global__ void __launch_bounds__(kThreads) k_moved_rank(const int64_t* __restrict__ m_ptr, int64_t cap,
+                                                         const K* __restrict__ ck, const int32_t* __restrict__ cv,
+                                                         K* __restrict__ sk, int32_t* __restrict__ sv) {
+    const int64_t m = *m_ptr;
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= m) return;
+    if (m > cap || m <= kChunk || j >= m) return;  // one chunk is already in order
     const K key = ck[j];
     const int32_t idx = cv[j];
     const int64_t own = j / kChunk;
@@ -824,16 +836,28 @@ __device__ __forceinline__ void put_sorted(int64_t pos, K key, int32_t idx, cons
 // sorted points (the gather of section 4).  changed_before[b] counts the
 // changed positions before block b.
 template <class T, int D, class K>
-__global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, int64_t m, const K* __restrict__ keys,
+__global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, const int64_t* __restrict__ m_ptr, int64_t cap,
+                                                           const K* __restrict__ keys,
                                                            const int32_t* __restrict__ perm,
                                                            const uint8_t* __restrict__ changed,
                                                            const int64_t* __restrict__ changed_before,
-                                                           const K* __restrict__ mk, const int32_t* __restrict__ mv,
+                                                           const K* __restrict__ mk1, const int32_t* __restrict__ mv1,
+                                                           const K* __restrict__ mk2, const int32_t* __restrict__ mv2,
                                                            const T* __restrict__ coords, K* __restrict__ okeys,
                                                            int32_t* __restrict__ operm, SPt<T, D>* __restrict__ spts,
                                                            int32_t* __restrict__ iperm) {
     __shared__ int wsum[kThreads / 32];
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t m = *m_ptr;
+    if (m > cap) {
+        // Too many changed keys for a merge (the caller sorts afresh): keep
+        // the previous order, so that what follows reads a valid permutation.
+        if (p < n) put_sorted<T, D, K>(p, keys[p], perm[p], coords, okeys, operm, spts, iperm);
+        return;
+    }
+    // Sorted changed keys: ranked across chunks when there are several.
+    const K* __restrict__ mk = m > kChunk ? mk2 : mk1;
+    const int32_t* __restrict__ mv = m > kChunk ? mv2 : mv1;
     if (m == n) {  // every key changed: the sorted changed keys are the result
         if (p < n) put_sorted<T, D, K>(p, mk[p], mv[p], coords, okeys, operm, spts, iperm);
         return;
@@ -919,7 +943,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
     const K* skeys;
     const int32_t* perm;
     int sorted = -1;  // buffer holding this build's sorted keys and permutation
-    if (moved < 0) {
+    if (moved == -1) {  // a full sort
         // --- encode
         if ((err = ensure(t.keys[0], (size_t)n * sizeof(K))) || (err = ensure(t.keys[1], (size_t)n * sizeof(K))) ||
             (err = ensure(t.vals[0], (size_t)n * 4)) || (err = ensure(t.vals[1], (size_t)n * 4)))
@@ -985,13 +1009,18 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             t.sorted_buf = sorted;
             t.perm_dev = vp;
             t.skeys_dev = skeys;
+            t.key_bytes = (int)sizeof(K);
             return OK;
         }
+        // The changed keys' count is read on the device; when it is not known
+        // yet (a speculative build) the grids cover the merge capacity.
         const int nb = div_up(n, kThreads);
-        const int64_t nchunks = div_up(moved, kChunk);
+        const int64_t mcap = merge_cap(n);
+        const int64_t mmax = moved == kSpeculate ? mcap : moved;
+        const int64_t nchunks = div_up(mmax, kChunk);
         int width = 64;
-        while (width < moved && width < kChunk) width <<= 1;
-        if ((err = ensure(t.mkeys2, (size_t)moved * sizeof(K))) || (err = ensure(t.mvals2, (size_t)moved * 4)))
+        while (width < mmax && width < kChunk) width <<= 1;
+        if ((err = ensure(t.mkeys2, (size_t)mmax * sizeof(K))) || (err = ensure(t.mvals2, (size_t)mmax * 4)))
             return cuda_status(ctx, err, "allocating changed keys");
         K* mk = t.mkeys.as<K>();
         int32_t* mv = t.mvals.as<int32_t>();
@@ -999,17 +1028,18 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         int32_t* ov = t.vals[1 - prev].as<int32_t>();
         {
             PhaseTimer pt_(ctx, PH_SORT);
-            k_moved_sort<K><<<(unsigned)nchunks, width / 2, 0, s>>>(moved, width, mk, mv);
+            // Threads per chunk: width / 2 when the count is known, else 256.
+            const int tpb = moved == kSpeculate ? 256 : std::max(32, width / 2);
+            k_moved_sort<K><<<(unsigned)nchunks, tpb, 0, s>>>(&hdr->n_moved, mcap, mk, mv);
             ctx.kernel_launches += 1;
             if (nchunks > 1) {
-                k_moved_rank<K><<<div_up(moved, kThreads), kThreads, 0, s>>>(moved, mk, mv, t.mkeys2.as<K>(),
-                                                                              t.mvals2.as<int32_t>());
-                mk = t.mkeys2.as<K>();
-                mv = t.mvals2.as<int32_t>();
+                k_moved_rank<K><<<div_up(mmax, kThreads), kThreads, 0, s>>>(&hdr->n_moved, mcap, mk, mv,
+                                                                             t.mkeys2.as<K>(), t.mvals2.as<int32_t>());
                 ctx.kernel_launches += 1;
             }
-            k_resort_merge<T, D, K><<<nb, kThreads, 0, s>>>(n, moved, kp, vp, t.rflag.as<uint8_t>(),
-                                                             t.roff.as<int64_t>(), mk, mv, coords, ok, ov,
+            k_resort_merge<T, D, K><<<nb, kThreads, 0, s>>>(n, &hdr->n_moved, mcap, kp, vp, t.rflag.as<uint8_t>(),
+                                                             t.roff.as<int64_t>(), mk, mv, t.mkeys2.as<K>(),
+                                                             t.mvals2.as<int32_t>(), coords, ok, ov,
                                                              t.spts.as<SPt<T, D>>(), t.iperm.as<int32_t>());
             ctx.kernel_launches += 1;
         }
@@ -1083,6 +1113,9 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
             (err = wait_stream(s)))
             return cuda_status(ctx, err, "tree build");
+        if (moved == kSpeculate &&
+            (t.hdr_host->nan_flag || t.hdr_host->n_moved > merge_cap(n) || (t.hdr_host->status & DF_KEY_WIDTH)))
+            return kRetry;  // the bounds say the merge did not apply: build again on the usual path
         if (t.hdr_host->status & DF_NODE_OVERFLOW) {
             t.capacity = t.hdr_host->n_nodes + t.hdr_host->n_nodes / 8 + 64;
             const int zero = 0;
@@ -1095,6 +1128,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         t.sorted_buf = sorted;
         t.perm_dev = perm;
         t.skeys_dev = skeys;
+        t.key_bytes = (int)sizeof(K);
         return OK;
     }
     return set_error(ctx, ERR_OVERFLOW, "tree build: node capacity retry did not converge");
@@ -1118,6 +1152,35 @@ int resort_mark(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int pre
                                                     t.mkeys.as<K>(), t.mvals.as<int32_t>(), cap);
     ctx.kernel_launches += 1 + exclusive_scan_i32_i64(t.rcnt.as<int32_t>(), t.roff.as<int64_t>(), nb, nullptr,
                                                       t.scan_tmp.as<int64_t>(), s);
+    return OK;
+}
+
+// Origin and key width on the host from the bounds in t.hdr_host, in T
+// (src/cpu/bin_cpu.jl:22,35,60); InexactError where the reference's
+// floor(Int32, ...) throws.
+template <class T, int D>
+int host_key_width(Ctx& ctx, Tree& t, T radius) {
+    if (t.hdr_host->nan_flag)
+        return set_error(ctx, ERR_INEXACT, "InexactError: floor(Int32, NaN/Inf) in bin_point (non-finite coordinate)");
+    const T inv_cs = T(1) / radius;
+    int64_t cmax_all = 0;
+    for (int d = 0; d < D; ++d) {
+        const T o = (T)t.hdr_host->gmin[d] - T(1e-6);
+        t.origin[d] = (double)o;
+        const T v = ((T)t.hdr_host->gmax[d] - o) * inv_cs;
+        const T f = std::floor(v);
+        if (!(f >= T(-2147483648.0) && f < T(2147483648.0)))
+            return set_error(ctx, ERR_INEXACT, "InexactError: floor(Int32, (p - origin) / radius) exceeds Int32");
+        int64_t c = (int64_t)f;
+        const int64_t cm = (1LL << Dims<D>::bits) - 1;
+        c = c < 0 ? 0 : (c > cm ? cm : c);
+        cmax_all = std::max(cmax_all, c);
+    }
+    int nbits_axis = 0;
+    while (nbits_axis < 63 && (cmax_all >> nbits_axis) != 0) ++nbits_axis;
+    t.key_bits = D * nbits_axis;
+    t.key_bytes = t.key_bits <= 32 ? 4 : 8;
+    t.sort_passes = (t.key_bits + 7) / 8;
     return OK;
 }
 
@@ -1147,38 +1210,38 @@ int build_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, double radius_d) 
     t.sorted_buf = -1;
     const bool try_resort = t.keep_morton && prev >= 0 && t.sorted_n == n && t.sorted_radius == radius_d;
     // Merge at most this many changed keys; more are cheaper to sort afresh.
-    const int64_t cap = std::min<int64_t>(kMaxMerged, std::max<int64_t>(kChunk, n / 8));
+    const int64_t cap = merge_cap(n);
     if (try_resort) {
         const int st = t.sorted_key_bytes == 4 ? resort_mark<T, D, uint32_t>(ctx, t, coords, n, radius, prev, cap)
                                                : resort_mark<T, D, uint64_t>(ctx, t, coords, n, radius, prev, cap);
         if (st != OK) return st;
     }
-    if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
-        (err = wait_stream(s)))
+    // Steady time stepping: the previous build merged its changed keys, so
+    // merge again without waiting for the bounds.  The round trip at the end
+    // of the topology brings the bounds, the count of changed keys and the
+    // key-width flag; if the merge did not apply, build again below.
+    if (try_resort && t.last_path == 1) {
+        const int st = t.sorted_key_bytes == 4
+                           ? run_pipeline<T, D, uint32_t>(ctx, t, coords, n, radius, kSpeculate, prev)
+                           : run_pipeline<T, D, uint64_t>(ctx, t, coords, n, radius, kSpeculate, prev);
+        if (st != kRetry) {
+            if (st != OK) return st;
+            const int kw = host_key_width<T, D>(ctx, t, radius);
+            if (kw != OK) return kw;
+            t.key_bytes = t.sorted_key_bytes;  // the width the keys were built with
+            t.last_moved = t.hdr_host->n_moved;
+            t.last_path = 1;
+            t.sorted_n = n;
+            t.sorted_radius = radius_d;
+            return OK;
+        }
+        t.sorted_buf = -1;
+    } else if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
+               (err = wait_stream(s))) {
         return cuda_status(ctx, err, "bounds reduce");
-    if (t.hdr_host->nan_flag)
-        return set_error(ctx, ERR_INEXACT, "InexactError: floor(Int32, NaN/Inf) in bin_point (non-finite coordinate)");
-
-    // --- origin and key width on the host, in T (src/cpu/bin_cpu.jl:22,35,60)
-    const T inv_cs = T(1) / radius;
-    int64_t cmax_all = 0;
-    for (int d = 0; d < D; ++d) {
-        const T o = (T)t.hdr_host->gmin[d] - T(1e-6);
-        t.origin[d] = (double)o;
-        const T v = ((T)t.hdr_host->gmax[d] - o) * inv_cs;
-        const T f = std::floor(v);
-        if (!(f >= T(-2147483648.0) && f < T(2147483648.0)))
-            return set_error(ctx, ERR_INEXACT, "InexactError: floor(Int32, (p - origin) / radius) exceeds Int32");
-        int64_t c = (int64_t)f;
-        const int64_t cm = (1LL << Dims<D>::bits) - 1;
-        c = c < 0 ? 0 : (c > cm ? cm : c);
-        cmax_all = std::max(cmax_all, c);
     }
-    int nbits_axis = 0;
-    while (nbits_axis < 63 && (cmax_all >> nbits_axis) != 0) ++nbits_axis;
-    t.key_bits = D * nbits_axis;
-    t.key_bytes = t.key_bits <= 32 ? 4 : 8;
-    t.sort_passes = (t.key_bits + 7) / 8;
+    const int kw = host_key_width<T, D>(ctx, t, radius);
+    if (kw != OK) return kw;
     // Merge the changed keys into the previous order unless they are too many
     // (or the key width changed).
     int64_t moved = -1;

@@ -27,6 +27,7 @@ enum DevFlag : int {
     DF_NODE_OVERFLOW = 2,
     DF_RANGE = 4,        // binning out of Int32 range
     DF_TIMEOUT = 8,
+    DF_KEY_WIDTH = 16,   // a re-encoded key does not fit the previous build's key width
 };
 
 constexpr int kWarp = 32;
