@@ -491,16 +491,18 @@ __global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n,
 // level, is cut into chunks of 32).  Siblings share a parent box, so a
 // group's points are spatially compact; a window of 32 consecutive sorted
 // positions can instead straddle a jump of the Morton curve and span the
-// whole domain.  pass 0 counts the groups formed under each node, pass 1
-// writes them at the scanned offsets.
-template <class T, int D, int PASS>
+// whole domain.  Each node counts the groups formed under it, a warp reserves
+// room for its nodes' groups with one atomic on hdr->n_groups, and each node
+// writes its groups there.  The groups' order does not matter: every result
+// is per query point.
+template <class T, int D>
 __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restrict__ tnode, int64_t capacity,
-                                                     int32_t* __restrict__ gcnt, const int64_t* __restrict__ goff,
-                                                     int2* __restrict__ groups, const int32_t* __restrict__ chain,
+                                                     int2* __restrict__ groups, int64_t group_cap,
+                                                     const int32_t* __restrict__ chain,
                                                      const int32_t* __restrict__ parent, OctHeader* hdr) {
     const int64_t nn = hdr->n_nodes;
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (!PASS && id == 0 && nn <= capacity) {
+    if (id == 0 && nn <= capacity) {
         // The DFS may start at the first chain node that is not an internal
         // node with a single child in slot 0: every node above it covers all
         // points (its box holds every query) and keeps descending order.
@@ -508,47 +510,64 @@ __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restri
         while (L < 32 && chain[32 + L] == 1) ++L;
         hdr->dfs_start = chain[L];
     }
-    if (nn > capacity || id >= capacity) return;
-    if (id >= nn) {
-        if (!PASS) gcnt[id] = 0;  // the scan runs over the whole capacity
-        return;
-    }
-    const TNode<T, D> nd = tnode[id];
-    int64_t out = PASS ? goff[id] : 0;
+    if (nn > capacity || (int64_t)blockIdx.x * blockDim.x >= nn) return;  // block-uniform
+    const bool live = id < nn;
+    // pass 0 counts the node's groups, pass 1 writes them from `out`.
+    int64_t out = 0;
     int32_t ng = 0;
-    auto emit = [&](int32_t first, int32_t count) {
-        if (PASS) groups[out + ng] = make_int2(first, count);
-        ++ng;
-    };
-    if (nd.b > 0) {
-        // Only a leaf root (one per cloud in a batch) forms groups of its own;
-        // other leaves are grouped by their parent.
-        if (parent[id] < 0)
-            for (int32_t c0 = 0; c0 < nd.b; c0 += 32) emit(nd.a + c0, min(32, nd.b - c0));
-    } else {
-        const int nc = __popc((unsigned)(-nd.b));
-        int32_t gfirst = 0, gcount = 0;
-        for (int j = 0; j < nc; ++j) {
-            const TNode<T, D> c = tnode[nd.a + j];
-            if (c.b <= 0) {  // internal child: close the open group
-                if (gcount) emit(gfirst, gcount);
-                gcount = 0;
-            } else if (c.b > 32) {
-                if (gcount) emit(gfirst, gcount);
-                gcount = 0;
-                for (int32_t c0 = 0; c0 < c.b; c0 += 32) emit(c.a + c0, min(32, c.b - c0));
+    for (int pass = 0; pass < 2; ++pass) {
+        ng = 0;
+        auto emit = [&](int32_t first, int32_t count) {
+            if (pass && out + ng < group_cap) groups[out + ng] = make_int2(first, count);
+            ++ng;
+        };
+        if (live) {
+            const TNode<T, D> nd = tnode[id];
+            if (nd.b > 0) {
+                // Only a leaf root (one per cloud in a batch) forms groups of
+                // its own; other leaves are grouped by their parent.
+                if (parent[id] < 0)
+                    for (int32_t c0 = 0; c0 < nd.b; c0 += 32) emit(nd.a + c0, min(32, nd.b - c0));
             } else {
-                if (gcount + c.b > 32) {
-                    emit(gfirst, gcount);
-                    gcount = 0;
+                const int nc = __popc((unsigned)(-nd.b));
+                int32_t gfirst = 0, gcount = 0;
+                for (int j = 0; j < nc; ++j) {
+                    const TNode<T, D> c = tnode[nd.a + j];
+                    if (c.b <= 0) {  // internal child: close the open group
+                        if (gcount) emit(gfirst, gcount);
+                        gcount = 0;
+                    } else if (c.b > 32) {
+                        if (gcount) emit(gfirst, gcount);
+                        gcount = 0;
+                        for (int32_t c0 = 0; c0 < c.b; c0 += 32) emit(c.a + c0, min(32, c.b - c0));
+                    } else {
+                        if (gcount + c.b > 32) {
+                            emit(gfirst, gcount);
+                            gcount = 0;
+                        }
+                        if (gcount == 0) gfirst = c.a;
+                        gcount += c.b;
+                    }
                 }
-                if (gcount == 0) gfirst = c.a;
-                gcount += c.b;
+                if (gcount) emit(gfirst, gcount);
             }
         }
-        if (gcount) emit(gfirst, gcount);
+        if (pass == 0) {
+            int incl = ng;
+            const int lane = threadIdx.x & 31;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int tot = __shfl_sync(0xffffffffu, incl, 31);
+            unsigned long long base = 0;
+            if (lane == 31 && tot) base = atomicAdd((unsigned long long*)&hdr->n_groups, (unsigned long long)tot);
+            base = __shfl_sync(0xffffffffu, base, 31);
+            out = (int64_t)base + incl - ng;
+            if (tot == 0) return;  // warp-uniform
+        }
     }
-    if (!PASS) gcnt[id] = ng;
 }
 
 // --------------------------------------------------- 8. reference views --
@@ -1063,12 +1082,13 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         const int64_t cap = t.capacity;
         if ((err = ensure(t.tnode, (size_t)cap * sizeof(TNode<T, D>))) || (err = ensure(t.nrange, (size_t)cap * 8)) ||
             (err = ensure(t.parent, (size_t)cap * 4)) || (err = ensure(t.arrive, (size_t)cap * 4)) ||
-            (err = ensure(t.fchild, (size_t)cap * 4)) || (err = ensure(t.gcnt, (size_t)cap * 4)) ||
-            (err = ensure(t.goff, (size_t)(cap + 1) * 8)) ||
-            (err = ensure(t.scan_tmp, (size_t)std::max(scan_tmp_elems(nbc), scan_tmp_elems(cap)) * 8)) ||
+            (err = ensure(t.fchild, (size_t)cap * 4)) ||
+            (err = ensure(t.scan_tmp, (size_t)scan_tmp_elems(nbc) * 8)) ||
             (err = ensure(t.groups, (size_t)(cap + n / 32 + 2) * 8)) || (err = ensure(t.chain, 64 * 4)))
             return cuda_status(ctx, err, "allocating node arrays");
-        if ((err = cudaMemsetAsync(t.chain.p, 0xff, 64 * 4, s))) return cuda_status(ctx, err, "chain reset");
+        if ((err = cudaMemsetAsync(t.chain.p, 0xff, 64 * 4, s)) ||
+            (err = cudaMemsetAsync(&hdr->n_groups, 0, sizeof(int64_t), s)))
+            return cuda_status(ctx, err, "chain reset");
         if (bt.n_clouds && (err = cudaMemsetAsync(bt.croot, 0xff, (size_t)bt.n_clouds * 4, s)))
             return cuda_status(ctx, err, "cloud root reset");
         {
@@ -1094,17 +1114,11 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         }
         {
             PhaseTimer pt_(ctx, PH_GROUPS);
-            k_groups<T, D, 0><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
-                                                                        t.gcnt.as<int32_t>(), nullptr, nullptr,
-                                                                        t.chain.as<int32_t>(), t.parent.as<int32_t>(),
-                                                                        hdr);
-            ctx.kernel_launches += exclusive_scan_i32_i64(t.gcnt.as<int32_t>(), t.goff.as<int64_t>(), cap,
-                                                          &hdr->n_groups, t.scan_tmp.as<int64_t>(), s);
-            k_groups<T, D, 1><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
-                                                                        t.gcnt.as<int32_t>(), t.goff.as<int64_t>(),
-                                                                        t.groups.as<int2>(), t.chain.as<int32_t>(),
-                                                                        t.parent.as<int32_t>(), hdr);
-            ctx.kernel_launches += 2;
+            k_groups<T, D><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
+                                                                     t.groups.as<int2>(), cap + n / 32 + 2,
+                                                                     t.chain.as<int32_t>(), t.parent.as<int32_t>(),
+                                                                     hdr);
+            ctx.kernel_launches += 1;
             if (bt.n_clouds) {
                 k_cloud_start<T, D><<<div_up(bt.n_clouds, 128), 128, 0, s>>>(t.tnode.as<TNode<T, D>>(), bt, cap, hdr);
                 ctx.kernel_launches += 1;

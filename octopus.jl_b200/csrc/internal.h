@@ -86,8 +86,6 @@ struct Tree {
     DevBuf hdr;                  // OctHeader
     DevBuf morton;               // uint64 per original point (refit mode), filled with the views
     DevBuf groups;               // int2 {first position, count <= 32}: query groups
-    DevBuf gcnt;                 // int32 per node: groups formed under it
-    DevBuf goff;                 // int64 exclusive scan of gcnt (+1)
     int64_t n_groups = 0;
     int32_t dfs_start = 0;
     DevBuf chain;                // int32[64]: full-range chain node ids and flags

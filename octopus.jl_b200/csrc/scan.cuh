@@ -46,7 +46,7 @@ int exclusive_scan_i32_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* 
 // In-place capable int32 scan; `out` holds n + 1 elements.
 int exclusive_scan_i32_i32(const int32_t* in, int32_t* out, int64_t n, int64_t* tile_tmp, cudaStream_t s);
 constexpr int kSmallScanThreads = 1024;
-constexpr int64_t kSmallScan = 16 * kSmallScanThreads;  // one block scans up to this many
+constexpr int64_t kSmallScan = 32 * kSmallScanThreads;  // one block scans up to this many
 inline int64_t scan_tmp_elems(int64_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
 
 }  // namespace oct

@@ -148,3 +148,44 @@ def test_refit_mode_off_always_sorts(ob, oracle_mod):
     st.step(x)
     assert st.step(x) == (0, -1)
     st.check(oracle_mod, x)
+
+
+def test_speculative_merge_fallbacks(ob, oracle_mod):
+    """After a merging step the next build merges before it has read the
+    bounds; when the merge does not apply (too many changed keys, a key past
+    the key width, a non-finite coordinate) the build is redone on the usual
+    path, with the same result as a full rebuild."""
+    x = uniform(20_000, 3, 80)
+    r = np.float32(0.05)
+    rng = np.random.default_rng(81)
+    st = Stepper(ob, x, r)
+    st.step(x)
+
+    def relocate(z, k):
+        z = z.copy()
+        pick = rng.choice(len(z), k, replace=False)
+        z[pick] = rng.random((k, 3)).astype(np.float32) * np.float32(0.99) + np.float32(0.005)
+        return z
+
+    y = relocate(x, 40)
+    assert st.step(y)[0] == 1  # merged
+    st.check(oracle_mod, y)
+    z = relocate(y, 8000)  # beyond the merge capacity (2,500 here)
+    path, moved = st.step(z)
+    assert path == 0 and moved > 2500
+    st.check(oracle_mod, z)
+    w = relocate(z, 40)
+    assert st.step(w)[0] == 1
+    v = w.copy()
+    v[123] = np.float32(900.0)  # 18,000 cells per axis: the key no longer fits 32 bits
+    path, _ = st.step(v)
+    assert path == 0
+    st.check(oracle_mod, v)
+    u = relocate(v, 30)
+    assert st.step(u)[0] == 1
+    bad = u.copy()
+    bad[7, 1] = np.float32(np.nan)
+    with pytest.raises(ob.InexactError):
+        st.step(bad)
+    assert st.step(u)[0] == 0  # rebuilt in full after the error
+    st.check(oracle_mod, u)
