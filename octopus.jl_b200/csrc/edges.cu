@@ -48,8 +48,8 @@ enum EdgePass {
 // 32-point part, for a larger leaf) and the bit mask of its points within the
 // radius of one query.  A query's records, in order, list its neighbors in
 // the reference's order.
-constexpr int kMaxRecords = 240;  // per query: the record count is stored in one byte
-constexpr uint8_t kOverflowMark = 255;  // record count of the queries of an overflowed group
+constexpr int kMaxRecords = 65000;  // per query: the record count is stored in 16 bits
+constexpr uint16_t kOverflowMark = 0xffff;  // record count of the queries of an overflowed group
 
 // Edge k of the COO: sender = target point t, receiver = query qi at px
 // (src/cpu/edges_cpu.jl:200-215: rel_displacement = (x_q - x_t) * inv(r),
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     const SPt<T, D>* __restrict__ tpts, int64_t n_tnodes, T r2, T inv_r, int exclude_self,
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ ocount,
-    int2* __restrict__ recs, int64_t rec_cap, uint8_t* __restrict__ rcount, uint8_t* __restrict__ gflag, Batch bt) {
+    int2* __restrict__ recs, int64_t rec_cap, uint16_t* __restrict__ rcount, uint8_t* __restrict__ gflag, Batch bt) {
     constexpr bool STAGE = PASS == EP_FILL;
     // The usual DFS bound, plus the room the multi-node expansions may take.
     constexpr int SD = stack_depth<D>() + kMultiLimit + 8;
@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     if (PASS != EP_FILL && valid) counts[q.idx] = (int32_t)cnt;
     if (PASS == EP_RECORD) {
         const bool over = __any_sync(0xffffffffu, nrec > cap);
-        if (valid) rcount[qpos] = over ? kOverflowMark : (uint8_t)nrec;
+        if (valid) rcount[qpos] = over ? kOverflowMark : (uint16_t)nrec;
         int mx = nrec;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -406,7 +406,7 @@ template <class T, int D>
 __global__ void __launch_bounds__(kExpandWarps * 32, 8) k_expand(
     int64_t nq, const int32_t* __restrict__ iperm, const SPt<T, D>* __restrict__ qpts,
     const SPt<T, D>* __restrict__ tpts, const int64_t* __restrict__ offsets, const int2* __restrict__ recs,
-    int64_t rec_cap, const uint8_t* __restrict__ rcount, T inv_r, int32_t* __restrict__ senders,
+    int64_t rec_cap, const uint16_t* __restrict__ rcount, T inv_r, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, Batch bt) {
     __shared__ ExpandSmem<T, D> sm_all[kExpandWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -607,12 +607,15 @@ __global__ void k_neighbors_of(const T* __restrict__ qcoords, int64_t nsel, cons
 namespace {
 
 // Hit records per query for the next count: 32 to start, then 1.25x the
-// largest record count of the last count (at most kMaxRecords), within
-// kRecordBudget bytes in all.
+// largest record count of the last count (at most kMaxRecords), within a
+// budget of 4 GiB or 8 bytes per edge of the last count (a third of the
+// COO's own size), whichever is larger, and at most 32 GiB.
 constexpr int64_t kRecordBudget = 4LL << 30;
+constexpr int64_t kRecordBudgetMax = 32LL << 30;
 
 int64_t record_cap(const Ctx& ctx, int64_t nq) {
-    const int64_t fit = kRecordBudget / (8 * std::max<int64_t>(nq, 1));
+    const int64_t budget = std::min(std::max(kRecordBudget, 8 * ctx.rec_edges_hint), kRecordBudgetMax);
+    const int64_t fit = budget / (8 * std::max<int64_t>(nq, 1));
     return std::min<int64_t>(ctx.rec_cap_hint, fit);
 }
 
@@ -641,7 +644,7 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
         // need not walk the tree again.
         const int64_t cap = record_cap(ctx, nq);
         if (cap >= 8) {
-            if ((err = ensure(ctx.recs, (size_t)nq * cap * 8)) || (err = ensure(ctx.rcount, (size_t)nq)) ||
+            if ((err = ensure(ctx.recs, (size_t)nq * cap * 8)) || (err = ensure(ctx.rcount, (size_t)nq * 2)) ||
                 (err = ensure(ctx.gflag, (size_t)std::max<int64_t>(q.n_groups, 1))))
                 return cuda_status(ctx, err, "allocating hit records");
             ctx.rec_cap = cap;
@@ -653,7 +656,7 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
                 nullptr, nullptr, nullptr, nullptr, (int*)(ctx.total.as<int64_t>() + 1), ctx.recs.as<int2>(),
-                ctx.rec_cap, ctx.rcount.as<uint8_t>(), ctx.gflag.as<uint8_t>(), t.batch());
+                ctx.rec_cap, ctx.rcount.as<uint16_t>(), ctx.gflag.as<uint8_t>(), t.batch());
         else
             k_edges<T, D, EP_COUNT><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
@@ -677,6 +680,7 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
         ctx.rec_overflow = w[0];
         const int64_t need = ((int64_t)w[1] * 5 / 4 + 7) / 8 * 8;
         ctx.rec_cap_hint = std::min<int64_t>(std::max<int64_t>(need, 16), kMaxRecords);
+        ctx.rec_edges_hint = *n_edges;
     }
     return OK;
 }
@@ -693,7 +697,7 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
     if (ctx.rec_cap) {
         k_expand<T, D><<<div_up(q.n, 32 * kExpandWarps), kExpandWarps * 32, 0, s>>>(
             q.n, q.iperm.as<int32_t>(), q.spts.as<SPt<T, D>>(), t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
-            ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint8_t>(), inv_r, senders, receivers, (T*)rel_disp,
+            ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint16_t>(), inv_r, senders, receivers, (T*)rel_disp,
             (T*)rel_dist, t.batch());
         ctx.kernel_launches += 1;
     }

@@ -152,6 +152,7 @@ struct Ctx {
     DevBuf recs, rcount, gflag;
     int64_t rec_cap = 0;
     int64_t rec_cap_hint = 32;
+    int64_t rec_edges_hint = 0;    // edge total of the last recording count
     int64_t rec_overflow = 0;
     // Adjoint scratch (diff.cu).
     DevBuf dkeys[2], dvals[2], dhist, dsort_tmp, droff, dsoff;
