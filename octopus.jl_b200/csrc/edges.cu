@@ -219,6 +219,10 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 const int mp = (total + 3) & ~3;  // padded to whole pairs of pairs with +inf points
                 ++chunk;
                 __syncwarp();
+                // A target farther than r from the group's box can be no
+                // query's neighbor (box_gap2 never exceeds a point distance):
+                // the pair loop skips the steps whose targets all are.
+                bool near = false;
                 if (lane < total) {
                     int k = 0;
                     while (sseg[w][k + 1].y <= lane) ++k;
@@ -226,6 +230,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                     const SPt<T, D> t = tpts[pos];
 #pragma unroll
                     for (int d = 0; d < D; ++d) sx[w][d][lane] = t.x[d];
+                    near = box_gap2<T, D>(qlo, qhi, t.x, t.x) <= r2;
                     if (self_pair) {  // query and target are the same tree: the group's own points
                         const int64_t sl = pos - grp.x;
                         if (sl >= 0 && sl < grp.y) sself[w][sl] = (chunk << 5) | lane;
@@ -234,13 +239,17 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
 #pragma unroll
                     for (int d = 0; d < D; ++d) sx[w][d][lane] = T(INFINITY);
                 }
+                const unsigned keep = __ballot_sync(0xffffffffu, near);
                 __syncwarp();
                 unsigned hm = 0;
                 if constexpr (std::is_same<T, float>::value) {
                     unsigned long long P[D];
 #pragma unroll
                     for (int d = 0; d < D; ++d) P[d] = pack2(q.x[d], q.x[d]);
-                    for (int j = 0; j < mp; j += 4) {
+                    // one bit per step of four targets with a target kept
+                    const unsigned steps = (keep | keep >> 1 | keep >> 2 | keep >> 3) & 0x11111111u;
+                    for (unsigned km = steps; km; km &= km - 1) {
+                        const int j = __ffs(km) - 1;
                         // Four targets per step, two per packed operation:
                         // packed differences and squares, scalar sums
                         // ((dx*dx + dy*dy) + dz*dz) per element.
@@ -261,7 +270,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                                (s3 <= r2 ? 8u : 0u)) << j;
                     }
                 } else {
-                    for (int j = 0; j < total; ++j) {
+                    for (unsigned km = keep; km; km &= km - 1) {
+                        const int j = __ffs(km) - 1;
                         T t[D], diff[D];
 #pragma unroll
                         for (int d = 0; d < D; ++d) t[d] = sx[w][d][j];

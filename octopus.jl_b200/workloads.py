@@ -13,6 +13,8 @@ Workloads (float32):
   mix2d        2D, 4,000,000 points: 64 Gaussians (sigma U[0.005, 0.05],
                Dirichlet(1) weights) + 10% uniform, in [0,1)^2, r = 0.002
   diff2m       3D, 2,000,000 points U[0,1)^3, r = 0.012
+  batch512     3D, 512 clouds, sizes log-uniform in [500, 20000], each U[0,1)^3,
+               radius U[0.03, 0.08] per cloud, one batched build + COO
 """
 from __future__ import annotations
 
@@ -81,6 +83,8 @@ def _run(name: str, steps: int, scale: float):
     elif name == "diff2m":
         xs = [uniform(int(2_000_000 * scale), 3, 2025)] * steps
         r = 0.012
+    elif name == "batch512":
+        return _run_batch(ob, torch, steps)
     else:
         raise SystemExit(f"unknown workload {name}")
     if name == "diff2m":
@@ -98,6 +102,25 @@ def _run(name: str, steps: int, scale: float):
         e = ob.build_edges(tns, sid, sid)
         ob.synchronize(tns)
         print(f"{name}: n={x.shape[1]} edges={e.senders.numel()}")
+
+
+def batch_clouds(n_clouds: int = 512, seed: int = 4):
+    """Sizes log-uniform in [500, 20000], points U[0,1)^3, radii U[0.03, 0.08]."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(500), np.log(20000), n_clouds)).astype(np.int64)
+    radii = rng.uniform(0.03, 0.08, n_clouds)
+    clouds = [rng.random((int(n), 3)).astype(np.float32) for n in sizes]
+    return clouds, sizes, radii
+
+
+def _run_batch(ob, torch, steps):
+    clouds, sizes, radii = batch_clouds()
+    cat = torch.from_numpy(np.concatenate(clouds)).cuda().t()
+    bs = ob.BatchedSearch(torch.float32, 3)
+    for _ in range(steps):
+        e = bs.run_(cat, sizes, radii).build_edges()
+        torch.cuda.synchronize()
+        print(f"batch512: n={int(sizes.sum())} edges={e.senders.numel()}")
 
 
 def _run_diff(ob, torch, xs, r):
