@@ -224,6 +224,23 @@ OCT_API int oct_edges_diff_backward_recompute(oct_ctx* ctx, int ndims, int dtype
                                               const void* d_rel_displacement, const void* d_rel_dist_norm,
                                               double radius, void* grad_coords);
 
+/* The self-pair pullback with a processing order: `order` (n_points entries,
+ * 1-based, a permutation such as the tree's perm from oct_tree_arrays) sets
+ * which points a warp handles together.  A spatial order keeps the mirror
+ * edges that each warp reads in the on-chip cache; the gradient is the same
+ * for every permutation (and NULL means 1..n).  Features are read from
+ * rel_displacement / rel_dist_norm, or recomputed from `coords` when it is
+ * non-NULL (then the features may be NULL).  Entries of `order` outside
+ * 1..n_points, and edge indices outside 1..n_points, return
+ * OCT_ERR_ARGUMENT.  Same adjoint as oct_edges_diff_backward
+ * (ext/OctopusChainRulesCoreExt.jl:137-192). */
+OCT_API int oct_edges_diff_backward_ordered(oct_ctx* ctx, int ndims, int dtype, int64_t n_points,
+                                            int64_t n_edges, const int32_t* senders,
+                                            const int32_t* receivers, const void* rel_displacement,
+                                            const void* rel_dist_norm, const void* coords,
+                                            const void* d_rel_displacement, const void* d_rel_dist_norm,
+                                            double radius, void* grad_coords, const int32_t* order);
+
 /* Edge count that allocates no device memory.  No counterpart in the
  * reference: it serves callers that cannot let a library call cudaMalloc --
  * hosts whose device memory belongs to their own pool allocator (a

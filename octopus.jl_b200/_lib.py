@@ -67,6 +67,7 @@ SIGNATURES = [
     ("oct_edges_diff_backward", I, [P, I, I, I64, I64, P, P, P, P, P, P, D, P]),
     ("oct_edges_diff_backward_pair", I, [P, I, I, I64, I64, I64, P, P, P, P, P, P, D, P, P]),
     ("oct_edges_diff_backward_recompute", I, [P, I, I, I64, I64, P, P, P, P, P, D, P]),
+    ("oct_edges_diff_backward_ordered", I, [P, I, I, I64, I64, P, P, P, P, P, P, P, D, P, P]),
     ("oct_edges_count_noalloc", I, [P, P, P, I, P, P, C.POINTER(I64)]),
     ("oct_profile_enable", I, [P, I]),
     ("oct_profile_phase_name", C.c_char_p, [I]),

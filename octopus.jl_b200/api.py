@@ -569,12 +569,24 @@ class _EdgesDiff(torch.autograd.Function):
         ctx.radius = float(radius)
         ctx.coords_shape = coords.shape
         ctx.recompute = bool(recompute)
+        # The tree's Morton permutation (1-based, gathered from 1..n by the
+        # tree's order): the backward pass visits the points in this order,
+        # which keeps the mirror edges it reads in L2.
+        n_pts = coords.shape[1]
+        order = torch.arange(1, n_pts + 1, dtype=torch.int32, device=snd.device)
+        if n_pts > 0:
+            lc = tns._ctx
+            lc.bind_stream()
+            tree = tns.trees[set_id - 1]
+            order_in, order = order, torch.empty_like(order)
+            lc.check(lc.lib.oct_zsort_apply(lc.handle, tree.handle, _ptr(order_in), _ptr(order), n_pts, 4, 0),
+                     "build_edges_diff order")
         if ctx.recompute:
             # Keep only the indices and the coordinates: the backward pass
             # recomputes the features (memory-lean mode).
-            ctx.save_for_backward(snd, rcv, colmajor(coords.detach()))
+            ctx.save_for_backward(snd, rcv, colmajor(coords.detach()), order)
         else:
-            ctx.save_for_backward(snd, rcv, disp, dist)
+            ctx.save_for_backward(snd, rcv, disp, dist, order)
         ctx.mark_non_differentiable(snd, rcv)
         return snd, rcv, disp, dist
 
@@ -590,15 +602,15 @@ class _EdgesDiff(torch.autograd.Function):
         lc = tns._ctx
         lc.bind_stream()
         if ctx.recompute:
-            snd, rcv, xc = ctx.saved_tensors
-            lc.check(lc.lib.oct_edges_diff_backward_recompute(
-                lc.handle, d, _dtype_code(T), n, snd.numel(), _ptr(snd), _ptr(rcv), _ptr(xc), _ptr(dd), _ptr(dn),
-                ctx.radius, _ptr(grad)), "build_edges_diff pullback")
+            snd, rcv, xc, order = ctx.saved_tensors
+            disp_p, dist_p, xc_p = None, None, _ptr(xc)
         else:
-            snd, rcv, disp, dist = ctx.saved_tensors
-            lc.check(lc.lib.oct_edges_diff_backward(
-                lc.handle, d, _dtype_code(T), n, snd.numel(), _ptr(snd), _ptr(rcv), _ptr(disp.t()), _ptr(dist),
-                _ptr(dd), _ptr(dn), ctx.radius, _ptr(grad)), "build_edges_diff pullback")
+            snd, rcv, disp, dist, order = ctx.saved_tensors
+            disp_p, dist_p, xc_p = _ptr(disp.t()), _ptr(dist), None
+        lc.check(lc.lib.oct_edges_diff_backward_ordered(
+            lc.handle, d, _dtype_code(T), n, snd.numel(), _ptr(snd), _ptr(rcv), disp_p, dist_p, xc_p, _ptr(dd),
+            _ptr(dn), ctx.radius, _ptr(grad), _ptr(order) if order.numel() == n else None),
+            "build_edges_diff pullback")
         return grad.t(), None, None, None, None
 
 

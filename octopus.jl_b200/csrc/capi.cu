@@ -145,7 +145,7 @@ OCT_API int oct_ctx_destroy(oct_ctx* ctx) {
     using oct::release;
     for (auto* b : {&ctx->c.counts, &ctx->c.offsets, &ctx->c.scan_tmp, &ctx->c.total, &ctx->c.dkeys[0],
                     &ctx->c.dkeys[1], &ctx->c.dvals[0], &ctx->c.dvals[1], &ctx->c.dhist, &ctx->c.dsort_tmp, &ctx->c.droff,
-                    &ctx->c.dsoff, &ctx->c.dstatus, &ctx->c.dnet, &ctx->c.recs, &ctx->c.rcount, &ctx->c.gflag})
+                    &ctx->c.dsoff, &ctx->c.dstatus, &ctx->c.dredge, &ctx->c.dterm, &ctx->c.dseg, &ctx->c.recs, &ctx->c.rcount, &ctx->c.gflag})
         release(*b);
     if (ctx->c.total_host) cudaFreeHost(ctx->c.total_host);
     for (auto& r : ctx->c.prof) {
@@ -368,7 +368,8 @@ OCT_API int oct_edges_diff_backward(oct_ctx* ctx, int ndims, int dtype, int64_t 
         return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge array is NULL");
     DeviceGuard g(ctx->c.device);
     return oct::diff_backward(ctx->c, ndims, dtype, n_points, n_edges, senders, receivers, rel_displacement,
-                              rel_dist_norm, d_rel_displacement, d_rel_dist_norm, radius, grad_coords, nullptr);
+                              rel_dist_norm, d_rel_displacement, d_rel_dist_norm, radius, grad_coords, nullptr,
+                              nullptr);
 }
 
 OCT_API int oct_edges_diff_backward_pair(oct_ctx* ctx, int ndims, int dtype, int64_t n_query, int64_t n_target,
@@ -409,7 +410,30 @@ OCT_API int oct_edges_diff_backward_recompute(oct_ctx* ctx, int ndims, int dtype
         return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge array is NULL");
     DeviceGuard g(ctx->c.device);
     return oct::diff_backward(ctx->c, ndims, dtype, n_points, n_edges, senders, receivers, nullptr, nullptr,
-                              d_rel_displacement, d_rel_dist_norm, radius, grad_coords, coords);
+                              d_rel_displacement, d_rel_dist_norm, radius, grad_coords, coords, nullptr);
+}
+
+OCT_API int oct_edges_diff_backward_ordered(oct_ctx* ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,
+                                            const int32_t* senders, const int32_t* receivers,
+                                            const void* rel_displacement, const void* rel_dist_norm,
+                                            const void* coords, const void* d_rel_displacement,
+                                            const void* d_rel_dist_norm, double radius, void* grad_coords,
+                                            const int32_t* order) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (bad_dims(ndims) || bad_dtype(dtype)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "bad ndims/dtype");
+    if (n_points < 0 || n_edges < 0 || n_edges > 2147483647LL || n_points > 2147483647LL)
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "sizes must fit Int32");
+    if (!(radius > 0.0)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "radius must be positive");
+    if (n_points > 0 && !grad_coords) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "grad_coords is NULL");
+    if (n_edges > 0 && (!senders || !receivers))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge array is NULL");
+    if (n_points > 0 && !coords && n_edges > 0 && (!rel_displacement || !rel_dist_norm))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "give either the features or coords");
+    DeviceGuard g(ctx->c.device);
+    return oct::diff_backward(ctx->c, ndims, dtype, n_points, n_edges, senders, receivers,
+                              coords ? nullptr : rel_displacement, coords ? nullptr : rel_dist_norm,
+                              d_rel_displacement, d_rel_dist_norm, radius, grad_coords, coords, order);
 }
 
 static const char* kPhaseNames[oct::PH_NUM] = {"bounds", "encode", "sort", "gather", "topology",

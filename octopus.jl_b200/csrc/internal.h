@@ -156,7 +156,9 @@ struct Ctx {
     int64_t rec_overflow = 0;
     // Adjoint scratch (diff.cu).
     DevBuf dkeys[2], dvals[2], dhist, dsort_tmp, droff, dsoff;
-    DevBuf dnet;         // double per edge and axis: net adjoint contribution
+    DevBuf dredge;       // edges ordered by receiver (adjoint of a COO not grouped by receiver)
+    DevBuf dterm;        // per-edge cotangent term of the self-pair adjoint (4 values)
+    DevBuf dseg;         // per-point {first, end} edge of the self-pair adjoint
     // Profiler.
     int64_t kernel_launches = 0;  // every kernel this context has launched
     bool profiling = false;
@@ -202,7 +204,7 @@ int zsort_apply(Ctx& ctx, const Tree& t, const void* in, void* out, int64_t n, i
 int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,
                   const int32_t* senders, const int32_t* receivers, const void* rel_disp,
                   const void* rel_dist, const void* d_disp, const void* d_dist, double radius,
-                  void* grad, const void* coords);
+                  void* grad, const void* coords, const int32_t* order);
 int diff_backward_pair(Ctx& ctx, int ndims, int dtype, int64_t nq, int64_t nt, int64_t m, const int32_t* snd,
                        const int32_t* rcv, const void* rel_disp, const void* rel_dist, const void* d_disp,
                        const void* d_dist, double radius, void* grad_q, void* grad_t);

@@ -82,7 +82,7 @@ def _run(name: str, steps: int, scale: float):
         r = 0.002
     elif name == "diff2m":
         xs = [uniform(int(2_000_000 * scale), 3, 2025)] * steps
-        r = 0.012
+        r = 0.012 / scale ** (1 / 3)  # same neighbors per point at every scale
     elif name == "batch512":
         return _run_batch(ob, torch, steps)
     else:

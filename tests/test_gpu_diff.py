@@ -212,3 +212,138 @@ def test_cross_pair_adjoint_fp64_central_differences(ob):
                 return f(xx, b) if which == 0 else f(a, xx)
             fd = (-fk(2 * eps) + 8 * fk(eps) - 8 * fk(-eps) + fk(-2 * eps)) / (12 * eps)
             assert abs(g.flat[k] - fd) <= 1e-5 * max(1.0, abs(fd))
+
+
+def _backward_raw(ob, tns, n, snd, rcv, rd, rn, gd, gn, r, dtype, order=None, coords=None):
+    """The C-ABI pullback on raw device arrays; returns (status, grad)."""
+    import ctypes as C
+    lc = tns._ctx
+    lc.bind_stream()
+    T = torch.float32 if dtype == np.float32 else torch.float64
+    grad = torch.full((n, 3), float("nan"), dtype=T, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+    if order is None and coords is None:
+        st = lc.lib.oct_edges_diff_backward(lc.handle, 3, 0 if dtype == np.float32 else 1, n, snd.numel(), p(snd),
+                                            p(rcv), p(rd), p(rn), p(gd), p(gn), float(r), p(grad))
+    else:
+        st = lc.lib.oct_edges_diff_backward_ordered(lc.handle, 3, 0 if dtype == np.float32 else 1, n, snd.numel(),
+                                                    p(snd), p(rcv), p(rd), p(rn), p(coords), p(gd), p(gn), float(r),
+                                                    p(grad), p(order))
+    return st, grad
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_adjoint_order_changes_nothing(ob, dtype):
+    """The processing order (tree perm, a random permutation, none) picks
+    which warp handles a point, never a point's sum: bit-identical grads."""
+    x = uniform(6000, 3, 8301, dtype=dtype)
+    r = dtype(0.07)
+    tns, sid, c = setup(ob, x, r)
+    e = ob.build_edges(tns, sid, sid)
+    snd, rcv = e.senders.clone(), e.receivers.clone()
+    rd = e.rel_displacement.t().contiguous()
+    rn = e.rel_dist_norm.reshape(-1).contiguous()
+    gd, gn = torch.sin(rd * 7), torch.cos(rn * 3)
+    n = x.shape[0]
+    perm = tns.trees[sid - 1].arrays()["perm"].clone()
+    rnd = (torch.randperm(n, generator=torch.Generator().manual_seed(3)) + 1).to(torch.int32).cuda()
+    out = []
+    for order in (None, perm, rnd):
+        st, g = _backward_raw(ob, tns, n, snd, rcv, rd, rn, gd, gn, r, dtype, order=order,
+                              coords=None)
+        assert st == 0
+        out.append(g)
+    xc = torch.from_numpy(x).cuda().contiguous()
+    st, g_re = _backward_raw(ob, tns, n, snd, rcv, None, None, gd, gn, r, dtype, order=perm, coords=xc)
+    assert st == 0
+    for g in out[1:] + [g_re]:
+        assert torch.equal(g, out[0])
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_adjoint_of_ungrouped_coo(ob, oracle_mod, dtype):
+    """Edges in any order (not grouped by receiver) go through the sorted
+    path with a receiver sort and still match the reference rrule."""
+    x = uniform(4000, 3, 8302, dtype=dtype)
+    r = dtype(0.06)
+    tns, sid, _ = setup(ob, x, r)
+    e = ob.build_edges(tns, sid, sid)
+    m = e.senders.numel()
+    sh = torch.randperm(m, generator=torch.Generator().manual_seed(5)).cuda()
+    snd, rcv = e.senders[sh].contiguous(), e.receivers[sh].contiguous()
+    rd = e.rel_displacement.t()[sh].contiguous()
+    rn = e.rel_dist_norm.reshape(-1)[sh].contiguous()
+    gd, gn = 2 * rd, rn.clone()
+    st, g = _backward_raw(ob, tns, x.shape[0], snd, rcv, rd, rn, gd, gn, r, dtype)
+    assert st == 0
+    go = oracle_mod.diff_backward(x.shape[0], snd.cpu().numpy(), rcv.cpu().numpy(), rd.cpu().numpy(),
+                                  rn.cpu().numpy(), gd.cpu().numpy(), gn.cpu().numpy(), r)
+    tol = 1e-12 if dtype == np.float64 else 2e-5
+    assert np.abs(g.cpu().numpy() - go).max() <= tol * np.abs(go).max()
+    # recomputing the features needs the grouped self-pair COO
+    xc = torch.from_numpy(x).cuda().contiguous()
+    st, _ = _backward_raw(ob, tns, x.shape[0], snd, rcv, None, None, gd, gn, r, dtype, coords=xc)
+    assert st != 0
+
+
+def test_adjoint_rejects_out_of_range_indices(ob):
+    """A sender, receiver or order entry outside 1..n is an argument error
+    (the kernels check every index before using it)."""
+    x = uniform(2000, 3, 8303)
+    r = np.float32(0.08)
+    tns, sid, _ = setup(ob, x, r)
+    e = ob.build_edges(tns, sid, sid)
+    n = x.shape[0]
+    rd = e.rel_displacement.t().contiguous()
+    rn = e.rel_dist_norm.reshape(-1).contiguous()
+    gd, gn = 2 * rd, rn.clone()
+    for field, val in (("snd", n + 1), ("snd", 0), ("rcv", n + 5)):
+        snd, rcv = e.senders.clone(), e.receivers.clone()
+        (snd if field == "snd" else rcv)[len(snd) // 2] = val
+        st, _ = _backward_raw(ob, tns, n, snd, rcv, rd, rn, gd, gn, r, np.float32)
+        assert st != 0
+        st, _ = _backward_raw(ob, tns, n, snd, rcv, rd, rn, gd, gn, r, np.float32,
+                              order=torch.arange(1, n + 1, dtype=torch.int32, device="cuda"))
+        assert st != 0
+    bad_order = torch.arange(1, n + 1, dtype=torch.int32, device="cuda")
+    bad_order[7] = n + 3
+    st, _ = _backward_raw(ob, tns, n, e.senders, e.receivers, rd, rn, gd, gn, r, np.float32, order=bad_order)
+    assert st != 0
+    # the context stays usable after the errors
+    st, g = _backward_raw(ob, tns, n, e.senders, e.receivers, rd, rn, gd, gn, r, np.float32)
+    assert st == 0 and torch.isfinite(g).all()
+
+
+def test_cross_pair_adjoint_ungrouped(ob):
+    """Cross-pair adjoint of a shuffled COO equals that of the grouped one
+    up to the order of the float64 sums."""
+    import ctypes as C
+    a = uniform(2500, 3, 8304)
+    b = uniform(3000, 3, 8305)
+    r = np.float32(0.09)
+    tns = ob.TNS(torch.float32, ndims=3)
+    ob.set_search_radius_(tns, r)
+    ia = ob.add_point_set_(tns, torch.from_numpy(a).cuda().t())
+    ib = ob.add_point_set_(tns, torch.from_numpy(b).cuda().t())
+    ob.set_active_search_(tns, ia, ib)
+    ob.run_(tns)
+    e = ob.build_edges(tns, ia, ib)
+    m = e.senders.numel()
+    sh = torch.randperm(m, generator=torch.Generator().manual_seed(9)).cuda()
+    rd = e.rel_displacement.t().contiguous()
+    rn = e.rel_dist_norm.reshape(-1).contiguous()
+    lc = tns._ctx
+    lc.bind_stream()
+    p = lambda t: C.c_void_p(t.data_ptr())
+    res = []
+    for idx in (torch.arange(m, device="cuda"), sh):
+        snd, rcv = e.senders[idx].contiguous(), e.receivers[idx].contiguous()
+        rdi, rni = rd[idx].contiguous(), rn[idx].contiguous()
+        gq = torch.empty((len(a), 3), device="cuda")
+        gt = torch.empty((len(b), 3), device="cuda")
+        gd, gn = 2 * rdi, rni.clone()  # held for the call
+        assert lc.lib.oct_edges_diff_backward_pair(lc.handle, 3, 0, len(a), len(b), m, p(snd), p(rcv), p(rdi),
+                                                   p(rni), p(gd), p(gn), float(r), p(gq), p(gt)) == 0
+        res.append((gq, gt))
+    for u, v in zip(res[0], res[1]):
+        assert torch.allclose(u, v, rtol=1e-5, atol=1e-6 * float(u.abs().max()))
