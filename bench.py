@@ -182,6 +182,14 @@ def barrier(world):
         dist.barrier()
 
 
+def replica_totals(ms: float, edges: float, world: int, device=None):
+    """Whole-job figures of N independent replicas: the slowest rank's time,
+    the edges of all ranks, and their throughput (edges/s) over that time."""
+    ms_max = max_over_ranks(ms, world, device)
+    tot = sum_over_ranks(float(edges), world, device)
+    return ms_max, tot, tot / (ms_max / 1e3)
+
+
 # ------------------------------------------------------------ our arm -----
 def run_ours(args, rank, world, local):
     import torch
@@ -282,11 +290,8 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     e2e_ms = t0.elapsed_time(t1)
 
-    ms_max = max_over_ranks(ms, world, dev)
-    e2e_ms_max = max_over_ranks(e2e_ms, world, dev)
-    tot_edges = sum_over_ranks(float(edges), world, dev)
-    tot_e2e = sum_over_ranks(float(e2e_edges), world, dev)
-    value = tot_edges / (ms_max / 1e3)
+    ms_max, tot_edges, value = replica_totals(ms, edges, world, dev)
+    e2e_ms_max, tot_e2e, _ = replica_totals(e2e_ms, e2e_edges, world, dev)
 
     # --- roofline of the dominant HBM kernel (edge write = fill), live timing
     from_peaks = None
