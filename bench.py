@@ -46,21 +46,32 @@ WORKLOAD = "sph_lattice_timestep_1M"
 FILL_DRAM_BYTES_PER_EDGE = 23.8
 
 
-def phase_bytes(n, e, n_nodes, path):
+def phase_bytes(n, e, n_nodes, path, passes=3):
     """Algorithmic HBM bytes per step of the HBM-bound build phases and of
     the edge write, for float32 3D and the kernels that run in `path`
-    (0 full sort: k_encode + 3 radix passes + k_gather; 1 refit-mode merge:
-    k_resort_mark + k_resort_merge, which also gathers)."""
+    (0 full sort: k_encode + `passes` radix passes + k_gather; 1 refit-mode
+    merge: k_resort_mark + k_resort_merge, which also gathers)."""
     b = {"bounds": 12 * n}                          # coordinates read once
     if path == 1:
         b["encode"] = (4 + 12 + 4 + 1) * n            # perm, gathered coords, old key in; changed flag out
         b["sort"] = (4 + 4 + 1 + 12 + 4 + 4 + 16 + 4) * n  # key, perm, flag, coords in; key, perm, point, inverse out
     else:
         b["encode"] = (12 + 4) * n                    # coords in; key out
-        b["sort"] = 3 * (4 + 4 + 4 + 4 + 4) * n + (4 + 12 + 16 + 4) * n  # 3 passes + gather
+        b["sort"] = passes * (4 + 4 + 4 + 4 + 4) * n  # per pass: keys for the histogram; keys, values in and out
+        b["gather"] = (4 + 12 + 16 + 4) * n           # perm, gathered coords in; sorted point, inverse out
     b["refit"] = 16 * n + 2 * 32 * n_nodes          # sorted points in; node records read and written
-    b["fill"] = (12 + 4 * 3) * e + 8 * n            # (12 + 4D) E + 8N
+    if e:
+        b["fill"] = (12 + 4 * 3) * e + 8 * n        # (12 + 4D) E + 8N
     return b
+
+
+def _peak_gbs():
+    """Measured HBM copy bandwidth (GB/s) of MEASURED_PEAKS.json, else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0
 
 
 def config_dict(extra=None):
@@ -399,6 +410,49 @@ def secondary_configs(ob, torch, dev):
 
     plain("uniform_100k_r0.04", wl.uniform(100_000, 3, 2024), 0.04, 10)
     plain("nonuniform2d_4M_r0.002_seed2026", wl.gaussian_mixture_2d(4_000_000, 64, 2026), 0.002, 2)
+
+    # --- the build alone (run!) at 16M uniform points, where its kernels move
+    # enough bytes to be bandwidth-bound rather than launch-bound
+    def build_only(name, x, r, reps):
+        lib = ob._lib.load()
+        tns = ob.TNS(torch.float32, ndims=3)
+        ob.set_search_radius_(tns, r)
+        xd = torch.from_numpy(x).to(dev).t()
+        sid = ob.add_point_set_(tns, xd)
+        ob.set_active_search_(tns, sid, sid)
+
+        def step():
+            ob.update_point_set_(tns, sid, xd)
+            ob.run_(tns)
+            return 0
+
+        step()
+        step()
+        ms, _ = _timed(torch, stream, step, reps)
+        nph = len(ob._lib.PHASES)
+        ms_buf = (C.c_double * nph)()
+        cnt_buf = (C.c_int64 * nph)()
+        ctx = tns._ctx
+        lib.oct_profile_read(ctx.handle, ms_buf, cnt_buf, nph)
+        lib.oct_profile_enable(ctx.handle, 1)
+        for _ in range(reps):
+            step()
+        torch.cuda.synchronize()
+        lib.oct_profile_read(ctx.handle, ms_buf, cnt_buf, nph)
+        lib.oct_profile_enable(ctx.handle, 0)
+        phases = {ob._lib.PHASES[i]: ms_buf[i] / reps for i in range(nph) if cnt_buf[i]}
+        n = x.shape[0]
+        # 8-bit radix passes over keys of 3 x (bits of the largest cell index), cell size r
+        passes = (3 * int(math.floor(1.0 / r)).bit_length() + 7) // 8
+        peak = _peak_gbs()
+        hbm = {k: {"bytes": v, "gbs": v / (phases[k] / 1e3) / 1e9, "frac": v / (phases[k] / 1e3) / 1e9 / peak}
+               for k, v in phase_bytes(n, 0, tns.trees[sid - 1].n_nodes, 0, passes).items() if phases.get(k)}
+        out[name] = {"n_points": n, "radius": r, "ms_per_build": ms / reps, "radix_passes": passes,
+                     "phases_ms": {k: round(v, 5) for k, v in phases.items()}, "phase_hbm": hbm}
+        del tns, xd
+        torch.cuda.empty_cache()
+
+    build_only("build_only_uniform_16M_r0.006", wl.uniform(16_000_000, 3, 2031), 0.006, 5)
 
     # --- batched: 512 clouds, sizes log-uniform [500, 20000], r ~ U[0.03, 0.08]
     rng = np.random.default_rng(4)

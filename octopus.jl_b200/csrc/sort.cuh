@@ -29,16 +29,26 @@ static __global__ void __launch_bounds__(kSortThreads) k_hist(const K* __restric
     hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = cnt[threadIdx.x];
 }
 
+// Stable scatter of one tile: each key's rank among the tile's keys of its
+// digit (warp match within a warp, per-warp counters across warps), then the
+// tile is staged in shared memory in digit order so that each digit's run is
+// written to global memory by consecutive threads (whole sectors instead of
+// one scattered store per key).
 template <class K>
 static __global__ void __launch_bounds__(kSortThreads) k_scatter(const K* __restrict__ kin, const int32_t* __restrict__ vin,
                                                       K* __restrict__ kout, int32_t* __restrict__ vout, int64_t n,
                                                       int shift, const int32_t* __restrict__ hoff, int ntiles) {
     __shared__ int32_t wc[kSortThreads / 32][256];
+    __shared__ int32_t tstart[256];
+    __shared__ int32_t scan_sm[kSortThreads / 32 + 1];
+    __shared__ K skey[kSortTile];
+    __shared__ int32_t sval[kSortTile];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int j = 0; j < kSortThreads / 32; ++j) wc[j][threadIdx.x] = 0;
     __syncthreads();
-    const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)w * (32 * kSortItems);
+    const int64_t tbase = (int64_t)blockIdx.x * kSortTile;
+    const int64_t wbase = tbase + (int64_t)w * (32 * kSortItems);
     K key[kSortItems];
     int32_t val[kSortItems], rk[kSortItems];
     int dg[kSortItems];
@@ -60,23 +70,33 @@ static __global__ void __launch_bounds__(kSortThreads) k_scatter(const K* __rest
         dg[it] = d;
     }
     __syncthreads();
-    {
-        int32_t run = 0;
+    // per digit (thread = digit): warp offsets within the tile's run, and the
+    // run's start in the tile (exclusive scan over digits)
+    int32_t run = 0;
 #pragma unroll
-        for (int j = 0; j < kSortThreads / 32; ++j) {
-            const int32_t c = wc[j][threadIdx.x];
-            wc[j][threadIdx.x] = run;
-            run += c;
-        }
+    for (int j = 0; j < kSortThreads / 32; ++j) {
+        const int32_t c = wc[j][threadIdx.x];
+        wc[j][threadIdx.x] = run;
+        run += c;
     }
+    int32_t tile_total;
+    tstart[threadIdx.x] = block_exclusive_scan<int32_t>(run, scan_sm, &tile_total);
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
         if (dg[it] < 256) {
-            const int64_t dst = (int64_t)hoff[(int64_t)dg[it] * ntiles + blockIdx.x] + wc[w][dg[it]] + rk[it];
-            kout[dst] = key[it];
-            vout[dst] = val[it];
+            const int lp = tstart[dg[it]] + wc[w][dg[it]] + rk[it];
+            skey[lp] = key[it];
+            sval[lp] = val[it];
         }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < tile_total; i += kSortThreads) {
+        const K k = skey[i];
+        const int d = (int)((unsigned)(k >> shift) & 255u);
+        const int64_t dst = (int64_t)hoff[(int64_t)d * ntiles + blockIdx.x] + (i - tstart[d]);
+        kout[dst] = k;
+        vout[dst] = sval[i];
     }
 }
 
