@@ -975,12 +975,20 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         }
 
         // --- sort (stable: ties keep ascending original index, src/sort.jl:15-24)
-        if ((err = ensure(t.hist, sort_hist_bytes(n))) || (err = ensure(t.sort_tmp, sort_scan_bytes(n))))
-            return cuda_status(ctx, err, "allocating histograms");
         K* kb[2] = {t.keys[0].as<K>(), t.keys[1].as<K>()};
         int32_t* vb[2] = {t.vals[0].as<int32_t>(), t.vals[1].as<int32_t>()};
         int src;
-        {
+        if (n < kOnesweepMaxKeys) {
+            if ((err = ensure(t.look, onesweep_words(n, (t.key_bits + 7) / 8) * 4)))
+                return cuda_status(ctx, err, "allocating sort scratch");
+            int sms = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
+            PhaseTimer pt_(ctx, PH_SORT);
+            src = onesweep_sort_pairs<K>(kb, vb, t.look.as<uint32_t>(), n, t.key_bits, false, &hdr->status, sms, s,
+                                         &ctx.kernel_launches);
+        } else {
+            if ((err = ensure(t.hist, sort_hist_bytes(n))) || (err = ensure(t.sort_tmp, sort_scan_bytes(n))))
+                return cuda_status(ctx, err, "allocating histograms");
             PhaseTimer pt_(ctx, PH_SORT);
             src = radix_sort_pairs<K>(kb, vb, t.hist.as<int32_t>(), t.sort_tmp.as<int64_t>(), n, t.key_bits, false,
                                       s, &ctx.kernel_launches);
@@ -1130,6 +1138,8 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         if (moved == kSpeculate &&
             (t.hdr_host->nan_flag || t.hdr_host->n_moved > merge_cap(n) || (t.hdr_host->status & DF_KEY_WIDTH)))
             return kRetry;  // the bounds say the merge did not apply: build again on the usual path
+        if (t.hdr_host->status & DF_TIMEOUT)
+            return set_error(ctx, ERR_TIMEOUT, "tree build: a radix-sort look-back wait ran out");
         if (t.hdr_host->status & DF_NODE_OVERFLOW) {
             t.capacity = t.hdr_host->n_nodes + t.hdr_host->n_nodes / 8 + 64;
             const int zero = 0;

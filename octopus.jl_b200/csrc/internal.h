@@ -69,6 +69,7 @@ struct Tree {
     DevBuf keys[2], vals[2];     // radix-sort ping-pong
     DevBuf hist;                 // radix digit histograms (+1 total slot)
     DevBuf sort_tmp;             // int64 tile sums of the histogram scan
+    DevBuf look;                 // one-pass-per-digit sort: digit counts and tile look-back words
     DevBuf spts;                 // SPt<T,D>[n] in Morton order
     DevBuf iperm;                // int32 [n]: sorted position of each original point
     const int32_t* perm_dev = nullptr;  // original index of each sorted position (null: identity)
