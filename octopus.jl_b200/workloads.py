@@ -15,6 +15,7 @@ Workloads (float32):
   diff2m       3D, 2,000,000 points U[0,1)^3, r = 0.012
   batch512     3D, 512 clouds, sizes log-uniform in [500, 20000], each U[0,1)^3,
                radius U[0.03, 0.08] per cloud, one batched build + COO
+  build16m     3D, 16,000,000 points U[0,1)^3, r = 0.006: run! alone (full sort path)
 """
 from __future__ import annotations
 
@@ -85,6 +86,8 @@ def _run(name: str, steps: int, scale: float):
         r = 0.012 / scale ** (1 / 3)  # same neighbors per point at every scale
     elif name == "batch512":
         return _run_batch(ob, torch, steps)
+    elif name == "build16m":
+        return _run_build(ob, torch, uniform(int(16_000_000 * scale), 3, 2031), 0.006 / scale ** (1 / 3), steps)
     else:
         raise SystemExit(f"unknown workload {name}")
     if name == "diff2m":
@@ -102,6 +105,20 @@ def _run(name: str, steps: int, scale: float):
         e = ob.build_edges(tns, sid, sid)
         ob.synchronize(tns)
         print(f"{name}: n={x.shape[1]} edges={e.senders.numel()}")
+
+
+def _run_build(ob, torch, x, r, steps):
+    """run! alone (full sort path every step: refit mode off)."""
+    tns = ob.TNS(torch.float32, ndims=3)
+    ob.set_search_radius_(tns, r)
+    xd = torch.from_numpy(x).cuda().t()
+    sid = ob.add_point_set_(tns, xd)
+    ob.set_active_search_(tns, sid, sid)
+    for _ in range(steps):
+        ob.update_point_set_(tns, sid, xd)
+        ob.run_(tns)
+        ob.synchronize(tns)
+        print(f"build16m: n={x.shape[0]} nodes={tns.trees[sid - 1].n_nodes}")
 
 
 def batch_clouds(n_clouds: int = 512, seed: int = 4):
