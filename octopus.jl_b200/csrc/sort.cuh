@@ -147,12 +147,13 @@ constexpr uint32_t kLookAggregate = 1u << 30;
 constexpr uint32_t kLookPrefix = 2u << 30;
 constexpr uint32_t kLookValue = (1u << 30) - 1;
 constexpr int64_t kLookSpinLimit = 1 << 22;
-// Keys per sort this path takes.  Below ~2M keys its 1 + passes launches beat
-// the 5 launches per pass of radix_sort_pairs (measured on B200: 0.036 vs
-// 0.052 ms at 100k keys, 0.084 vs 0.101 ms at 1M); above, the serial walk
-// of each tile's look-back costs more than the launches save (0.82 vs 0.56 ms
-// at 16M).  Counts and prefixes are 30-bit values, far above this bound.
-constexpr int64_t kOnesweepMaxKeys = 2 * 1024 * 1024;
+// Keys per sort this path takes.  Below ~6M keys its 1 + passes launches beat
+// the 5 launches per pass of radix_sort_pairs (measured on B200, 3 passes:
+// 0.032 vs 0.035 ms at 100k keys, 0.078 vs 0.083 ms at 1M, 0.179 vs 0.190 ms
+// at 4M); above, the tiles' look-back walks cost more than the launches save
+// (0.33 vs 0.32 ms at 8M, 0.65 vs 0.57 ms at 16M).  Counts and prefixes are
+// 30-bit values, far above this bound.
+constexpr int64_t kOnesweepMaxKeys = 6 * 1024 * 1024;
 
 // Scratch words: for each of up to kOnesweepMaxPasses passes 256 digit counts
 // and a tile counter, then per pass 256 look-back words per tile; all zero
@@ -236,22 +237,37 @@ static __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K* __res
     uint32_t excl = 0;
     bool timed_out = false;
     if (t > 0) {
+        // Four predecessors per round trip: their words are read together,
+        // then added in order up to the first inclusive prefix; a word not
+        // yet published stops the round and is read again.
         int j = t - 1;
         int64_t spins = 0;
-        while (j >= 0) {
-            const uint32_t v = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(look[(size_t)j * 256 + d])
-                                   .load(cuda::memory_order_relaxed);
-            if ((v & ~kLookValue) == 0) {
+        while (true) {
+            uint32_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                v[u] = j - u >= 0 ? cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(look[(size_t)(j - u) * 256 + d])
+                                        .load(cuda::memory_order_relaxed)
+                                  : kLookPrefix;  // before tile 0: nothing more to add
+            int u = 0;
+            bool done = false;
+            for (; u < 4; ++u) {
+                if ((v[u] & ~kLookValue) == 0) break;
+                excl += v[u] & kLookValue;
+                if ((v[u] & ~kLookValue) == kLookPrefix) {
+                    done = true;
+                    break;
+                }
+            }
+            if (done) break;
+            j -= u;
+            if (u < 4) {
                 if (++spins > kLookSpinLimit) {
                     timed_out = true;
                     break;
                 }
                 __nanosleep(32);
-                continue;
             }
-            excl += v & kLookValue;
-            if ((v & ~kLookValue) == kLookPrefix) break;
-            --j;
         }
         mine.store(kLookPrefix | (excl + (uint32_t)run), cuda::memory_order_relaxed);
     }

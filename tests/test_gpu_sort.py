@@ -4,7 +4,7 @@ oracle's stable sort (src/sort.jl:15-24: ties keep ascending original index).
 Sizes sit at and around the sort's 2048-key tiles, and the points are drawn
 from a handful of positions, so most keys tie: the ranks of equal keys across
 tiles, and the prefixes each tile takes from the tiles before it, decide the
-permutation.  One size runs the staged passes used from 2M keys on."""
+permutation.  One size runs the staged passes used from 6M keys on."""
 import numpy as np
 import pytest
 import torch
@@ -37,9 +37,9 @@ def test_sort_uniform_matches_oracle(ob, oracle_mod, n):
     assert_tree_equal(tns.trees[sid - 1], oracle_mod.build_tree(x, r))
 
 
-def test_sort_staged_passes_above_2m_keys(ob, oracle_mod):
-    """2.2M keys take the staged radix passes; permutation as the oracle's."""
-    n = 2_200_000
+def test_sort_staged_passes_above_6m_keys(ob, oracle_mod):
+    """6.5M keys take the staged radix passes; permutation as the oracle's."""
+    n = 6_500_000
     x = tied_points(n, 5000, 77)
     r = np.float32(0.004)
     tns, sid = gpu_run(ob, x, r)
