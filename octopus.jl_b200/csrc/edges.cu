@@ -191,7 +191,6 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     __syncwarp();
     while (sp > 0) {
         const int2 ent = stack[w][--sp];
-        const bool asc = ent.x < 0;
         const int32_t na = ent.x & 0x7fffffff;
         const int32_t nb = ent.y;
         if (nb > 0) {
