@@ -258,17 +258,28 @@ __global__ void __launch_bounds__(kThreads) k_mark(const K* __restrict__ skeys, 
     }
     __syncthreads();
     const int64_t k = base + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    // max of sc[x .. x + 32] for x = threadIdx.x: the suffix maximum of the
+    // warp's first 32 entries from this lane on, with the prefix maximum of
+    // the next 32 up to this lane
+    int sa = sc[threadIdx.x], pb = sc[threadIdx.x + 32];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int a = __shfl_down_sync(0xffffffffu, sa, o);
+        const int b = __shfl_up_sync(0xffffffffu, pb, o);
+        if (lane + o < 32) sa = max(sa, a);
+        if (lane >= o) pb = max(pb, b);
+    }
     int lo = 1, hi = 0;
     if (k < n) {
         lo = (k == 0) ? 0 : common_levels_b<D, K>(sk[threadIdx.x + 31], sk[threadIdx.x + 32], bt) + 1;
-        int m = -1;
-#pragma unroll 11
-        for (int t = 0; t <= 32; ++t) m = max(m, (int)sc[threadIdx.x + t]);
-        hi = min(m + 1, MAXLEV);
+        hi = min(max(sa, pb) + 1, MAXLEV);
         lohi[k] = (uint16_t)(lo | (hi << 8));
     }
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int L = 0; L < NLEV; ++L) {
+    // per-level node counts of the warp, over the levels its positions span
+    const int wlo = warp_min(lo <= hi ? lo : NLEV), whi = warp_max(lo <= hi ? hi : -1);
+    if (lane < NLEV && (lane < wlo || lane > whi)) wcnt[lane][w] = 0;
+    for (int L = wlo; L <= whi; ++L) {
         const unsigned b = __ballot_sync(0xffffffffu, lo <= L && L <= hi);
         if (lane == 0) wcnt[L][w] = __popc(b);
     }
@@ -299,7 +310,9 @@ __global__ void __launch_bounds__(kThreads) k_emit_ids(int64_t n, const uint16_t
         lo = v & 0xff;
         hi = v >> 8;
     }
-    for (int L = 0; L < NLEV; ++L) {
+    const int wlo = warp_min(lo <= hi ? lo : NLEV), whi = warp_max(lo <= hi ? hi : -1);
+    if (lane < NLEV && (lane < wlo || lane > whi)) wpre[lane][w] = 0;
+    for (int L = wlo; L <= whi; ++L) {
         const unsigned b = __ballot_sync(0xffffffffu, lo <= L && L <= hi);
         if (lane == 0) wpre[L][w] = __popc(b);
     }
@@ -319,7 +332,7 @@ __global__ void __launch_bounds__(kThreads) k_emit_ids(int64_t n, const uint16_t
         return;
     }
     int32_t prev = -1;
-    for (int L = NLEV - 1; L >= 0; --L) {
+    for (int L = whi; L >= wlo; --L) {
         const bool in = lo <= L && L <= hi;
         const unsigned b = __ballot_sync(0xffffffffu, in);
         if (in) {
