@@ -622,18 +622,16 @@ def cpu_other_configs(oracle, nthreads):
 
 
 # ------------------------------------------------------ reference arm -----
-REF_PER = 40  # sample: a 40^3 sub-lattice per step
-
-
 def run_reference(args, rank, world):
     """The reference's CPU path (the oracle port: the Julia original cannot
-    run here) on all host threads; each step one time step of a 40^3
-    sub-lattice of the workload (same spacing, radius and displacement)."""
+    run here) on all host threads, on the same workload as our arm: the same
+    1,000,000-point lattice trajectory (same seed), W warm-up steps and K
+    timed steps, each step a full build + count + scan + fill."""
     if rank != 0:
         return None
     import oracle
     nthreads = oracle.max_threads()
-    snaps = snapshots_np(REF_PER, args.warmup + args.steps, 4242)
+    snaps = snapshots_np(PER, args.warmup + args.steps, 12345)
     r = np.float32(RADIUS)
     for x in snaps[:args.warmup]:
         oracle.build_edges(oracle.build_tree(x, r, nthreads=nthreads), x, exclude_self=True, nthreads=nthreads)
@@ -645,14 +643,16 @@ def run_reference(args, rank, world):
         secs += time.perf_counter() - t0
         edges += len(e["senders"])
     v = edges / secs
-    sample = f"{args.steps} time steps of a {REF_PER}^3-point sub-lattice (same h, radius, displacement)"
+    sample = (f"{args.steps} time steps of the {PER}^3-point lattice trajectory (the timed steps of our arm, "
+              f"same seed), each a full build + count + scan + fill")
     return {
         "impl": "reference",
         "metric": METRIC, "value": v, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded jittered lattice + Gaussian steps)",
-        "config": config_dict({"reference_sample": sample}),
+        "config": config_dict({"edges_per_step": edges / args.steps, "parallelism": "host threads",
+                               "reference_sample": sample}),
         "cpu_baseline": {"value": v, "unit": "edges/s", "cores": nthreads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -247,20 +247,62 @@ OCT_API int oct_edges_diff_backward_ordered(oct_ctx* ctx, int ndims, int dtype, 
  * framework's caching allocator, a fixed memory budget), where a raw
  * cudaMalloc may fail or fragment the pool, and latency-critical loops that
  * cannot afford the implicit device synchronization of cudaMalloc/cudaFree.
- * Same result as oct_edges_count for the pair, but the caller passes
- * counts[n_q] (int32, per query point) and offsets[n_q + 1] (int64 exclusive
- * scan, offsets[n_q] = edge total) as device outputs; *n_edges (optional,
- * host) receives the total after a stream synchronize.  The scan's scratch is
+ * Same result and the same argument rules as oct_edges_count for the pair
+ * (a batched tree only against itself with exclude_self = 1), but the caller
+ * passes counts[n_q] (int32, per query point) and offsets[n_q + 1] (int64
+ * exclusive scan, offsets[n_q] = edge total) as device outputs; *n_edges
+ * (optional, host) receives the total after a stream synchronize, so it must
+ * be NULL while the stream is being captured (OCT_ERR_STATE otherwise).  The scan's scratch is
  * a fixed 64 KiB device array that every GPU loading this library holds until
  * exit, which limits the query set to 16,777,216 points (larger sets get
  * OCT_ERR_CAPACITY).  The first call on a device looks up that array's device
- * address (make this first call before any stream capture begins).  All calls
+ * address (make this first call before any stream capture begins); that
+ * address does not survive cudaDeviceReset in the same process.  All calls
  * share the array: calls whose GPU work overlaps (other streams, other host
  * threads, other contexts on the same device) race and must not be issued.
  * It does not prepare oct_edges_fill. */
 OCT_API int oct_edges_count_noalloc(oct_ctx* ctx, const oct_tree* query, const oct_tree* target,
                                     int exclude_self, int32_t* counts, int64_t* offsets,
                                     int64_t* n_edges);
+
+/* Options of a context, read by every later call on it.  No counterpart in
+ * the reference, whose launch shapes and capacities are fixed in its CUDA
+ * extension; its overflow test drives the build kernels with a smaller node
+ * capacity than they need and a canary region past it
+ * (test/edges_cuda.jl:147-265), which OCT_OPT_NODE_CAPACITY and
+ * OCT_OPT_GUARD_CHECK do through this interface.
+ *   OCT_OPT_WAIT_LIMIT     polling rounds of a bounded device wait (the key
+ *                          sort's look-back) before it gives up; the build
+ *                          then returns OCT_ERR_TIMEOUT (default 4,194,304)
+ *   OCT_OPT_NODE_CAPACITY  node capacity of each build's first topology
+ *                          attempt, 0 = the estimate from the point count
+ *                          (default); a smaller one overflows and the build
+ *                          retries with the exact count
+ *   OCT_OPT_RECORD_CAP     hit records per query point of the next counts,
+ *                          0 = sized from the previous count (default); query
+ *                          groups that run out are written by a second walk
+ *   OCT_OPT_GUARD_CHECK    1: a canary region follows the written part of the
+ *                          sort buffers and node arrays, checked after each
+ *                          topology attempt (OCT_ERR_STATE if overwritten)
+ *   OCT_OPT_WITHHOLD_TILE  test aid: tile k (0-based) of the first pass of the
+ *                          look-back key sort never publishes its counts, so
+ *                          the waits after it run out (-1 = off, default)
+ * Read-only (oct_ctx_get_option):
+ *   OCT_STAT_BUILD_ATTEMPTS   topology attempts of the last build (1 = none retried)
+ *   OCT_STAT_RECORD_OVERFLOW  query groups of the last count whose records overflowed
+ *   OCT_STAT_RECORD_CAP       hit records per query point the last count used (0 = none) */
+enum {
+    OCT_OPT_WAIT_LIMIT = 1,
+    OCT_OPT_NODE_CAPACITY = 2,
+    OCT_OPT_RECORD_CAP = 3,
+    OCT_OPT_GUARD_CHECK = 4,
+    OCT_OPT_WITHHOLD_TILE = 5,
+    OCT_STAT_BUILD_ATTEMPTS = 100,
+    OCT_STAT_RECORD_OVERFLOW = 101,
+    OCT_STAT_RECORD_CAP = 102
+};
+OCT_API int oct_ctx_set_option(oct_ctx* ctx, int option, int64_t value);
+OCT_API int oct_ctx_get_option(const oct_ctx* ctx, int option, int64_t* value);
 
 /* Per-phase device timing with CUDA events on the context's stream (the
  * phase timers of benchmarks/profile_phases.jl:29-46, taken on the device).

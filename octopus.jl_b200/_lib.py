@@ -22,6 +22,16 @@ ERR_CAPACITY = 6
 ERR_TIMEOUT = 7
 ERR_STATE = 8
 
+# Context options (oct_ctx_set_option / oct_ctx_get_option).
+OPT_WAIT_LIMIT = 1
+OPT_NODE_CAPACITY = 2
+OPT_RECORD_CAP = 3
+OPT_GUARD_CHECK = 4
+OPT_WITHHOLD_TILE = 5
+STAT_BUILD_ATTEMPTS = 100
+STAT_RECORD_OVERFLOW = 101
+STAT_RECORD_CAP = 102
+
 
 class TreeView(C.Structure):
     """oct_tree_view."""
@@ -69,6 +79,8 @@ SIGNATURES = [
     ("oct_edges_diff_backward_recompute", I, [P, I, I, I64, I64, P, P, P, P, P, D, P]),
     ("oct_edges_diff_backward_ordered", I, [P, I, I, I64, I64, P, P, P, P, P, P, P, D, P, P]),
     ("oct_edges_count_noalloc", I, [P, P, P, I, P, P, C.POINTER(I64)]),
+    ("oct_ctx_set_option", I, [P, I, I64]),
+    ("oct_ctx_get_option", I, [P, I, C.POINTER(I64)]),
     ("oct_profile_enable", I, [P, I]),
     ("oct_profile_phase_name", C.c_char_p, [I]),
     ("oct_profile_read", I, [P, P, P, I]),

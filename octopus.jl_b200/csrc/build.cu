@@ -193,13 +193,21 @@ __global__ void __launch_bounds__(kThreads) k_encode(const T* __restrict__ coord
 }
 
 // ------------------------------------------------------------ 4. gather --
+// A permutation entry outside [0, n) can only come from a sort whose
+// look-back wait ran out (DF_TIMEOUT is then set already): it is skipped, so
+// neither the coordinate read nor the inverse-permutation store leaves its
+// array.
 template <class T, int D>
 __global__ void __launch_bounds__(kThreads) k_gather(const T* __restrict__ coords, const int32_t* __restrict__ perm,
                                                      int64_t n, SPt<T, D>* __restrict__ spts,
-                                                     int32_t* __restrict__ iperm) {
+                                                     int32_t* __restrict__ iperm, int* __restrict__ status) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int32_t j = perm ? perm[k] : (int32_t)k;
+    if ((uint64_t)(uint32_t)j >= (uint64_t)n) {
+        atomicOr(status, (int)DF_TIMEOUT);
+        return;
+    }
     SPt<T, D> p;
 #pragma unroll
     for (int d = 0; d < D; ++d) p.x[d] = coords[(int64_t)D * j + d];
@@ -955,8 +963,39 @@ __global__ void __launch_bounds__(kThreads) k_refit_prepare(int64_t nn, int64_t 
     }
 }
 
+// ----------------------------------------------------------- 11. guards --
+// Guard-check mode (OCT_OPT_GUARD_CHECK): a canary region follows the part of
+// each sort buffer and node array that the build may write; after each
+// topology attempt every canary byte is compared and the mismatches are
+// counted into hdr->guard_bad.
+constexpr size_t kGuardBytes = 16384;
+constexpr unsigned char kGuardByte = 0xA5;
+
+__global__ void k_guard_check(const unsigned char* __restrict__ p, int64_t len, int* __restrict__ bad) {
+    int c = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+        c += p[i] != kGuardByte;
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(bad, c);
+}
+
 // ------------------------------------------------------------- host side --
 namespace {
+
+// In guard-check mode, `b` holds `bytes` plus a canary region after them.
+cudaError_t ensure_g(const Ctx& ctx, DevBuf& b, size_t bytes) {
+    return ensure(b, bytes + (ctx.guard_check ? kGuardBytes : 0));
+}
+cudaError_t guard_fill(const Ctx& ctx, const DevBuf& b, size_t bytes) {
+    if (!ctx.guard_check) return cudaSuccess;
+    return cudaMemsetAsync(static_cast<unsigned char*>(b.p) + bytes, kGuardByte, kGuardBytes, ctx.stream);
+}
+void guard_check(Ctx& ctx, const DevBuf& b, size_t bytes, OctHeader* hdr) {
+    if (!ctx.guard_check) return;
+    k_guard_check<<<8, 256, 0, ctx.stream>>>(static_cast<const unsigned char*>(b.p) + bytes, (int64_t)kGuardBytes,
+                                            &hdr->guard_bad);
+    ctx.kernel_launches += 1;
+}
 
 template <class T, int D, class K>
 int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_t moved = -1, int prev = -1) {
@@ -977,9 +1016,13 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
     int sorted = -1;  // buffer holding this build's sorted keys and permutation
     if (moved == -1) {  // a full sort
         // --- encode
-        if ((err = ensure(t.keys[0], (size_t)n * sizeof(K))) || (err = ensure(t.keys[1], (size_t)n * sizeof(K))) ||
-            (err = ensure(t.vals[0], (size_t)n * 4)) || (err = ensure(t.vals[1], (size_t)n * 4)))
+        if ((err = ensure_g(ctx, t.keys[0], (size_t)n * sizeof(K))) ||
+            (err = ensure_g(ctx, t.keys[1], (size_t)n * sizeof(K))) || (err = ensure_g(ctx, t.vals[0], (size_t)n * 4)) ||
+            (err = ensure_g(ctx, t.vals[1], (size_t)n * 4)))
             return cuda_status(ctx, err, "allocating sort buffers");
+        for (int b = 0; b < 2; ++b)
+            if ((err = guard_fill(ctx, t.keys[b], (size_t)n * sizeof(K))) || (err = guard_fill(ctx, t.vals[b], (size_t)n * 4)))
+                return cuda_status(ctx, err, "sort buffer guards");
         {
             PhaseTimer pt_(ctx, PH_ENCODE);
             k_encode<T, D, K><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, n, o[0], o[1], o[2], inv_cs,
@@ -998,7 +1041,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
             PhaseTimer pt_(ctx, PH_SORT);
             src = onesweep_sort_pairs<K>(kb, vb, t.look.as<uint32_t>(), n, t.key_bits, false, &hdr->status, sms, s,
-                                         &ctx.kernel_launches);
+                                         &ctx.kernel_launches, ctx.wait_limit, ctx.withhold_tile);
         } else {
             if ((err = ensure(t.hist, sort_hist_bytes(n))) || (err = ensure(t.sort_tmp, sort_scan_bytes(n))))
                 return cuda_status(ctx, err, "allocating histograms");
@@ -1014,7 +1057,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         {
             PhaseTimer pt_(ctx, PH_GATHER);
             k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, perm, n, t.spts.as<SPt<T, D>>(),
-                                                                    t.iperm.as<int32_t>());
+                                                                    t.iperm.as<int32_t>(), &hdr->status);
             ctx.kernel_launches += 1;
         }
         t.last_path = 0;
@@ -1030,7 +1073,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             {
                 PhaseTimer pt_(ctx, PH_GATHER);
                 k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, vp, n, t.spts.as<SPt<T, D>>(),
-                                                                    t.iperm.as<int32_t>());
+                                                                    t.iperm.as<int32_t>(), &hdr->status);
                 ctx.kernel_launches += 1;
             }
             {
@@ -1098,18 +1141,28 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         (err = ensure(t.scan_tmp, (size_t)scan_tmp_elems(nbc) * 8)))
         return cuda_status(ctx, err, "allocating topology scratch");
     int64_t est = (int64_t)Dims<D>::nch * ((n + 31) / 32) + 2 * NLEV + 64;
-    if (t.capacity < est) t.capacity = est;
+    if (ctx.node_cap_override > 0)
+        t.capacity = ctx.node_cap_override;  // the first attempt's capacity, as set by the caller
+    else if (t.capacity < est)
+        t.capacity = est;
     for (int attempt = 0; attempt < 3; ++attempt) {
+        ctx.last_attempts = attempt + 1;
         const int64_t cap = t.capacity;
-        if ((err = ensure(t.tnode, (size_t)cap * sizeof(TNode<T, D>))) || (err = ensure(t.nrange, (size_t)cap * 8)) ||
-            (err = ensure(t.parent, (size_t)cap * 4)) || (err = ensure(t.arrive, (size_t)cap * 4)) ||
-            (err = ensure(t.fchild, (size_t)cap * 4)) ||
+        const size_t gcap = (size_t)(cap + n / 32 + 2);
+        if ((err = ensure_g(ctx, t.tnode, (size_t)cap * sizeof(TNode<T, D>))) ||
+            (err = ensure_g(ctx, t.nrange, (size_t)cap * 8)) || (err = ensure_g(ctx, t.parent, (size_t)cap * 4)) ||
+            (err = ensure_g(ctx, t.arrive, (size_t)cap * 4)) || (err = ensure_g(ctx, t.fchild, (size_t)cap * 4)) ||
             (err = ensure(t.scan_tmp, (size_t)scan_tmp_elems(nbc) * 8)) ||
-            (err = ensure(t.groups, (size_t)(cap + n / 32 + 2) * 8)) || (err = ensure(t.chain, 64 * 4)))
+            (err = ensure_g(ctx, t.groups, gcap * 8)) || (err = ensure(t.chain, 64 * 4)))
             return cuda_status(ctx, err, "allocating node arrays");
         if ((err = cudaMemsetAsync(t.chain.p, 0xff, 64 * 4, s)) ||
             (err = cudaMemsetAsync(&hdr->n_groups, 0, sizeof(int64_t), s)))
             return cuda_status(ctx, err, "chain reset");
+        if ((err = guard_fill(ctx, t.tnode, (size_t)cap * sizeof(TNode<T, D>))) ||
+            (err = guard_fill(ctx, t.nrange, (size_t)cap * 8)) || (err = guard_fill(ctx, t.parent, (size_t)cap * 4)) ||
+            (err = guard_fill(ctx, t.arrive, (size_t)cap * 4)) || (err = guard_fill(ctx, t.fchild, (size_t)cap * 4)) ||
+            (err = guard_fill(ctx, t.groups, gcap * 8)))
+            return cuda_status(ctx, err, "node array guards");
         if (bt.n_clouds && (err = cudaMemsetAsync(bt.croot, 0xff, (size_t)bt.n_clouds * 4, s)))
             return cuda_status(ctx, err, "cloud root reset");
         {
@@ -1145,9 +1198,24 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
                 ctx.kernel_launches += 1;
             }
         }
+        if (ctx.guard_check) {
+            guard_check(ctx, t.tnode, (size_t)cap * sizeof(TNode<T, D>), hdr);
+            guard_check(ctx, t.nrange, (size_t)cap * 8, hdr);
+            guard_check(ctx, t.parent, (size_t)cap * 4, hdr);
+            guard_check(ctx, t.arrive, (size_t)cap * 4, hdr);
+            guard_check(ctx, t.fchild, (size_t)cap * 4, hdr);
+            guard_check(ctx, t.groups, gcap * 8, hdr);
+            if (moved == -1)
+                for (int b = 0; b < 2; ++b) {
+                    guard_check(ctx, t.keys[b], (size_t)n * sizeof(K), hdr);
+                    guard_check(ctx, t.vals[b], (size_t)n * 4, hdr);
+                }
+        }
         if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
             (err = wait_stream(s)))
             return cuda_status(ctx, err, "tree build");
+        if (t.hdr_host->guard_bad)
+            return set_error(ctx, ERR_STATE, "tree build: a kernel wrote past the end of a sort buffer or node array");
         if (moved == kSpeculate &&
             (t.hdr_host->nan_flag || t.hdr_host->n_moved > merge_cap(n) || (t.hdr_host->status & DF_KEY_WIDTH)))
             return kRetry;  // the bounds say the merge did not apply: build again on the usual path

@@ -291,17 +291,27 @@ static int check_pair(oct_ctx* ctx, const oct_tree* query, const oct_tree* targe
     return OCT_OK;
 }
 
-OCT_API int oct_edges_count(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
-                            int64_t* n_edges) {
-    if (!ctx || !n_edges) return OCT_ERR_ARGUMENT;
-    ctx->c.last_error.clear();
-    *n_edges = 0;
-    int st = check_pair(ctx, query, target);
+}  // extern "C"
+
+int oct_check_count_pair(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self) {
+    const int st = check_pair(ctx, query, target);
     if (st != OCT_OK) return st;
     if (exclude_self && query != target)
         return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "exclude_self requires the same tree as query and target");
     if ((query->t.n_clouds > 0 || target->t.n_clouds > 0) && (query != target || !exclude_self))
         return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "a batched tree is searched against itself, self pairs excluded");
+    return OCT_OK;
+}
+
+extern "C" {
+
+OCT_API int oct_edges_count(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
+                            int64_t* n_edges) {
+    if (!ctx || !n_edges) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    *n_edges = 0;
+    const int st = oct_check_count_pair(ctx, query, target, exclude_self);
+    if (st != OCT_OK) return st;
     DeviceGuard g(ctx->c.device);
     return oct::edges_count(ctx->c, query->t, target->t, exclude_self != 0, n_edges);
 }
@@ -434,6 +444,53 @@ OCT_API int oct_edges_diff_backward_ordered(oct_ctx* ctx, int ndims, int dtype, 
     return oct::diff_backward(ctx->c, ndims, dtype, n_points, n_edges, senders, receivers,
                               coords ? nullptr : rel_displacement, coords ? nullptr : rel_dist_norm,
                               d_rel_displacement, d_rel_dist_norm, radius, grad_coords, coords, order);
+}
+
+OCT_API int oct_ctx_set_option(oct_ctx* ctx, int option, int64_t value) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    oct::Ctx& c = ctx->c;
+    c.last_error.clear();
+    switch (option) {
+        case OCT_OPT_WAIT_LIMIT:
+            if (value < 0) return oct::set_error(c, OCT_ERR_ARGUMENT, "wait limit must be >= 0");
+            c.wait_limit = value;
+            return OCT_OK;
+        case OCT_OPT_NODE_CAPACITY:
+            if (value < 0 || value > 2147483647LL)
+                return oct::set_error(c, OCT_ERR_ARGUMENT, "node capacity must be in [0, 2^31 - 1]");
+            c.node_cap_override = value;
+            return OCT_OK;
+        case OCT_OPT_RECORD_CAP:
+            if (value < 0) return oct::set_error(c, OCT_ERR_ARGUMENT, "record count must be >= 0");
+            c.rec_cap_override = value;
+            return OCT_OK;
+        case OCT_OPT_GUARD_CHECK:
+            c.guard_check = value != 0;
+            return OCT_OK;
+        case OCT_OPT_WITHHOLD_TILE:
+            if (value < -1 || value > 2147483647LL)
+                return oct::set_error(c, OCT_ERR_ARGUMENT, "withheld tile must be -1 or a tile index");
+            c.withhold_tile = (int32_t)value;
+            return OCT_OK;
+        default:
+            return oct::set_error(c, OCT_ERR_ARGUMENT, "unknown or read-only option");
+    }
+}
+
+OCT_API int oct_ctx_get_option(const oct_ctx* ctx, int option, int64_t* value) {
+    if (!ctx || !value) return OCT_ERR_ARGUMENT;
+    const oct::Ctx& c = ctx->c;
+    switch (option) {
+        case OCT_OPT_WAIT_LIMIT: *value = c.wait_limit; return OCT_OK;
+        case OCT_OPT_NODE_CAPACITY: *value = c.node_cap_override; return OCT_OK;
+        case OCT_OPT_RECORD_CAP: *value = c.rec_cap_override; return OCT_OK;
+        case OCT_OPT_GUARD_CHECK: *value = c.guard_check ? 1 : 0; return OCT_OK;
+        case OCT_OPT_WITHHOLD_TILE: *value = c.withhold_tile; return OCT_OK;
+        case OCT_STAT_BUILD_ATTEMPTS: *value = c.last_attempts; return OCT_OK;
+        case OCT_STAT_RECORD_OVERFLOW: *value = c.rec_overflow; return OCT_OK;
+        case OCT_STAT_RECORD_CAP: *value = c.rec_cap; return OCT_OK;
+        default: return OCT_ERR_ARGUMENT;
+    }
 }
 
 static const char* kPhaseNames[oct::PH_NUM] = {"bounds", "encode", "sort", "gather", "topology",

@@ -69,7 +69,7 @@ struct OctHeader {
     int32_t pad;
     int64_t n_groups;
     int32_t dfs_start;  // first node of the DFS below the root's single-child chain
-    int32_t pad2;
+    int32_t guard_bad;  // canary bytes found overwritten (guard-check mode)
     int64_t n_moved;    // refit mode: keys that changed since the previous build
 };
 

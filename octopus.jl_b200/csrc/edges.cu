@@ -622,10 +622,16 @@ namespace {
 constexpr int64_t kRecordBudget = 4LL << 30;
 constexpr int64_t kRecordBudgetMax = 32LL << 30;
 
+// A caller-set record count (OCT_OPT_RECORD_CAP) replaces the hint, within
+// the same budget; records are used when there is room for 8 per query point
+// (for a caller-set count, for 1).
 int64_t record_cap(const Ctx& ctx, int64_t nq) {
     const int64_t budget = std::min(std::max(kRecordBudget, 8 * ctx.rec_edges_hint), kRecordBudgetMax);
     const int64_t fit = budget / (8 * std::max<int64_t>(nq, 1));
-    return std::min<int64_t>(ctx.rec_cap_hint, fit);
+    const int64_t want = ctx.rec_cap_override > 0 ? std::min<int64_t>(ctx.rec_cap_override, kMaxRecords)
+                                                  : ctx.rec_cap_hint;
+    const int64_t cap = std::min<int64_t>(want, fit);
+    return cap >= (ctx.rec_cap_override > 0 ? 1 : 8) ? cap : 0;
 }
 
 template <class T, int D>
@@ -652,7 +658,7 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
         // Record each query's hits while counting, so that the fill pass
         // need not walk the tree again.
         const int64_t cap = record_cap(ctx, nq);
-        if (cap >= 8) {
+        if (cap > 0) {
             if ((err = ensure(ctx.recs, (size_t)nq * cap * 8)) || (err = ensure(ctx.rcount, (size_t)nq * 2)) ||
                 (err = ensure(ctx.gflag, (size_t)std::max<int64_t>(q.n_groups, 1))))
                 return cuda_status(ctx, err, "allocating hit records");

@@ -160,6 +160,17 @@ struct Ctx {
     DevBuf dredge;       // edges ordered by receiver (adjoint of a COO not grouped by receiver)
     DevBuf dterm;        // per-edge cotangent term of the self-pair adjoint (4 values)
     DevBuf dseg;         // per-point {first, end} edge of the self-pair adjoint
+    // Options (oct_ctx_set_option): the polling rounds of a bounded device
+    // wait; a node capacity for each build's first topology attempt (0 =
+    // estimate); hit records per query point (0 = automatic); canary regions
+    // after the sort buffers and node arrays, checked after each topology
+    // attempt; a look-back tile that never publishes (a test aid, -1 = off).
+    int64_t wait_limit = 1 << 22;
+    int64_t node_cap_override = 0;
+    int64_t rec_cap_override = 0;
+    bool guard_check = false;
+    int32_t withhold_tile = -1;
+    int32_t last_attempts = 0;    // topology attempts of the last build
     // Profiler.
     int64_t kernel_launches = 0;  // every kernel this context has launched
     bool profiling = false;

@@ -30,7 +30,10 @@ static __device__ __align__(256) int64_t g_count_scratch[kNoAllocTiles + 1];
 
 // Device address of g_count_scratch, looked up once per device.  In host
 // code the symbol's name is only a stand-in for the device array, so kernels
-// must be given this address instead.
+// must be given this address instead.  The cached address belongs to the
+// device's primary context: it does not survive cudaDeviceReset (nor a
+// primary-context reset by another library in the process), after which this
+// entry point must not be called again in the same process.
 constexpr int kMaxDevices = 64;
 int64_t* g_scratch_addr[kMaxDevices] = {};
 std::mutex g_scratch_mu;
@@ -69,15 +72,11 @@ extern "C" OCT_API int oct_edges_count_noalloc(oct_ctx* ctx, const oct_tree* que
     oct::Ctx& c = ctx->c;
     c.last_error.clear();
     if (n_edges) *n_edges = 0;
-    if (!query || !target) return oct::set_error(c, OCT_ERR_ARGUMENT, "query/target tree is NULL");
+    // The same rules as oct_edges_count, the batched-tree rule included.
+    const int st = oct_check_count_pair(ctx, query, target, exclude_self);
+    if (st != OCT_OK) return st;
     const oct::Tree& q = query->t;
     const oct::Tree& t = target->t;
-    if (q.ndims != t.ndims || q.dtype != t.dtype)
-        return oct::set_error(c, OCT_ERR_DIMENSION, "query and target trees differ in ndims or dtype");
-    if (!q.built || !t.built)
-        return oct::set_error(c, OCT_ERR_STATE, "query and target trees must be built before build_edges");
-    if (exclude_self && query != target)
-        return oct::set_error(c, OCT_ERR_ARGUMENT, "exclude_self requires the same tree as query and target");
     if (q.n > kNoAllocMaxQueries)
         return oct::set_error(c, OCT_ERR_CAPACITY,
                               "oct_edges_count_noalloc: the query set has more than 16,777,216 points, the "
@@ -85,8 +84,20 @@ extern "C" OCT_API int oct_edges_count_noalloc(oct_ctx* ctx, const oct_tree* que
     if (!offsets || (q.n > 0 && !counts))
         return oct::set_error(c, OCT_ERR_ARGUMENT, "counts/offsets output is NULL");
     CurrentDevice guard(c.device);
+    cudaError_t e;
+    if (n_edges) {
+        // Reading the total back means a host copy and a stream synchronize,
+        // neither of which a stream being captured allows.
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if ((e = cudaStreamIsCapturing(c.stream, &cs)) != cudaSuccess)
+            return oct::cuda_status(c, e, "cudaStreamIsCapturing");
+        if (cs != cudaStreamCaptureStatusNone)
+            return oct::set_error(c, OCT_ERR_STATE,
+                                  "oct_edges_count_noalloc: n_edges must be NULL while the stream is being captured "
+                                  "(the total is offsets[n_query])");
+    }
     int64_t* scratch = nullptr;
-    cudaError_t e = scratch_address(c.device, &scratch);
+    e = scratch_address(c.device, &scratch);
     if (e != cudaSuccess) return oct::cuda_status(c, e, "cudaGetSymbolAddress(scan scratch)");
     if ((e = oct::count_into(q, t, exclude_self != 0, counts, c.stream)) != cudaSuccess)
         return oct::cuda_status(c, e, "edge count launch");

@@ -146,6 +146,8 @@ constexpr int kOnesweepMaxPasses = 8;
 constexpr uint32_t kLookAggregate = 1u << 30;
 constexpr uint32_t kLookPrefix = 2u << 30;
 constexpr uint32_t kLookValue = (1u << 30) - 1;
+// Default number of polling rounds a look-back wait makes before it gives up
+// (a context option, OCT_OPT_WAIT_LIMIT, overrides it).
 constexpr int64_t kLookSpinLimit = 1 << 22;
 // Keys per sort this path takes.  Below ~6M keys its 1 + passes launches beat
 // the 5 launches per pass of radix_sort_pairs (measured on B200, 3 passes:
@@ -183,7 +185,8 @@ static __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K* __res
                                                                    K* __restrict__ kout, int32_t* __restrict__ vout,
                                                                    int64_t n, int pass, int ntiles,
                                                                    uint32_t* __restrict__ scratch,
-                                                                   int* __restrict__ status) {
+                                                                   int* __restrict__ status, int64_t spin_limit,
+                                                                   int withhold_tile) {
     __shared__ int32_t wc[kSortThreads / 32][256];
     __shared__ int32_t tstart[256];
     __shared__ int64_t gstart[256];
@@ -233,7 +236,10 @@ static __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K* __res
     }
     const int d = threadIdx.x;
     cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(look[(size_t)t * 256 + d]);
-    mine.store((t == 0 ? kLookPrefix : kLookAggregate) | (uint32_t)run, cuda::memory_order_relaxed);
+    // A withheld tile (a test aid: pass 0, tile `withhold_tile`) never
+    // publishes, so the waits of the tiles after it run out.
+    const bool publish = !(pass == 0 && t == withhold_tile);
+    if (publish) mine.store((t == 0 ? kLookPrefix : kLookAggregate) | (uint32_t)run, cuda::memory_order_relaxed);
     uint32_t excl = 0;
     bool timed_out = false;
     if (t > 0) {
@@ -262,14 +268,14 @@ static __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K* __res
             if (done) break;
             j -= u;
             if (u < 4) {
-                if (++spins > kLookSpinLimit) {
+                if (++spins > spin_limit) {
                     timed_out = true;
                     break;
                 }
                 __nanosleep(32);
             }
         }
-        mine.store(kLookPrefix | (excl + (uint32_t)run), cuda::memory_order_relaxed);
+        if (publish) mine.store(kLookPrefix | (excl + (uint32_t)run), cuda::memory_order_relaxed);
     }
     int32_t tile_total, all;
     tstart[d] = block_exclusive_scan<int32_t>(run, scan_sm, &tile_total);
@@ -302,10 +308,13 @@ static __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K* __res
 // The same contract as radix_sort_pairs (stable, result in buffers
 // (k[r], v[r]) with r returned), for n < kOnesweepMaxKeys; `scratch` holds
 // onesweep_words(n, kOnesweepMaxPasses) words.  A look-back wait that ran out
-// leaves DF_TIMEOUT in *status and an unusable result.
+// (after spin_limit polling rounds) leaves DF_TIMEOUT in *status and an
+// unusable result, whose values may be stale; every store stays inside the
+// n-entry outputs.  withhold_tile >= 0 is a test aid (see k_onesweep).
 template <class K>
 int onesweep_sort_pairs(K* k[2], int32_t* v[2], uint32_t* scratch, int64_t n, int bits, bool vals_in,
-                        int* status, int sms, cudaStream_t s, int64_t* launches) {
+                        int* status, int sms, cudaStream_t s, int64_t* launches,
+                        int64_t spin_limit = kLookSpinLimit, int withhold_tile = -1) {
     const int passes = (bits + 7) / 8;
     if (passes == 0) return 0;
     const int ntiles = sort_tiles(n);
@@ -316,7 +325,8 @@ int onesweep_sort_pairs(K* k[2], int32_t* v[2], uint32_t* scratch, int64_t n, in
     int src = 0;
     for (int p = 0; p < passes; ++p) {
         k_onesweep<K><<<ntiles, kSortThreads, 0, s>>>(k[src], (p == 0 && !vals_in) ? nullptr : v[src], k[src ^ 1],
-                                                      v[src ^ 1], n, p, ntiles, scratch, status);
+                                                      v[src ^ 1], n, p, ntiles, scratch, status, spin_limit,
+                                                      withhold_tile);
         src ^= 1;
     }
     *launches += 1 + passes;

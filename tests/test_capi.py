@@ -48,6 +48,9 @@ def test_null_arguments_are_rejected_without_a_device(ob):
     assert lib.oct_tree_build(None, None, None, 0, 1.0, 0) == ob._lib.ERR_ARGUMENT
     assert lib.oct_edges_count(None, None, None, 0, None) == ob._lib.ERR_ARGUMENT
     assert lib.oct_ctx_destroy(None) == ob._lib.OK
+    assert lib.oct_ctx_set_option(None, ob._lib.OPT_WAIT_LIMIT, 10) == ob._lib.ERR_ARGUMENT
+    assert lib.oct_ctx_get_option(None, ob._lib.OPT_WAIT_LIMIT, None) == ob._lib.ERR_ARGUMENT
+    assert lib.oct_edges_count_noalloc(None, None, None, 1, None, None, None) == ob._lib.ERR_ARGUMENT
     assert lib.oct_ctx_last_error(None) == b""
 
 
