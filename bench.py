@@ -49,16 +49,21 @@ FILL_DRAM_BYTES_PER_EDGE = 23.9
 def phase_bytes(n, e, n_nodes, path, passes=3):
     """Algorithmic HBM bytes per step of the HBM-bound build phases and of
     the edge write, for float32 3D and the kernels that run in `path`
-    (0 full sort: k_encode + `passes` radix passes + k_gather; 1 refit-mode
-    merge: k_resort_mark + k_resort_merge, which also gathers)."""
+    (0 full sort: the key sort that carries the points, with the encode fused
+    in; 1 refit-mode merge: k_resort_mark + k_resort_merge, which also gathers)."""
     b = {"bounds": 12 * n}                          # coordinates read once
     if path == 1:
         b["encode"] = (4 + 12 + 4 + 1) * n            # perm, gathered coords, old key in; changed flag out
         b["sort"] = (4 + 4 + 1 + 12 + 4 + 4 + 16 + 4) * n  # key, perm, flag, coords in; key, perm, point, inverse out
     else:
-        b["encode"] = (12 + 4) * n                    # coords in; key out
-        b["sort"] = passes * (4 + 4 + 4 + 4 + 4) * n  # per pass: keys for the histogram; keys, values in and out
-        b["gather"] = (4 + 12 + 16 + 4) * n           # perm, gathered coords in; sorted point, inverse out
+        # digit counts read the coordinates (12); the first pass reads them
+        # again and writes key + point (12 + 20); a middle pass moves key +
+        # point (20 + 20); the last also writes the permutation and its
+        # inverse (20 + 20 + 4 + 4)
+        if passes <= 1:
+            b["sort"] = (12 + 12 + 20 + 8) * n
+        else:
+            b["sort"] = (12 + 32 + 40 * (passes - 2) + 48) * n
     b["refit"] = 16 * n + 2 * 32 * n_nodes          # sorted points in; node records read and written
     if e:
         b["fill"] = (12 + 4 * 3) * e + 8 * n        # (12 + 4D) E + 8N
@@ -201,6 +206,20 @@ def replica_totals(ms: float, edges: float, world: int, device=None):
     return ms_max, tot, tot / (ms_max / 1e3)
 
 
+def tuning_used(ob, lib, ctx, ndims, n, nbrs):
+    """The tuning-table row the last count used and the shapes it gives."""
+    row = C.c_int64(-1)
+    lib.oct_ctx_get_option(ctx.handle, ob._lib.STAT_TUNING_ROW, C.byref(row))
+    table = os.environ.get("OCTOPUS_B200_TUNING", ob.api.TUNING_TABLE)
+    shapes = (C.c_int32 * 5)()
+    r2 = C.c_int32(-1)
+    st = lib.oct_tuning_select((table if table and os.path.exists(table) else "").encode(), ndims, 0, int(n),
+                               float(nbrs), shapes, C.byref(r2))
+    names = ("max_seg", "multi_pop", "fill_chunk", "group_cap", "sub_boxes")
+    return {"table": os.path.relpath(table, ROOT) if table and os.path.exists(table) else None,
+            "row": int(row.value), "shapes": dict(zip(names, list(shapes))) if st == 0 else None}
+
+
 # ------------------------------------------------------------ our arm -----
 def run_ours(args, rank, world, local):
     import torch
@@ -254,6 +273,7 @@ def run_ours(args, rank, world, local):
     clk = clocks.stop()
     ms = t0.elapsed_time(t1)
     launches = lib.oct_profile_kernel_launches(ctx.handle) - launches0
+    tuning = tuning_used(ob, lib, ctx, 3, N, edges / K / N)
     # phase breakdown: the next K steps with the per-phase event timers on
     lib.oct_profile_read(ctx.handle, ms_buf, cnt_buf, nph)  # clear
     lib.oct_profile_enable(ctx.handle, 1)
@@ -357,6 +377,7 @@ def run_ours(args, rank, world, local):
             "phase_records": phase_calls,
             "dominant_phase": dominant,
             "gpu_launches": int(launches),
+            "tuning": tuning,
             "clocks": clk,
             "cpu_baseline": cpu,
             "other_configs": sec,

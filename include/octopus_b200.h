@@ -144,6 +144,19 @@ OCT_API int oct_tree_view_get(oct_ctx* ctx, oct_tree* tree, oct_tree_view* out);
 OCT_API int oct_edges_count(oct_ctx* ctx, const oct_tree* query, const oct_tree* target,
                             int exclude_self, int64_t* n_edges);
 
+/* Traversal statistics of the count pass for the pair (a diagnostic; the
+ * reference's phase timers, benchmarks/profile_phases.jl:29-46, have no
+ * counterpart at this level).  Runs the count pass once more with counters
+ * and writes up to n_stats totals: [0] query groups, [1] query points,
+ * [2] internal-node expansion rounds, [3] child boxes tested, [4] leaf chunks
+ * staged, [5] target points staged, [6] pair-loop steps (four targets each),
+ * [7] query-target distance tests issued, [8] pairs within the radius,
+ * [9] SM cycles of the traversing warps, [10] of which in leaf chunks,
+ * [11] of which in the pair loop.  Synchronizes; an oct_edges_fill must be
+ * preceded by a new oct_edges_count. */
+OCT_API int oct_edges_traversal_stats(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
+                                      uint64_t* stats, int n_stats);
+
 /* Pass B of build_edges: write the flat COO of the last oct_edges_count on
  * the same pair into caller-owned device buffers of at least `capacity`
  * edges: senders (target j), receivers (query i), rel_displacement =
@@ -153,6 +166,15 @@ OCT_API int oct_edges_count(oct_ctx* ctx, const oct_tree* query, const oct_tree*
 OCT_API int oct_edges_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* target,
                            int exclude_self, int32_t* senders, int32_t* receivers,
                            void* rel_displacement, void* rel_dist_norm, int64_t capacity);
+
+/* The forward of build_edges_diff for a self pair (the primal of
+ * ext/OctopusCUDAChainRulesCoreExt.jl:21-32): oct_edges_fill of the last
+ * oct_edges_count on (tree, tree, exclude_self = 1), plus mirror[k] = the
+ * 0-based COO index of edge k's mirror (for k = (i <- j), the edge (j <- i)),
+ * for oct_edges_diff_backward_mirror.  Not for a batched tree; at most
+ * 2^31 - 1 edges (OCT_ERR_OVERFLOW). */
+OCT_API int oct_edges_fill_diff(oct_ctx* ctx, const oct_tree* tree, int32_t* senders, int32_t* receivers,
+                                void* rel_displacement, void* rel_dist_norm, int32_t* mirror, int64_t capacity);
 
 /* materialize_all_neighbors! for the pair of the last oct_edges_count:
  * CSR neighbor lists, offsets (n_query + 1 Int32, offsets[0] = 0, row i of
@@ -176,6 +198,20 @@ OCT_API int oct_csr_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* ta
  * prepare_zsort's error, src/api.jl:380-386). */
 OCT_API int oct_zsort_apply(oct_ctx* ctx, const oct_tree* tree, const void* in, void* out, int64_t n,
                             int64_t row_bytes, int direction);
+
+/* The zsort hook in the reference's own shape: _apply_zsort_cuda(perm,
+ * user_array) (ext/OctopusCUDAExt.jl:422-432, called from apply_zsort,
+ * src/api.jl:404-408) with `perm` any 1-based Int32 device vector of n
+ * entries (tns.permutation[set_id]).  `in` and `out` are distinct device
+ * arrays of n rows of row_bytes bytes (a (F, n) column-major matrix has rows
+ * of F elements).  direction 0: out[:, i] = in[:, perm[i]] (the reference's
+ * user_array[:, perm]); direction 1: out[:, perm[i]] = in[:, i] (the scatter
+ * of its rrule's pullback, ext/OctopusChainRulesCoreExt.jl:83-94).  An entry
+ * outside 1..n is not dereferenced: the call returns OCT_ERR_ARGUMENT (the
+ * reference's BoundsError).  Waits for the permute (it reads that check
+ * back). */
+OCT_API int oct_permute_rows(oct_ctx* ctx, const int32_t* perm, int64_t n, const void* in, void* out,
+                             int64_t row_bytes, int direction);
 
 /* Neighbors of n_queries points (device coords, (ndims, n_queries)) in the
  * target tree, in the reference's traversal order and without the self
@@ -241,6 +277,20 @@ OCT_API int oct_edges_diff_backward_ordered(oct_ctx* ctx, int ndims, int dtype, 
                                             const void* d_rel_displacement, const void* d_rel_dist_norm,
                                             double radius, void* grad_coords, const int32_t* order);
 
+/* The self-pair pullback in one pass, with the mirror indices that
+ * oct_edges_fill_diff wrote for this COO: the same gradient, bit for bit, as
+ * oct_edges_diff_backward_ordered (same arguments, plus `mirror`), without
+ * searching each edge's mirror.  A mirror index outside the COO, or a COO not
+ * grouped by receiver, falls back to that entry point's path.  Replaces the
+ * pullback of ext/OctopusCUDAChainRulesCoreExt.jl:118-167
+ * (ext/OctopusChainRulesCoreExt.jl:137-192 on the CPU). */
+OCT_API int oct_edges_diff_backward_mirror(oct_ctx* ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,
+                                           const int32_t* senders, const int32_t* receivers, const int32_t* mirror,
+                                           const void* rel_displacement, const void* rel_dist_norm,
+                                           const void* coords, const void* d_rel_displacement,
+                                           const void* d_rel_dist_norm, double radius, void* grad_coords,
+                                           const int32_t* order);
+
 /* Edge count that allocates no device memory.  No counterpart in the
  * reference: it serves callers that cannot let a library call cudaMalloc --
  * hosts whose device memory belongs to their own pool allocator (a
@@ -287,7 +337,16 @@ OCT_API int oct_edges_count_noalloc(oct_ctx* ctx, const oct_tree* query, const o
  *   OCT_OPT_WITHHOLD_TILE  test aid: tile k (0-based) of the first pass of the
  *                          look-back key sort never publishes its counts, so
  *                          the waits after it run out (-1 = off, default)
+ * Kernel shapes (no result depends on them; 0 = the tuning table's choice,
+ * or the default when no table is loaded, see oct_ctx_load_tuning):
+ *   OCT_OPT_MAX_SEG        leaves sharing one staged chunk of the traversal, 1..16 (16)
+ *   OCT_OPT_MULTI_POP      internal nodes the traversal expands together, 1..4 (4)
+ *   OCT_OPT_FILL_CHUNK     edges per bulk-copy chunk of the fill: 32, 64 or 128 (64)
+ *   OCT_OPT_GROUP_CAP      query points per traversal group, 8..32 (32), set at the build
+ *   OCT_OPT_SUB_BOXES      boxes a group's queries are split into (runs of 32/k lanes)
+ *                          for the test that skips distant target points: 1, 2 or 4 (1)
  * Read-only (oct_ctx_get_option):
+ *   OCT_STAT_TUNING_ROW       tuning-table row the last count or build used (-1 = defaults)
  *   OCT_STAT_BUILD_ATTEMPTS   topology attempts of the last build (1 = none retried)
  *   OCT_STAT_RECORD_OVERFLOW  query groups of the last count whose records overflowed
  *   OCT_STAT_RECORD_CAP       hit records per query point the last count used (0 = none) */
@@ -297,12 +356,36 @@ enum {
     OCT_OPT_RECORD_CAP = 3,
     OCT_OPT_GUARD_CHECK = 4,
     OCT_OPT_WITHHOLD_TILE = 5,
+    OCT_OPT_MAX_SEG = 6,
+    OCT_OPT_MULTI_POP = 7,
+    OCT_OPT_FILL_CHUNK = 8,
+    OCT_OPT_GROUP_CAP = 9,
+    OCT_OPT_SUB_BOXES = 10,
+    OCT_STAT_TUNING_ROW = 99,
     OCT_STAT_BUILD_ATTEMPTS = 100,
     OCT_STAT_RECORD_OVERFLOW = 101,
     OCT_STAT_RECORD_CAP = 102
 };
 OCT_API int oct_ctx_set_option(oct_ctx* ctx, int option, int64_t value);
 OCT_API int oct_ctx_get_option(const oct_ctx* ctx, int option, int64_t* value);
+
+/* Load the kernel-shape table written by the autotuner
+ * (octopus.jl_b200/tune.py; the package ships octopus.jl_b200/tuning.tsv):
+ * one row per line, "ndims dtype nlog2 nbr_log2 max_seg multi_pop fill_chunk
+ * group_cap [sub_boxes]", '#' comments.  Each count (and each build, for group_cap) then
+ * uses the row of the same ndims and dtype nearest to its point count
+ * (log2) and neighbors per point (log2 of 1 + the last count's average),
+ * unless an option forces a shape.  NULL or "" unloads the table.  No
+ * counterpart in the reference, whose launch shapes are fixed
+ * (ext/OctopusCUDAExt.jl:374-376, ext/cuda_build.jl:240-241). */
+OCT_API int oct_ctx_load_tuning(oct_ctx* ctx, const char* path);
+
+/* The selection of oct_ctx_load_tuning without a context or a device: the
+ * shapes {max_seg, multi_pop, fill_chunk, group_cap, sub_boxes} the table at
+ * `path` ("" = no table) gives a set of n points with nbrs_per_point neighbors per point
+ * (< 0: not known yet), and the row (-1 = defaults). */
+OCT_API int oct_tuning_select(const char* path, int ndims, int dtype, int64_t n, double nbrs_per_point,
+                              int32_t* shapes, int32_t* row);
 
 /* Per-phase device timing with CUDA events on the context's stream (the
  * phase timers of benchmarks/profile_phases.jl:29-46, taken on the device).

@@ -28,6 +28,12 @@ OPT_NODE_CAPACITY = 2
 OPT_RECORD_CAP = 3
 OPT_GUARD_CHECK = 4
 OPT_WITHHOLD_TILE = 5
+OPT_MAX_SEG = 6
+OPT_MULTI_POP = 7
+OPT_FILL_CHUNK = 8
+OPT_GROUP_CAP = 9
+OPT_SUB_BOXES = 10
+STAT_TUNING_ROW = 99
 STAT_BUILD_ATTEMPTS = 100
 STAT_RECORD_OVERFLOW = 101
 STAT_RECORD_CAP = 102
@@ -70,22 +76,31 @@ SIGNATURES = [
     ("oct_tree_n_nodes", I, [P, P, C.POINTER(I64)]),
     ("oct_tree_view_get", I, [P, P, C.POINTER(TreeView)]),
     ("oct_edges_count", I, [P, P, P, I, C.POINTER(I64)]),
+    ("oct_edges_traversal_stats", I, [P, P, P, I, P, I]),
     ("oct_edges_fill", I, [P, P, P, I, P, P, P, P, I64]),
+    ("oct_edges_fill_diff", I, [P, P, P, P, P, P, P, I64]),
     ("oct_csr_fill", I, [P, P, P, I, P, P, I64]),
     ("oct_zsort_apply", I, [P, P, P, P, I64, I64, I]),
+    ("oct_permute_rows", I, [P, P, I64, P, P, I64, I]),
     ("oct_neighbors", I, [P, P, P, I64, P, P, I64]),
     ("oct_edges_diff_backward", I, [P, I, I, I64, I64, P, P, P, P, P, P, D, P]),
     ("oct_edges_diff_backward_pair", I, [P, I, I, I64, I64, I64, P, P, P, P, P, P, D, P, P]),
     ("oct_edges_diff_backward_recompute", I, [P, I, I, I64, I64, P, P, P, P, P, D, P]),
     ("oct_edges_diff_backward_ordered", I, [P, I, I, I64, I64, P, P, P, P, P, P, P, D, P, P]),
+    ("oct_edges_diff_backward_mirror", I, [P, I, I, I64, I64, P, P, P, P, P, P, P, P, D, P, P]),
     ("oct_edges_count_noalloc", I, [P, P, P, I, P, P, C.POINTER(I64)]),
     ("oct_ctx_set_option", I, [P, I, I64]),
     ("oct_ctx_get_option", I, [P, I, C.POINTER(I64)]),
+    ("oct_ctx_load_tuning", I, [P, C.c_char_p]),
+    ("oct_tuning_select", I, [C.c_char_p, I, I, I64, D, P, P]),
     ("oct_profile_enable", I, [P, I]),
     ("oct_profile_phase_name", C.c_char_p, [I]),
     ("oct_profile_read", I, [P, P, P, I]),
     ("oct_profile_kernel_launches", I64, [P]),
 ]
+
+TRAVERSAL_STATS = ["groups", "queries", "expansions", "children_tested", "leaf_chunks", "targets_staged",
+                   "pair_steps", "pair_tests", "hits", "cycles_total", "cycles_leaf", "cycles_pairs"]
 
 PHASES = ["bounds", "encode", "sort", "gather", "topology", "refit", "count", "scan", "fill", "adjoint", "groups"]
 

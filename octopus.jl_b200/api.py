@@ -15,6 +15,7 @@ Exceptions mirror the reference's: :class:`ArgumentError`,
 from __future__ import annotations
 
 import ctypes as C
+import os
 from collections import namedtuple
 from typing import Callable
 
@@ -22,6 +23,9 @@ import numpy as np
 import torch
 
 from . import _lib
+
+
+TUNING_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.tsv")
 
 
 # ----------------------------------------------------------------- errors --
@@ -62,6 +66,11 @@ class _Context:
             raise RuntimeError(f"oct_ctx_create({device}) failed: status {st}")
         self.handle = h
         self.device = device
+        # Kernel shapes measured by tune.py: the packaged table unless
+        # OCTOPUS_B200_TUNING names another (or is empty: built-in defaults).
+        table = os.environ.get("OCTOPUS_B200_TUNING", TUNING_TABLE)
+        if table and os.path.exists(table):
+            self.check(self.lib.oct_ctx_load_tuning(self.handle, table.encode()), "oct_ctx_load_tuning")
 
     @classmethod
     def get(cls, device: int) -> "_Context":
@@ -561,10 +570,25 @@ def device_view(tns: TNS, qid: int, tid: int) -> DeviceView:
 class _EdgesDiff(torch.autograd.Function):
     @staticmethod
     def forward(ctx, coords, tns, set_id, radius, recompute):
-        e = build_edges(tns, set_id, set_id)
-        snd, rcv = e.senders.clone(), e.receivers.clone()
-        disp = e.rel_displacement.t().contiguous().t()  # fresh copy, column-major
-        dist = e.rel_dist_norm.t().contiguous().t()
+        # The primal writes fresh arrays (the reference copies build_edges'
+        # buffer, ext/OctopusCUDAChainRulesCoreExt.jl:21-32) together with
+        # each edge's mirror index, which the backward pass uses.
+        n_edges = 0
+        got = _count_pair(tns, set_id, set_id, "build_edges_diff")
+        if got is not None:
+            lc, qtree, ttree, excl, n_edges = got
+            if n_edges > 2**31 - 1:
+                raise OctopusError(f"build_edges_diff: {n_edges} edges exceed the Int32 edge count")
+        dev = f"cuda:{tns.device}"
+        snd = torch.empty(n_edges, dtype=torch.int32, device=dev)
+        rcv = torch.empty(n_edges, dtype=torch.int32, device=dev)
+        disp_rows = torch.empty((n_edges, tns.ndims), dtype=tns.T, device=dev)
+        dist = torch.empty((1, n_edges), dtype=tns.T, device=dev)
+        mirror = torch.empty(n_edges, dtype=torch.int32, device=dev)
+        if n_edges > 0:
+            lc.check(lc.lib.oct_edges_fill_diff(lc.handle, ttree.handle, _ptr(snd), _ptr(rcv), _ptr(disp_rows),
+                                                _ptr(dist), _ptr(mirror), n_edges), "build_edges_diff")
+        disp = disp_rows.t()  # (D, E) column-major
         ctx.tns = tns
         ctx.radius = float(radius)
         ctx.coords_shape = coords.shape
@@ -584,9 +608,9 @@ class _EdgesDiff(torch.autograd.Function):
         if ctx.recompute:
             # Keep only the indices and the coordinates: the backward pass
             # recomputes the features (memory-lean mode).
-            ctx.save_for_backward(snd, rcv, colmajor(coords.detach()), order)
+            ctx.save_for_backward(snd, rcv, mirror, colmajor(coords.detach()), order)
         else:
-            ctx.save_for_backward(snd, rcv, disp, dist, order)
+            ctx.save_for_backward(snd, rcv, mirror, disp, dist, order)
         ctx.mark_non_differentiable(snd, rcv)
         return snd, rcv, disp, dist
 
@@ -602,14 +626,14 @@ class _EdgesDiff(torch.autograd.Function):
         lc = tns._ctx
         lc.bind_stream()
         if ctx.recompute:
-            snd, rcv, xc, order = ctx.saved_tensors
+            snd, rcv, mirror, xc, order = ctx.saved_tensors
             disp_p, dist_p, xc_p = None, None, _ptr(xc)
         else:
-            snd, rcv, disp, dist, order = ctx.saved_tensors
+            snd, rcv, mirror, disp, dist, order = ctx.saved_tensors
             disp_p, dist_p, xc_p = _ptr(disp.t()), _ptr(dist), None
-        lc.check(lc.lib.oct_edges_diff_backward_ordered(
-            lc.handle, d, _dtype_code(T), n, snd.numel(), _ptr(snd), _ptr(rcv), disp_p, dist_p, xc_p, _ptr(dd),
-            _ptr(dn), ctx.radius, _ptr(grad), _ptr(order) if order.numel() == n else None),
+        lc.check(lc.lib.oct_edges_diff_backward_mirror(
+            lc.handle, d, _dtype_code(T), n, snd.numel(), _ptr(snd), _ptr(rcv), _ptr(mirror), disp_p, dist_p, xc_p,
+            _ptr(dd), _ptr(dn), ctx.radius, _ptr(grad), _ptr(order) if order.numel() == n else None),
             "build_edges_diff pullback")
         return grad.t(), None, None, None, None
 

@@ -25,6 +25,7 @@
 #include <cuda/atomic>
 
 #include "internal.h"
+#include "pointsort.cuh"
 #include "scan.cuh"
 #include "sort.cuh"
 
@@ -507,9 +508,9 @@ __global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n,
 }
 
 // ------------------------------------------------------- 7. query groups --
-// A query group is a run of consecutive sibling leaves holding at most 32
-// points in total (a leaf of more than 32 points, possible at the last
-// level, is cut into chunks of 32).  Siblings share a parent box, so a
+// A query group is a run of consecutive sibling leaves holding at most gmax
+// (<= 32, a tuned shape) points in total (a leaf of more than gmax points is
+// cut into chunks of gmax).  Siblings share a parent box, so a
 // group's points are spatially compact; a window of 32 consecutive sorted
 // positions can instead straddle a jump of the Morton curve and span the
 // whole domain.  Each node counts the groups formed under it, a warp reserves
@@ -520,7 +521,7 @@ template <class T, int D>
 __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restrict__ tnode, int64_t capacity,
                                                      int2* __restrict__ groups, int64_t group_cap,
                                                      const int32_t* __restrict__ chain,
-                                                     const int32_t* __restrict__ parent, OctHeader* hdr) {
+                                                     const int32_t* __restrict__ parent, OctHeader* hdr, int gmax) {
     const int64_t nn = hdr->n_nodes;
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id == 0 && nn <= capacity) {
@@ -548,7 +549,7 @@ __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restri
                 // Only a leaf root (one per cloud in a batch) forms groups of
                 // its own; other leaves are grouped by their parent.
                 if (parent[id] < 0)
-                    for (int32_t c0 = 0; c0 < nd.b; c0 += 32) emit(nd.a + c0, min(32, nd.b - c0));
+                    for (int32_t c0 = 0; c0 < nd.b; c0 += gmax) emit(nd.a + c0, min(gmax, nd.b - c0));
             } else {
                 const int nc = __popc((unsigned)(-nd.b));
                 int32_t gfirst = 0, gcount = 0;
@@ -557,12 +558,12 @@ __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restri
                     if (c.b <= 0) {  // internal child: close the open group
                         if (gcount) emit(gfirst, gcount);
                         gcount = 0;
-                    } else if (c.b > 32) {
+                    } else if (c.b > gmax) {
                         if (gcount) emit(gfirst, gcount);
                         gcount = 0;
-                        for (int32_t c0 = 0; c0 < c.b; c0 += 32) emit(c.a + c0, min(32, c.b - c0));
+                        for (int32_t c0 = 0; c0 < c.b; c0 += gmax) emit(c.a + c0, min(gmax, c.b - c0));
                     } else {
-                        if (gcount + c.b > 32) {
+                        if (gcount + c.b > gmax) {
                             emit(gfirst, gcount);
                             gcount = 0;
                         }
@@ -1015,51 +1016,53 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
     const int32_t* perm;
     int sorted = -1;  // buffer holding this build's sorted keys and permutation
     if (moved == -1) {  // a full sort
-        // --- encode
+        // Keys and points sorted together (stable: ties keep ascending
+        // original index, src/sort.jl:15-24), the encode fused into the sort.
+        const int passes = t.sort_passes;
         if ((err = ensure_g(ctx, t.keys[0], (size_t)n * sizeof(K))) ||
             (err = ensure_g(ctx, t.keys[1], (size_t)n * sizeof(K))) || (err = ensure_g(ctx, t.vals[0], (size_t)n * 4)) ||
-            (err = ensure_g(ctx, t.vals[1], (size_t)n * 4)))
+            (err = ensure_g(ctx, t.spts, (size_t)n * sizeof(SPt<T, D>))) ||
+            (err = ensure_g(ctx, t.spts_tmp, (size_t)n * sizeof(SPt<T, D>))) ||
+            (err = ensure_g(ctx, t.iperm, (size_t)n * 4)) ||
+            (err = ensure(t.vals[1], (size_t)n * 4)))  // the next refit-mode merge writes here
             return cuda_status(ctx, err, "allocating sort buffers");
         for (int b = 0; b < 2; ++b)
-            if ((err = guard_fill(ctx, t.keys[b], (size_t)n * sizeof(K))) || (err = guard_fill(ctx, t.vals[b], (size_t)n * 4)))
-                return cuda_status(ctx, err, "sort buffer guards");
-        {
-            PhaseTimer pt_(ctx, PH_ENCODE);
+            if ((err = guard_fill(ctx, t.keys[b], (size_t)n * sizeof(K)))) return cuda_status(ctx, err, "sort guards");
+        if ((err = guard_fill(ctx, t.vals[0], (size_t)n * 4)) ||
+            (err = guard_fill(ctx, t.spts, (size_t)n * sizeof(SPt<T, D>))) ||
+            (err = guard_fill(ctx, t.spts_tmp, (size_t)n * sizeof(SPt<T, D>))) ||
+            (err = guard_fill(ctx, t.iperm, (size_t)n * 4)))
+            return cuda_status(ctx, err, "sort guards");
+        if (passes == 0) {
+            // Every point in one cell: keys all equal, the input order stands.
+            PhaseTimer pt_(ctx, PH_SORT);
             k_encode<T, D, K><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, n, o[0], o[1], o[2], inv_cs,
                                                                         t.keys[0].as<K>(), bt);
-            ctx.kernel_launches += 1;
-        }
-
-        // --- sort (stable: ties keep ascending original index, src/sort.jl:15-24)
-        K* kb[2] = {t.keys[0].as<K>(), t.keys[1].as<K>()};
-        int32_t* vb[2] = {t.vals[0].as<int32_t>(), t.vals[1].as<int32_t>()};
-        int src;
-        if (n < kOnesweepMaxKeys) {
-            if ((err = ensure(t.look, onesweep_words(n, (t.key_bits + 7) / 8) * 4)))
+            k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, nullptr, n, t.spts.as<SPt<T, D>>(),
+                                                                    t.iperm.as<int32_t>(), &hdr->status);
+            ctx.kernel_launches += 2;
+            perm = nullptr;
+        } else {
+            if ((err = ensure(t.look, onesweep_words(n, passes) * 4)))
                 return cuda_status(ctx, err, "allocating sort scratch");
             int sms = 0;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
+            EncodeParams<T> ep;
+            ep.o[0] = o[0];
+            ep.o[1] = o[1];
+            ep.o[2] = o[2];
+            ep.inv_cs = inv_cs;
+            ep.bt = bt;
             PhaseTimer pt_(ctx, PH_SORT);
-            src = onesweep_sort_pairs<K>(kb, vb, t.look.as<uint32_t>(), n, t.key_bits, false, &hdr->status, sms, s,
-                                         &ctx.kernel_launches, ctx.wait_limit, ctx.withhold_tile);
-        } else {
-            if ((err = ensure(t.hist, sort_hist_bytes(n))) || (err = ensure(t.sort_tmp, sort_scan_bytes(n))))
-                return cuda_status(ctx, err, "allocating histograms");
-            PhaseTimer pt_(ctx, PH_SORT);
-            src = radix_sort_pairs<K>(kb, vb, t.hist.as<int32_t>(), t.sort_tmp.as<int64_t>(), n, t.key_bits, false,
-                                      s, &ctx.kernel_launches);
+            err = point_sort<T, D, K>(coords, ep, n, passes, t.keys[0].as<K>(), t.keys[1].as<K>(),
+                                      t.spts.as<SPt<T, D>>(), t.spts_tmp.as<SPt<T, D>>(), t.vals[0].as<int32_t>(),
+                                      t.iperm.as<int32_t>(), t.look.as<uint32_t>(), &hdr->status, sms, ctx.wait_limit,
+                                      ctx.withhold_tile, s, &ctx.kernel_launches);
+            if (err) return cuda_status(ctx, err, "key sort launch");
+            perm = t.vals[0].as<int32_t>();
+            if (!bt.n_clouds) sorted = 0;
         }
-        skeys = kb[src];
-        perm = t.sort_passes ? vb[src] : nullptr;
-        if (perm && !bt.n_clouds) sorted = src;
-
-        // --- sorted points
-        {
-            PhaseTimer pt_(ctx, PH_GATHER);
-            k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, perm, n, t.spts.as<SPt<T, D>>(),
-                                                                    t.iperm.as<int32_t>(), &hdr->status);
-            ctx.kernel_launches += 1;
-        }
+        skeys = t.keys[0].as<K>();
         t.last_path = 0;
     } else {
         // Refit mode, keys already re-encoded in the previous order (section 10).
@@ -1145,10 +1148,13 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         t.capacity = ctx.node_cap_override;  // the first attempt's capacity, as set by the caller
     else if (t.capacity < est)
         t.capacity = est;
+    // Query points per traversal group (a tuned shape; 32 by default).
+    const int gmax = ctx.tuning_for(t.ndims, t.dtype, n, t.nbrs_hint).group_cap;
+    t.group_cap = gmax;
     for (int attempt = 0; attempt < 3; ++attempt) {
         ctx.last_attempts = attempt + 1;
         const int64_t cap = t.capacity;
-        const size_t gcap = (size_t)(cap + n / 32 + 2);
+        const size_t gcap = (size_t)(cap + n / gmax + 2);
         if ((err = ensure_g(ctx, t.tnode, (size_t)cap * sizeof(TNode<T, D>))) ||
             (err = ensure_g(ctx, t.nrange, (size_t)cap * 8)) || (err = ensure_g(ctx, t.parent, (size_t)cap * 4)) ||
             (err = ensure_g(ctx, t.arrive, (size_t)cap * 4)) || (err = ensure_g(ctx, t.fchild, (size_t)cap * 4)) ||
@@ -1189,9 +1195,9 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         {
             PhaseTimer pt_(ctx, PH_GROUPS);
             k_groups<T, D><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
-                                                                     t.groups.as<int2>(), cap + n / 32 + 2,
+                                                                     t.groups.as<int2>(), (int64_t)gcap,
                                                                      t.chain.as<int32_t>(), t.parent.as<int32_t>(),
-                                                                     hdr);
+                                                                     hdr, gmax);
             ctx.kernel_launches += 1;
             if (bt.n_clouds) {
                 k_cloud_start<T, D><<<div_up(bt.n_clouds, 128), 128, 0, s>>>(t.tnode.as<TNode<T, D>>(), bt, cap, hdr);
@@ -1205,11 +1211,13 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             guard_check(ctx, t.arrive, (size_t)cap * 4, hdr);
             guard_check(ctx, t.fchild, (size_t)cap * 4, hdr);
             guard_check(ctx, t.groups, gcap * 8, hdr);
-            if (moved == -1)
-                for (int b = 0; b < 2; ++b) {
-                    guard_check(ctx, t.keys[b], (size_t)n * sizeof(K), hdr);
-                    guard_check(ctx, t.vals[b], (size_t)n * 4, hdr);
-                }
+            if (moved == -1) {
+                for (int b = 0; b < 2; ++b) guard_check(ctx, t.keys[b], (size_t)n * sizeof(K), hdr);
+                guard_check(ctx, t.vals[0], (size_t)n * 4, hdr);
+                guard_check(ctx, t.spts, (size_t)n * sizeof(SPt<T, D>), hdr);
+                guard_check(ctx, t.spts_tmp, (size_t)n * sizeof(SPt<T, D>), hdr);
+                guard_check(ctx, t.iperm, (size_t)n * 4, hdr);
+            }
         }
         if ((err = cudaMemcpyAsync(t.hdr_host, hdr, sizeof(OctHeader), cudaMemcpyDeviceToHost, s)) ||
             (err = wait_stream(s)))

@@ -1,6 +1,7 @@
 // C ABI (include/octopus_b200.h): argument checks, object lifetime and error
 // reporting around the build / edge / adjoint pipelines.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -60,6 +61,86 @@ PhaseTimer::~PhaseTimer() {
     ctx->prof.push_back({phase, start, stop});
 }
 
+bool parse_tuning(const char* path, std::vector<TuneRow>& rows, std::string& err) {
+    rows.clear();
+    FILE* f = std::fopen(path, "r");
+    if (!f) {
+        err = std::string("cannot open tuning table ") + path;
+        return false;
+    }
+    char line[512];
+    int lineno = 0;
+    bool ok = true;
+    while (std::fgets(line, sizeof line, f)) {
+        ++lineno;
+        if (char* h = std::strchr(line, '#')) *h = '\0';
+        int v[9];
+        v[8] = 1;
+        char extra[2];
+        const int got = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %1s", &v[0], &v[1], &v[2], &v[3], &v[4],
+                                    &v[5], &v[6], &v[7], &v[8], extra);
+        if (got <= 0) continue;  // blank or comment
+        const bool valid = (got == 8 || got == 9) && (v[0] == 2 || v[0] == 3) && (v[1] == 0 || v[1] == 1) &&
+                           v[2] >= 0 && v[2] <= 40 && v[3] >= 0 && v[3] <= 40 && v[4] >= 1 && v[4] <= 16 &&
+                           v[5] >= 1 && v[5] <= 4 && (v[6] == 32 || v[6] == 64 || v[6] == 128) && v[7] >= 8 &&
+                           v[7] <= 32 && (v[8] == 1 || v[8] == 2 || v[8] == 4);
+        if (!valid) {
+            err = std::string("tuning table ") + path + ": bad row at line " + std::to_string(lineno);
+            ok = false;
+            break;
+        }
+        TuneRow r;
+        r.ndims = v[0];
+        r.dtype = v[1];
+        r.nlog2 = v[2];
+        r.nbr_log2 = v[3];
+        r.tn.max_seg = v[4];
+        r.tn.multi_pop = v[5];
+        r.tn.fill_chunk = v[6];
+        r.tn.group_cap = v[7];
+        r.tn.sub_boxes = v[8];
+        rows.push_back(r);
+    }
+    std::fclose(f);
+    if (!ok) rows.clear();
+    return ok;
+}
+
+int select_tuning(const std::vector<TuneRow>& rows, int ndims, int dtype, int64_t n, double nbrs, Tuning& out) {
+    out = Tuning{};
+    int nlog2 = 0;
+    while (nlog2 < 62 && (int64_t(1) << (nlog2 + 1)) <= n) ++nlog2;
+    // an unknown neighbor count (no count yet) keys as the mid bucket 4 (~15 per point)
+    int blog2 = 4;
+    if (nbrs >= 0.0) {
+        blog2 = 0;
+        while (blog2 < 40 && (double)(int64_t(1) << (blog2 + 1)) <= nbrs + 1.0) ++blog2;
+    }
+    int best = -1, best_d = 1 << 30;
+    for (size_t i = 0; i < rows.size(); ++i) {
+        const TuneRow& r = rows[i];
+        if (r.ndims != ndims || r.dtype != dtype) continue;
+        const int d = std::abs(r.nlog2 - nlog2) + 2 * std::abs(r.nbr_log2 - blog2);
+        if (d < best_d) {
+            best_d = d;
+            best = (int)i;
+        }
+    }
+    if (best >= 0) out = rows[(size_t)best].tn;
+    return best;
+}
+
+Tuning Ctx::tuning_for(int ndims, int dtype, int64_t n, double nbrs) {
+    Tuning tn;
+    last_tune_row = select_tuning(tune_table, ndims, dtype, n, nbrs, tn);
+    if (tune_force.max_seg) tn.max_seg = tune_force.max_seg;
+    if (tune_force.multi_pop) tn.multi_pop = tune_force.multi_pop;
+    if (tune_force.fill_chunk) tn.fill_chunk = tune_force.fill_chunk;
+    if (tune_force.group_cap) tn.group_cap = tune_force.group_cap;
+    if (tune_force.sub_boxes) tn.sub_boxes = tune_force.sub_boxes;
+    return tn;
+}
+
 int set_error(Ctx& ctx, int status, const std::string& msg) {
     ctx.last_error = msg;
     return status;
@@ -91,7 +172,7 @@ void release_tree(oct::Tree& t) {
     using oct::release;
     for (auto* b : {&t.b_coff, &t.b_cparam, &t.b_croot, &t.b_cstart, &t.b_cbounds, &t.b_eoff})
         release(*b);
-    for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.sort_tmp, &t.look, &t.spts, &t.tnode, &t.nrange,
+    for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.sort_tmp, &t.look, &t.spts, &t.spts_tmp, &t.tnode, &t.nrange,
                     &t.parent, &t.fchild, &t.arrive, &t.groups, &t.chain, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
                     &t.morton, &t.v_first, &t.v_last, &t.v_children, &t.v_bmin, &t.v_bmax, &t.v_perm, &t.iperm,
                     &t.rflag, &t.rcnt, &t.roff, &t.mkeys, &t.mvals, &t.mkeys2, &t.mvals2})
@@ -145,7 +226,7 @@ OCT_API int oct_ctx_destroy(oct_ctx* ctx) {
     using oct::release;
     for (auto* b : {&ctx->c.counts, &ctx->c.offsets, &ctx->c.scan_tmp, &ctx->c.total, &ctx->c.dkeys[0],
                     &ctx->c.dkeys[1], &ctx->c.dvals[0], &ctx->c.dvals[1], &ctx->c.dhist, &ctx->c.dsort_tmp, &ctx->c.droff,
-                    &ctx->c.dsoff, &ctx->c.dstatus, &ctx->c.dredge, &ctx->c.dterm, &ctx->c.dseg, &ctx->c.recs, &ctx->c.rcount, &ctx->c.gflag})
+                    &ctx->c.dsoff, &ctx->c.dstatus, &ctx->c.dredge, &ctx->c.dterm, &ctx->c.dseg, &ctx->c.tstats, &ctx->c.recs, &ctx->c.rcount, &ctx->c.gflag})
         release(*b);
     if (ctx->c.total_host) cudaFreeHost(ctx->c.total_host);
     for (auto& r : ctx->c.prof) {
@@ -316,6 +397,16 @@ OCT_API int oct_edges_count(oct_ctx* ctx, const oct_tree* query, const oct_tree*
     return oct::edges_count(ctx->c, query->t, target->t, exclude_self != 0, n_edges);
 }
 
+OCT_API int oct_edges_traversal_stats(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
+                                      uint64_t* stats, int n_stats) {
+    if (!ctx || !stats || n_stats < 0) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    const int st = oct_check_count_pair(ctx, query, target, exclude_self);
+    if (st != OCT_OK) return st;
+    DeviceGuard g(ctx->c.device);
+    return oct::traversal_stats(ctx->c, query->t, target->t, exclude_self != 0, stats, n_stats);
+}
+
 OCT_API int oct_edges_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
                            int32_t* senders, int32_t* receivers, void* rel_displacement, void* rel_dist_norm,
                            int64_t capacity) {
@@ -328,6 +419,19 @@ OCT_API int oct_edges_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* 
     DeviceGuard g(ctx->c.device);
     return oct::edges_fill(ctx->c, query->t, target->t, exclude_self != 0, senders, receivers, rel_displacement,
                            rel_dist_norm, capacity);
+}
+
+OCT_API int oct_edges_fill_diff(oct_ctx* ctx, const oct_tree* tree, int32_t* senders, int32_t* receivers,
+                                void* rel_displacement, void* rel_dist_norm, int32_t* mirror, int64_t capacity) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    int st = check_pair(ctx, tree, tree);
+    if (st != OCT_OK) return st;
+    if (capacity > 0 && (!senders || !receivers || !rel_displacement || !rel_dist_norm || !mirror))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge output buffer is NULL");
+    DeviceGuard g(ctx->c.device);
+    return oct::edges_fill_diff(ctx->c, tree->t, senders, receivers, rel_displacement, rel_dist_norm, mirror,
+                                capacity);
 }
 
 OCT_API int oct_csr_fill(oct_ctx* ctx, const oct_tree* query, const oct_tree* target, int exclude_self,
@@ -348,6 +452,14 @@ OCT_API int oct_zsort_apply(oct_ctx* ctx, const oct_tree* tree, const void* in, 
     ctx->c.last_error.clear();
     DeviceGuard g(ctx->c.device);
     return oct::zsort_apply(ctx->c, tree->t, in, out, n, row_bytes, direction);
+}
+
+OCT_API int oct_permute_rows(oct_ctx* ctx, const int32_t* perm, int64_t n, const void* in, void* out,
+                             int64_t row_bytes, int direction) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    DeviceGuard g(ctx->c.device);
+    return oct::permute_rows(ctx->c, perm, n, in, out, row_bytes, direction);
 }
 
 OCT_API int oct_neighbors(oct_ctx* ctx, const oct_tree* target, const void* query_coords, int64_t n_queries,
@@ -472,6 +584,29 @@ OCT_API int oct_ctx_set_option(oct_ctx* ctx, int option, int64_t value) {
                 return oct::set_error(c, OCT_ERR_ARGUMENT, "withheld tile must be -1 or a tile index");
             c.withhold_tile = (int32_t)value;
             return OCT_OK;
+        case OCT_OPT_MAX_SEG:
+            if (value < 0 || value > 16) return oct::set_error(c, OCT_ERR_ARGUMENT, "max_seg must be in [0, 16]");
+            c.tune_force.max_seg = (int)value;
+            return OCT_OK;
+        case OCT_OPT_MULTI_POP:
+            if (value < 0 || value > 4) return oct::set_error(c, OCT_ERR_ARGUMENT, "multi_pop must be in [0, 4]");
+            c.tune_force.multi_pop = (int)value;
+            return OCT_OK;
+        case OCT_OPT_FILL_CHUNK:
+            if (value != 0 && value != 32 && value != 64 && value != 128)
+                return oct::set_error(c, OCT_ERR_ARGUMENT, "fill_chunk must be 0, 32, 64 or 128");
+            c.tune_force.fill_chunk = (int)value;
+            return OCT_OK;
+        case OCT_OPT_GROUP_CAP:
+            if (value != 0 && (value < 8 || value > 32))
+                return oct::set_error(c, OCT_ERR_ARGUMENT, "group_cap must be 0 or in [8, 32]");
+            c.tune_force.group_cap = (int)value;
+            return OCT_OK;
+        case OCT_OPT_SUB_BOXES:
+            if (value != 0 && value != 1 && value != 2 && value != 4)
+                return oct::set_error(c, OCT_ERR_ARGUMENT, "sub_boxes must be 0, 1, 2 or 4");
+            c.tune_force.sub_boxes = (int)value;
+            return OCT_OK;
         default:
             return oct::set_error(c, OCT_ERR_ARGUMENT, "unknown or read-only option");
     }
@@ -486,11 +621,70 @@ OCT_API int oct_ctx_get_option(const oct_ctx* ctx, int option, int64_t* value) {
         case OCT_OPT_RECORD_CAP: *value = c.rec_cap_override; return OCT_OK;
         case OCT_OPT_GUARD_CHECK: *value = c.guard_check ? 1 : 0; return OCT_OK;
         case OCT_OPT_WITHHOLD_TILE: *value = c.withhold_tile; return OCT_OK;
+        case OCT_OPT_MAX_SEG: *value = c.tune_force.max_seg; return OCT_OK;
+        case OCT_OPT_MULTI_POP: *value = c.tune_force.multi_pop; return OCT_OK;
+        case OCT_OPT_FILL_CHUNK: *value = c.tune_force.fill_chunk; return OCT_OK;
+        case OCT_OPT_GROUP_CAP: *value = c.tune_force.group_cap; return OCT_OK;
+        case OCT_OPT_SUB_BOXES: *value = c.tune_force.sub_boxes; return OCT_OK;
+        case OCT_STAT_TUNING_ROW: *value = c.last_tune_row; return OCT_OK;
         case OCT_STAT_BUILD_ATTEMPTS: *value = c.last_attempts; return OCT_OK;
         case OCT_STAT_RECORD_OVERFLOW: *value = c.rec_overflow; return OCT_OK;
         case OCT_STAT_RECORD_CAP: *value = c.rec_cap; return OCT_OK;
         default: return OCT_ERR_ARGUMENT;
     }
+}
+
+OCT_API int oct_ctx_load_tuning(oct_ctx* ctx, const char* path) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (!path || !*path) {
+        ctx->c.tune_table.clear();
+        return OCT_OK;
+    }
+    std::vector<oct::TuneRow> rows;
+    std::string err;
+    if (!oct::parse_tuning(path, rows, err)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, err);
+    ctx->c.tune_table.swap(rows);
+    return OCT_OK;
+}
+
+OCT_API int oct_tuning_select(const char* path, int ndims, int dtype, int64_t n, double nbrs_per_point,
+                              int32_t* shapes, int32_t* row) {
+    if (!path || !shapes || !row) return OCT_ERR_ARGUMENT;
+    std::vector<oct::TuneRow> rows;
+    std::string err;
+    if (*path && !oct::parse_tuning(path, rows, err)) return OCT_ERR_ARGUMENT;
+    oct::Tuning tn;
+    *row = oct::select_tuning(rows, ndims, dtype, n, nbrs_per_point, tn);
+    shapes[0] = tn.max_seg;
+    shapes[1] = tn.multi_pop;
+    shapes[2] = tn.fill_chunk;
+    shapes[3] = tn.group_cap;
+    shapes[4] = tn.sub_boxes;
+    return OCT_OK;
+}
+
+OCT_API int oct_edges_diff_backward_mirror(oct_ctx* ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,
+                                           const int32_t* senders, const int32_t* receivers, const int32_t* mirror,
+                                           const void* rel_displacement, const void* rel_dist_norm,
+                                           const void* coords, const void* d_rel_displacement,
+                                           const void* d_rel_dist_norm, double radius, void* grad_coords,
+                                           const int32_t* order) {
+    if (!ctx) return OCT_ERR_ARGUMENT;
+    ctx->c.last_error.clear();
+    if (bad_dims(ndims) || bad_dtype(dtype)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "bad ndims/dtype");
+    if (n_points < 0 || n_edges < 0 || n_edges > 2147483647LL || n_points > 2147483647LL)
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "sizes must fit Int32");
+    if (!(radius > 0.0)) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "radius must be positive");
+    if (n_points > 0 && !grad_coords) return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "grad_coords is NULL");
+    if (n_edges > 0 && (!senders || !receivers || !mirror))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "edge array is NULL");
+    if (n_points > 0 && !coords && n_edges > 0 && (!rel_displacement || !rel_dist_norm))
+        return oct::set_error(ctx->c, OCT_ERR_ARGUMENT, "give either the features or coords");
+    DeviceGuard g(ctx->c.device);
+    return oct::diff_backward_mirror(ctx->c, ndims, dtype, n_points, n_edges, senders, receivers, mirror,
+                                     coords ? nullptr : rel_displacement, coords ? nullptr : rel_dist_norm, coords,
+                                     d_rel_displacement, d_rel_dist_norm, radius, grad_coords, order);
 }
 
 static const char* kPhaseNames[oct::PH_NUM] = {"bounds", "encode", "sort", "gather", "topology",

@@ -336,6 +336,149 @@ __global__ void __launch_bounds__(kTwinWarps * 32) k_adjoint_twins(
     if (bad) atomicOr(status, bad);
 }
 
+// Self-pair adjoint in one pass, from the mirror index of every edge that the
+// differentiable fill writes (oct_edges_fill_diff): edge k = (i <- j) and its
+// mirror t = (j <- i).  The mirror's features are exactly the edge's own with
+// rel_displacement negated (x_j - x_i is the exact negation of x_i - x_j, and
+// the squares and the distance are the same), so term(t) is formed from the
+// mirror's cotangents and the edge's own features, bit for bit what the
+// mirror's stored features give.  Same warp layout, arithmetic and summation
+// order as k_edge_terms + k_adjoint_twins, without the per-edge term buffer
+// and the mirror search.  A mirror index outside 0..m-1 sets kAdjMissingTwin.
+template <class T, int D, bool RECOMPUTE>
+__device__ __forceinline__ Term4<T> mirror_term(const T* rd, T rn, const T* __restrict__ d_disp,
+                                                 const T* __restrict__ d_dist, int64_t e, T r, T sign) {
+    Term4<T> o;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) o.v[d] = T(0);
+    if (d_disp) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) o.v[d] = div_rn(d_disp[(int64_t)D * e + d], r);
+    }
+    if (d_dist && rn > T(1e-8)) {
+        const T a = div_rn(d_dist[e], mul_rn(rn, r));
+#pragma unroll
+        for (int d = 0; d < D; ++d) o.v[d] = add_rn(o.v[d], mul_rn(sign * rd[d], a));
+    }
+    return o;
+}
+
+template <class T, int D, bool RECOMPUTE>
+__global__ void __launch_bounds__(kTwinWarps * 32) k_adjoint_mirror(
+    int64_t n, int64_t m, const int32_t* __restrict__ order, const int2* __restrict__ seg,
+    const int32_t* __restrict__ snd, const int32_t* __restrict__ rcv, const int32_t* __restrict__ mirror,
+    const T* __restrict__ rel_disp, const T* __restrict__ rel_dist, const T* __restrict__ coords,
+    const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r, T inv_r, T* __restrict__ grad,
+    int* __restrict__ status) {
+    __shared__ double snet[kTwinWarps][3][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t s0 = ((int64_t)blockIdx.x * kTwinWarps + w) * kTwinPoints;
+    if (s0 >= n) return;  // warp-uniform
+    const int64_t sl = s0 + lane;
+    int p = -1, k0 = 0, ne = 0;
+    int bad = 0;
+    if (lane < kTwinPoints && sl < n) {
+        const int64_t pp = order ? (int64_t)order[sl] - 1 : sl;
+        if (pp < 0 || pp >= n) {
+            bad |= kAdjBadOrder;
+        } else {
+            p = (int)pp;
+            const int2 sg = seg[p];
+            k0 = sg.x;
+            ne = sg.y - sg.x;
+            if (ne < 0 || (p == 0 && k0 != 0) || (p == n - 1 && sg.y != m)) {
+                bad |= kAdjUngrouped;
+                ne = 0;
+            }
+        }
+    }
+    int incl = ne;
+#pragma unroll
+    for (int o = 1; o < kTwinPoints; o <<= 1) {
+        const int a = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += a;
+    }
+    const int excl = incl - ne;
+    const int total = __shfl_sync(0xffffffffu, incl, kTwinPoints - 1);
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int f0 = 0; f0 < total; f0 += 32) {
+        const int f = f0 + lane;
+        int o = 0;
+#pragma unroll
+        for (int st = kTwinPoints / 2; st; st >>= 1) {
+            const int v = __shfl_sync(0xffffffffu, incl, o + st - 1);
+            if (v <= f) o += st;
+        }
+        const int ko = __shfl_sync(0xffffffffu, k0, o);
+        const int eo = __shfl_sync(0xffffffffu, excl, o);
+        const int po = __shfl_sync(0xffffffffu, p, o);
+        double net[3] = {0.0, 0.0, 0.0};
+        if (f < total) {
+            const int32_t k = ko + (f - eo);
+            if (rcv[k] != po + 1) bad |= kAdjUngrouped;
+            const int32_t t = mirror[k];
+            T rd[D], rn = T(0);
+            bool ok = t >= 0 && (int64_t)t < m;
+            if (!ok) bad |= kAdjMissingTwin;
+            if (RECOMPUTE) {
+                const int32_t j = snd[k] - 1;
+                if (j < 0 || j >= n) {
+                    bad |= kAdjBadIndex;
+                    ok = false;
+                } else {
+                    T diff[D];
+                    const T d2 = dist2<T, D>(coords + (int64_t)D * j, coords + (int64_t)D * po, diff);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) rd[d] = mul_rn(-diff[d], inv_r);
+                    rn = mul_rn(sqrt_rn(d2), inv_r);
+                }
+            } else {
+#pragma unroll
+                for (int d = 0; d < D; ++d) rd[d] = rel_disp[(int64_t)D * k + d];
+                rn = rel_dist[k];
+            }
+            if (ok) {
+                const Term4<T> tk = mirror_term<T, D, RECOMPUTE>(rd, rn, d_disp, d_dist, k, r, T(1));
+                const Term4<T> tt = mirror_term<T, D, RECOMPUTE>(rd, rn, d_disp, d_dist, t, r, T(-1));
+#pragma unroll
+                for (int d = 0; d < 3; ++d) net[d] = (double)tk.v[d] - (double)tt.v[d];
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) snet[w][d][lane] = net[d];
+        __syncwarp();
+        const int e1 = min(incl, f0 + 32);
+        for (int e = max(excl, f0); e < e1; ++e) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) acc[d] += snet[w][d][e - f0];
+        }
+        __syncwarp();
+    }
+    if (p >= 0) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) grad[(int64_t)D * p + d] = (T)acc[d];
+    }
+    if (bad) atomicOr(status, bad);
+}
+
+// Mirror index of every edge of a self-pair COO grouped by receiver, by
+// scanning the sender's segment (off: int64 segment starts) -- for the
+// differentiable fill when the hit records were incomplete.  -1 when absent.
+__global__ void k_mirror_scan(const int32_t* __restrict__ snd, const int32_t* __restrict__ rcv, int64_t m, int64_t n,
+                              const int64_t* __restrict__ off, int32_t* __restrict__ mirror) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const int32_t i1 = rcv[k], j = snd[k] - 1;
+    int32_t t = -1;
+    if (j >= 0 && j < n)
+        for (int64_t q = off[j]; q < off[j + 1]; ++q)
+            if (snd[q] == i1) {
+                t = (int32_t)q;
+                break;
+            }
+    mirror[k] = t;
+}
+
 namespace {
 
 // Word 1 of the status buffer (word 0 belongs to the edge fill guard).
@@ -530,6 +673,74 @@ int diff_backward_pair(Ctx& ctx, int ndims, int dtype, int64_t nq, int64_t nt, i
                                                        radius, grad_q, grad_t)
                       : backward_pair_typed<double, 2>(ctx, nq, nt, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist,
                                                        radius, grad_q, grad_t);
+}
+
+namespace {
+
+template <class T, int D>
+int mirror_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_t* rcv, const int32_t* mirror,
+                 const void* rel_disp, const void* rel_dist, const void* coords, const void* d_disp,
+                 const void* d_dist, double radius, void* grad, const int32_t* order, int* flags) {
+    cudaStream_t s = ctx.stream;
+    cudaError_t err;
+    const T r = (T)radius;
+    const T inv_r = T(1) / r;
+    if ((err = ensure(ctx.droff, (n + 1) * 8)) || (err = ensure(ctx.dstatus, 8)) || (err = ensure(ctx.dseg, n * 8)))
+        return cuda_status(ctx, err, "allocating adjoint scratch");
+    const int tb = 256;
+    PhaseTimer pt_(ctx, PH_ADJOINT);
+    int* status = adjoint_status(ctx);
+    if ((err = cudaMemsetAsync(status, 0, 4, s))) return cuda_status(ctx, err, "status reset");
+    k_segment_starts<<<div_up(n + 1, tb), tb, 0, s>>>(rcv, m, n, ctx.droff.as<int64_t>());
+    k_seg_pairs<<<div_up(n, tb), tb, 0, s>>>(ctx.droff.as<int64_t>(), n, ctx.dseg.as<int2>());
+    const unsigned blocks = (unsigned)div_up(n, kTwinPoints * kTwinWarps);
+    if (coords)
+        k_adjoint_mirror<T, D, true><<<blocks, 32 * kTwinWarps, 0, s>>>(
+            n, m, order, ctx.dseg.as<int2>(), snd, rcv, mirror, nullptr, nullptr, (const T*)coords, (const T*)d_disp,
+            (const T*)d_dist, r, inv_r, (T*)grad, status);
+    else
+        k_adjoint_mirror<T, D, false><<<blocks, 32 * kTwinWarps, 0, s>>>(
+            n, m, order, ctx.dseg.as<int2>(), snd, rcv, mirror, (const T*)rel_disp, (const T*)rel_dist, nullptr,
+            (const T*)d_disp, (const T*)d_dist, r, inv_r, (T*)grad, status);
+    ctx.kernel_launches += 3;
+    if ((err = cudaGetLastError())) return cuda_status(ctx, err, "adjoint launch");
+    return read_status(ctx, flags);
+}
+
+}  // namespace
+
+int edges_mirror_scan(Ctx& ctx, const int32_t* snd, const int32_t* rcv, int64_t m, int64_t n, const int64_t* off,
+                      int32_t* mirror) {
+    if (m == 0) return OK;
+    k_mirror_scan<<<div_up(m, 256), 256, 0, ctx.stream>>>(snd, rcv, m, n, off, mirror);
+    ctx.kernel_launches += 1;
+    return cuda_status(ctx, cudaGetLastError(), "mirror scan launch");
+}
+
+int diff_backward_mirror(Ctx& ctx, int ndims, int dtype, int64_t n, int64_t m, const int32_t* snd,
+                         const int32_t* rcv, const int32_t* mirror, const void* rel_disp, const void* rel_dist,
+                         const void* coords, const void* d_disp, const void* d_dist, double radius, void* grad,
+                         const int32_t* order) {
+    if (n == 0) return OK;
+    if (m > 0 && (d_disp || d_dist)) {
+        int flags = 0, st;
+        if (dtype == 0)
+            st = ndims == 3 ? mirror_typed<float, 3>(ctx, n, m, snd, rcv, mirror, rel_disp, rel_dist, coords, d_disp,
+                                                     d_dist, radius, grad, order, &flags)
+                            : mirror_typed<float, 2>(ctx, n, m, snd, rcv, mirror, rel_disp, rel_dist, coords, d_disp,
+                                                     d_dist, radius, grad, order, &flags);
+        else
+            st = ndims == 3 ? mirror_typed<double, 3>(ctx, n, m, snd, rcv, mirror, rel_disp, rel_dist, coords, d_disp,
+                                                      d_dist, radius, grad, order, &flags)
+                            : mirror_typed<double, 2>(ctx, n, m, snd, rcv, mirror, rel_disp, rel_dist, coords, d_disp,
+                                                      d_dist, radius, grad, order, &flags);
+        if (st != OK || flags == 0) return st;
+        if (flags & kAdjBadOrder) return bad_coo(ctx, flags);
+        // A mirror index that does not fit, or a COO not grouped by receiver:
+        // the general path checks and handles the COO from scratch.
+    }
+    return diff_backward(ctx, ndims, dtype, n, m, snd, rcv, rel_disp, rel_dist, d_disp, d_dist, radius, grad, coords,
+                         order);
 }
 
 int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n, int64_t m, const int32_t* snd, const int32_t* rcv,

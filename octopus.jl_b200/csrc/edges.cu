@@ -33,15 +33,33 @@ namespace oct {
 constexpr int kEdgeWarps = 4;
 constexpr int kEdgeThreads = kEdgeWarps * 32;
 constexpr int kStage = 32;  // staged hits per lane, and points per leaf sub-chunk
-constexpr int kMultiPop = 4;     // internal nodes expanded together
+constexpr int kMultiPop = 4;     // most internal nodes expanded together (the tuned multi_pop is <= this)
 constexpr int kMultiLimit = 64;  // stack depth up to which they are
-constexpr int kMaxSeg = 16;  // leaves sharing one chunk
+constexpr int kMaxSeg = 16;      // most leaves sharing one chunk (the tuned max_seg is <= this)
 
 // The three passes of k_edges.
 enum EdgePass {
     EP_COUNT = 0,   // per-query neighbor counts only
     EP_RECORD = 1,  // counts, plus each query's hit records (up to rec_cap of them)
     EP_FILL = 2,    // the COO at the scanned offsets by a second walk (groups whose records overflowed)
+    EP_STATS = 3,   // the count pass with traversal statistics (a diagnostic, oct_edges_traversal_stats)
+};
+
+// Traversal statistics of EP_STATS, summed over the launch.
+enum TraversalStat {
+    TS_GROUPS = 0,     // query groups (warps)
+    TS_QUERIES,        // query points
+    TS_EXPANSIONS,     // internal-node expansion rounds
+    TS_CHILDREN,       // child boxes tested
+    TS_CHUNKS,         // leaf chunks staged
+    TS_TARGETS,        // target points staged
+    TS_STEPS,          // pair-loop steps executed (four targets each)
+    TS_PAIR_TESTS,     // query-target distance tests issued (steps x 4 x queries of the group)
+    TS_HITS,           // pairs within the radius (self pair excluded when asked)
+    TS_CYCLES_TOTAL,   // SM cycles of the warps, summed
+    TS_CYCLES_LEAF,    // ... of which in leaf chunks (staging and pair tests)
+    TS_CYCLES_PAIRS,   // ... of which in the pair loop
+    TS_NUM
 };
 
 // A hit record: the sorted position of a leaf's first point (of a leaf's
@@ -95,8 +113,13 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     const SPt<T, D>* __restrict__ tpts, int64_t n_tnodes, T r2, T inv_r, int exclude_self,
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ ocount,
-    int2* __restrict__ recs, int64_t rec_cap, uint16_t* __restrict__ rcount, uint8_t* __restrict__ gflag, Batch bt) {
+    int2* __restrict__ recs, int64_t rec_cap, uint16_t* __restrict__ rcount, uint8_t* __restrict__ gflag, Batch bt,
+    unsigned long long* __restrict__ stats, int max_seg, int multi_pop, int nbox) {
     constexpr bool STAGE = PASS == EP_FILL;
+    constexpr bool STATS = PASS == EP_STATS;
+    long long st_t0 = 0, st_leaf = 0, st_pairs = 0;
+    unsigned long long st_exp = 0, st_children = 0, st_chunks = 0, st_targets = 0, st_steps = 0;
+    if constexpr (STATS) st_t0 = clock64();
     // The usual DFS bound, plus the room the multi-node expansions may take.
     constexpr int SD = stack_depth<D>() + kMultiLimit + 8;
     // Stack entries are the pushed node's (a, b) record; bit 31 of a marks
@@ -113,6 +136,9 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     __shared__ __align__(16) T sx[kEdgeWarps][D][32];
     __shared__ int2 sseg[kEdgeWarps][kMaxSeg + 1];
     __shared__ int sself[kEdgeWarps][32];
+    // The boxes of the group's nbox runs of 32 / nbox consecutive queries
+    // (lo then hi per box): a target is tested only if it is within r of one.
+    __shared__ T sbox[kEdgeWarps][4][2 * D];
     // Fill pass: each lane stages the sorted positions of its next hits; a
     // flush writes them as runs of consecutive edges of one query.
     __shared__ int32_t obuf[STAGE ? kEdgeWarps : 1][32][STAGE ? kStage + 1 : 1];
@@ -133,6 +159,24 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     for (int d = 0; d < D; ++d) {
         qlo[d] = warp_min(q.x[d]);
         qhi[d] = warp_max(q.x[d]);
+    }
+    if (nbox > 1) {
+        // sub-boxes over runs of 16 (nbox 2) or 8 (nbox 4) lanes; a lane
+        // past the group's end holds the group's first point, inside the box
+        const int width = 32 / nbox;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            T lo = q.x[d], hi = q.x[d];
+            for (int o = width >> 1; o > 0; o >>= 1) {
+                lo = jl_min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = jl_max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+            }
+            if ((lane & (width - 1)) == 0) {
+                sbox[w][lane / width][d] = lo;
+                sbox[w][lane / width][D + d] = hi;
+            }
+        }
+        __syncwarp();
     }
     int64_t cnt = 0;
     int64_t cur = 0, cur_end = 0;
@@ -200,12 +244,14 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             // share one chunk of at most kStage points as consecutive
             // segments; a leaf of more than kStage points is cut into chunks.
             for (int32_t c0 = 0; c0 < nb; c0 += kStage) {
+                long long st_c0 = 0;
+                if constexpr (STATS) st_c0 = clock64();
                 __syncwarp();  // every lane is done with the previous chunk's segment table
                 int total = min(kStage, nb - c0);
                 int nseg = 1;
                 if (lane == 0) sseg[w][0] = make_int2(na + c0, 0);
                 if (nb <= kStage) {
-                    while (sp > 0 && nseg < kMaxSeg) {
+                    while (sp > 0 && nseg < max_seg) {
                         const int2 nx = stack[w][sp - 1];
                         if (nx.y <= 0 || total + nx.y > kStage) break;
                         --sp;
@@ -229,7 +275,12 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                     const SPt<T, D> t = tpts[pos];
 #pragma unroll
                     for (int d = 0; d < D; ++d) sx[w][d][lane] = t.x[d];
-                    near = box_gap2<T, D>(qlo, qhi, t.x, t.x) <= r2;
+                    if (nbox == 1) {
+                        near = box_gap2<T, D>(qlo, qhi, t.x, t.x) <= r2;
+                    } else {
+                        for (int b = 0; b < nbox && !near; ++b)
+                            near = box_gap2<T, D>(&sbox[w][b][0], &sbox[w][b][D], t.x, t.x) <= r2;
+                    }
                     if (self_pair) {  // query and target are the same tree: the group's own points
                         const int64_t sl = pos - grp.x;
                         if (sl >= 0 && sl < grp.y) sself[w][sl] = (chunk << 5) | lane;
@@ -241,6 +292,15 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 const unsigned keep = __ballot_sync(0xffffffffu, near);
                 __syncwarp();
                 unsigned hm = 0;
+                long long st_p0 = 0;
+                if constexpr (STATS) {
+                    st_p0 = clock64();
+                    ++st_chunks;
+                    st_targets += total;
+                    st_steps += std::is_same<T, float>::value
+                                    ? __popc((keep | keep >> 1 | keep >> 2 | keep >> 3) & 0x11111111u)
+                                    : __popc(keep);
+                }
                 if constexpr (std::is_same<T, float>::value) {
                     unsigned long long P[D];
 #pragma unroll
@@ -277,6 +337,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                         hm |= (dist2<T, D>(t, q.x, diff) <= r2 ? 1u : 0u) << j;
                     }
                 }
+                if constexpr (STATS) st_pairs += clock64() - st_p0;
                 if (!valid) hm = 0;
                 if (self_pair) {
                     const int v = sself[w][lane];
@@ -308,6 +369,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                         }
                     }
                 }
+                if constexpr (STATS) st_leaf += clock64() - st_c0;
             }
         } else {
             // Internal nodes.  The popped node and up to kMultiPop - 1 further
@@ -326,7 +388,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 snode[w][0] = ent;
                 soff[w][0] = 0;
             }
-            while (nnodes < kMultiPop && sp > 0) {
+            while (nnodes < multi_pop && sp > 0) {
                 const int2 nx = stack[w][sp - 1];
                 if (nx.y > 0) break;
                 const int c = __popc((unsigned)(-nx.y));
@@ -340,6 +402,10 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 ++nnodes;
             }
             if (lane == 0) soff[w][nnodes] = totc;
+            if constexpr (STATS) {
+                ++st_exp;
+                st_children += totc;
+            }
             __syncwarp();
             int j = 0;
             if (lane < totc)
@@ -370,6 +436,18 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     }
     if (STAGE) flush(true);
     if (PASS != EP_FILL && valid) counts[q.idx] = (int32_t)cnt;
+    if constexpr (STATS) {
+        const unsigned long long hits = warp_sum((unsigned long long)cnt);
+        const int nv = __popc(__ballot_sync(0xffffffffu, valid));
+        if (lane == 0) {
+            const unsigned long long v[TS_NUM] = {1ull, (unsigned long long)nv, st_exp, st_children, st_chunks,
+                                                  st_targets, st_steps, 4ull * st_steps * (unsigned long long)nv, hits,
+                                                  (unsigned long long)(clock64() - st_t0), (unsigned long long)st_leaf,
+                                                  (unsigned long long)st_pairs};
+#pragma unroll
+            for (int k = 0; k < TS_NUM; ++k) atomicAdd(stats + k, v[k]);
+        }
+    }
     if (PASS == EP_RECORD) {
         const bool over = __any_sync(0xffffffffu, nrec > cap);
         if (valid) rcount[qpos] = over ? kOverflowMark : (uint16_t)nrec;
@@ -385,183 +463,272 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     }
 }
 
-// Fill pass from the records, in original index order: warp v writes the
-// edges of queries 32v .. 32v+31, which the COO stores contiguously, so its
-// stores cover whole sectors.  The warp's edges form one flat list, query
-// ql's first at flat index epre(ql), COO slot kq[ql] + flat index.  Records are expanded into shared memory
-// (lanes over consecutive records, each record's first hit at the running sum
-// of the hit counts before it), then each batch of flat edges is written with
-// lanes on consecutive edges.  Queries of an overflowed group (record count
-// kOverflowMark) are left to the walking fill.
-constexpr int kExpandWarps = 4;
-constexpr int kExpandCap = 512;  // staged positions per warp (at least 32: one record)
+// Fill pass from the records, in original index order.  Warp v writes the
+// edges of queries 32v .. 32v+31, which own one contiguous range [K0, K1) of
+// the COO.  The warp takes its queries one at a time, lanes over the query's
+// edges: a round of up to 32 records is loaded (one per lane) and scanned by
+// hit count, and each lane finds its edge's record by a binary search over the
+// scanned counts (shuffles) and its point as the k-th set bit of the record's
+// mask.  The query's coordinates, index and radius are warp-uniform.
+//
+// Output goes through a per-warp ring of NCH chunks of CHUNK edges in shared
+// memory, one array per COO array, in the COO's own layout; a completed chunk
+// is written to global memory by 1-D bulk copies (cp.async.bulk, issued by
+// lane 0), so the stores leave the load/store pipe.  Ring slot s holds COO
+// edge k with s = (k - base) mod RING, base = K0 rounded down to a multiple of
+// 4: a bulk copy starts at an edge index that is a multiple of 4, which makes
+// every source and destination address a multiple of 16 bytes (4-byte and
+// 8-byte elements, D values per edge for rel_displacement) given 16-byte
+// aligned output arrays, and every size a multiple of 16.  The at most three
+// edges at each end of the warp's range that do not fill an aligned group of
+// four are stored by lanes.  A warp with a query whose records overflowed
+// (left to the walking fill), or with unaligned outputs, stores every edge
+// from registers instead.
+constexpr int kFillWarps = 4;
 
-template <class T, int D>
-struct ExpandSmem {
-    int32_t pos[kExpandCap];
-    uint8_t who[kExpandCap];  // query (lane) of each staged position
-    long long kq[32];    // COO slot of each query's flat edge 0: first slot - epre
-    long long key[32];   // COO slot of each entry of a write batch
-    T qx[D][32];
-    T disp[D * 32];
-    T inv_r[32];
-    int32_t qpos[32];    // sorted position of each query
-    int32_t qi[32];      // 1-based receiver index of each query
-    int32_t base[32];    // index base of each query's point set
-    int32_t rpre[33];    // flat record index where each query starts
-};
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(s), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Orders this thread's shared-memory writes before later bulk-copy reads.
+__device__ __forceinline__ void fence_smem_to_bulk() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-template <class T, int D>
-__global__ void __launch_bounds__(kExpandWarps * 32, 8) k_expand(
+// Position (0..31) of the k-th set bit (k from 0) of m; k < popc(m).
+__device__ __forceinline__ int kth_set_bit(unsigned m, int k) {
+    int pos = 0;
+    int c = __popc(m & 0xffffu);
+    if (k >= c) { k -= c; m >>= 16; pos += 16; }
+    c = __popc(m & 0xffu);
+    if (k >= c) { k -= c; m >>= 8; pos += 8; }
+    c = __popc(m & 0xfu);
+    if (k >= c) { k -= c; m >>= 4; pos += 4; }
+    c = __popc(m & 0x3u);
+    if (k >= c) { k -= c; m >>= 2; pos += 2; }
+    if (k >= (int)(m & 1u)) pos += 1;
+    return pos;
+}
+
+// Shared-memory bytes of one warp's ring of `ring` edges.
+template <class T, int D, bool FEAT, bool TWIN>
+__host__ __device__ constexpr size_t fill_ring_bytes(int ring) {
+    return (FEAT ? (size_t)ring * (8 + (D + 1) * sizeof(T)) : (size_t)ring * 4) + (TWIN ? (size_t)ring * 4 : 0);
+}
+
+// TWIN (a self pair whose records are complete): also writes, for every edge
+// k = (i <- j), the index of its mirror (j <- i) in the COO: j's first edge
+// plus the number of j's hits before i, counted over j's records in order.
+// A mirror not found there (only for a COO that is not a self pair) is
+// written as -1 and sets bit 2 of *status.
+template <class T, int D, bool FEAT, bool TWIN, int CHUNK, int NCH>
+__global__ void __launch_bounds__(kFillWarps * 32) k_expand(
     int64_t nq, const int32_t* __restrict__ iperm, const SPt<T, D>* __restrict__ qpts,
     const SPt<T, D>* __restrict__ tpts, const int64_t* __restrict__ offsets, const int2* __restrict__ recs,
     int64_t rec_cap, const uint16_t* __restrict__ rcount, T inv_r, int32_t* __restrict__ senders,
-    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, Batch bt) {
-    __shared__ ExpandSmem<T, D> sm_all[kExpandWarps];
+    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int32_t* __restrict__ twins,
+    int* __restrict__ status, Batch bt, int bulk_ok) {
+    constexpr int RING = CHUNK * NCH;
+    static_assert(CHUNK % 32 == 0 && (RING & (RING - 1)) == 0 && NCH >= 2, "ring shape");
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ __align__(128) unsigned char fill_smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t i0 = ((int64_t)blockIdx.x * kExpandWarps + w) * 32;
+    const int64_t i0 = ((int64_t)blockIdx.x * kFillWarps + w) * 32;
     if (i0 >= nq) return;  // warp-uniform
-    ExpandSmem<T, D>& sm = sm_all[w];
+    unsigned char* wsm = fill_smem + (size_t)w * fill_ring_bytes<T, D, FEAT, TWIN>(RING);
+    int32_t* r_snd = reinterpret_cast<int32_t*>(wsm);
+    int32_t* r_rcv = r_snd + RING;
+    T* r_dist = reinterpret_cast<T*>(r_rcv + RING);
+    T* r_disp = r_dist + RING;
+    int32_t* r_twin = FEAT ? reinterpret_cast<int32_t*>(r_disp + D * RING) : r_snd + RING;
+
+    // Lane j: query i0 + j.
     const int64_t i = i0 + lane;
     const bool valid = i < nq;
+    const int nval = nq - i0 < 32 ? (int)(nq - i0) : 32;
     const int32_t qp = valid ? iperm[i] : 0;
     int nr = valid ? rcount[qp] : 0;
-    long long cur = 0;
-    int ne = 0;
-    if (valid && nr != kOverflowMark) {
-        cur = offsets[i];
-        ne = (int)(offsets[i + 1] - cur);
-    } else {
+    const bool over = valid && nr == kOverflowMark;
+    const long long k0 = valid ? offsets[i] : 0;
+    const long long kn = valid ? offsets[i + 1] : 0;
+    int ne = (int)(kn - k0);
+    if (over) {  // written by the walking fill
         nr = 0;
+        ne = 0;
     }
     const SPt<T, D> q = qpts[qp];
     T r2 = T(0), ir = inv_r;
     int32_t start_node = 0, base = 0;
     cloud_params<T>(bt, qp, r2, ir, start_node, base);
-    int ie = ne, irc = nr;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int a = __shfl_up_sync(0xffffffffu, ie, o);
-        const int b = __shfl_up_sync(0xffffffffu, irc, o);
-        if (lane >= o) {
-            ie += a;
-            irc += b;
-        }
-    }
-    sm.kq[lane] = cur - (ie - ne);
-#pragma unroll
-    for (int d = 0; d < D; ++d) sm.qx[d][lane] = q.x[d];
-    sm.inv_r[lane] = ir;
-    sm.qpos[lane] = qp;
-    sm.qi[lane] = q.idx - base + 1;
-    sm.base[lane] = base;
-    sm.rpre[lane + 1] = irc;
-    if (lane == 0) sm.rpre[0] = 0;
-    __syncwarp();
-    const int total_r = __shfl_sync(0xffffffffu, irc, 31);
-    const bool feat = rdisp != nullptr;  // false: neighbor lists (CSR values) only
-    int used = 0;      // positions staged (warp-uniform)
-    int ebase = 0;     // flat edge index of pos[0]
-    int qr = 0;        // this lane's query, for records
+    const long long K0 = __shfl_sync(FULL, k0, 0);
+    const long long K1 = __shfl_sync(FULL, kn, nval - 1);
+    const bool bulk = bulk_ok && !__any_sync(FULL, over) && K1 - K0 >= 32;
+    const long long kbase = K0 & ~3LL;  // ring slot 0 <-> COO edge kbase (mod RING)
+    long long next_flush = 0;           // next ring chunk to write out (chunk c: [kbase + c*CHUNK, +CHUNK))
+    long long cur_chunk = -1;           // highest chunk written so far
 
-    // Writes flat edges [ebase, ebase + cnt) from the staged positions: four
-    // entries per lane in flight, rel_displacement through shared memory so
-    // that each store of the warp covers consecutive values.
-    auto write_batch = [&](int cnt) {
-        for (int f0 = 0; f0 < cnt; f0 += 4 * 32) {
-            int qv[4];
-            long long kv[4];
-            SPt<T, D> tp[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int f = f0 + 32 * u + lane;
-                if (f < cnt) {
-                    const int qe = sm.who[f];
-                    qv[u] = qe;
-                    kv[u] = sm.kq[qe] + (ebase + f);
-                    tp[u] = tpts[sm.pos[f]];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int fb = f0 + 32 * u;
-                if (fb >= cnt) break;
-                const int nb = min(32, cnt - fb);
-                if (lane < nb) {
-                    const int q2 = qv[u];
-                    const long long k = kv[u];
-                    senders[k] = tp[u].idx - sm.base[q2] + 1;
-                    if (feat) {
-                        const T iv = sm.inv_r[q2];
-                        T px[D], diff[D];
-#pragma unroll
-                        for (int d = 0; d < D; ++d) px[d] = sm.qx[d][q2];
-                        const T d2 = dist2<T, D>(tp[u].x, px, diff);
-                        receivers[k] = sm.qi[q2];
-                        rdist[k] = mul_rn(sqrt_rn(d2), iv);
-#pragma unroll
-                        for (int d = 0; d < D; ++d) sm.disp[D * lane + d] = mul_rn(-diff[d], iv);
-                        sm.key[lane] = k;
+    // Writes out the chunks that end at or before `upto` (all that remain of
+    // the range when `last`): the aligned part by bulk copies (one group per
+    // chunk), the unaligned ends by lanes.
+    auto flush = [&](long long upto, bool last) {
+        while (true) {
+            const long long cs = kbase + next_flush * CHUNK, ce = cs + CHUNK;
+            if (cs >= K1 || (ce > upto && !last)) break;
+            const long long lo = cs > K0 ? cs : K0, hi = ce < K1 ? ce : K1;
+            long long a = (lo + 3) & ~3LL;
+            if (a > hi) a = hi;
+            const long long b = a + ((hi - a) & ~3LL);
+            if (lane == 0) {
+                if (b > a) {
+                    const int sl = (int)((a - kbase) & (RING - 1));
+                    const uint32_t m = (uint32_t)(b - a);
+                    bulk_store(senders + a, r_snd + sl, 4u * m);
+                    if (FEAT) {
+                        bulk_store(receivers + a, r_rcv + sl, 4u * m);
+                        bulk_store(rdist + a, r_dist + sl, (uint32_t)sizeof(T) * m);
+                        bulk_store(rdisp + (long long)D * a, r_disp + D * sl, (uint32_t)(D * sizeof(T)) * m);
                     }
+                    if (TWIN) bulk_store(twins + a, r_twin + sl, 4u * m);
                 }
-                if (feat) {
-                    __syncwarp();
-#pragma unroll
-                    for (int c = 0; c < D; ++c) {
-                        const int v = 32 * c + lane;  // value v of the batch: entry v / D, axis v % D
-                        const int ent = v / D;
-                        if (ent < nb) rdisp[D * sm.key[ent] + (v - D * ent)] = sm.disp[v];
-                    }
-                    __syncwarp();
-                }
+                bulk_commit();  // one group per chunk, empty or not
             }
+            // [lo, a) and [b, hi): at most three edges each
+            const long long k = lane < 4 ? lo + lane : b + (lane - 4);
+            if ((lane < 4 && k < a) || (lane >= 4 && lane < 8 && k < hi)) {
+                const int sl = (int)((k - kbase) & (RING - 1));
+                senders[k] = r_snd[sl];
+                if (FEAT) {
+                    receivers[k] = r_rcv[sl];
+                    rdist[k] = r_dist[sl];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) rdisp[(long long)D * k + d] = r_disp[D * sl + d];
+                }
+                if (TWIN) twins[k] = r_twin[sl];
+            }
+            ++next_flush;
         }
     };
 
-    for (int r0 = 0; r0 < total_r; r0 += 32) {
-        const int rho = r0 + lane;
-        int2 rec = make_int2(0, 0);
-        if (rho < total_r) {
-            while (sm.rpre[qr + 1] <= rho) ++qr;
-            rec = recs[(int64_t)sm.qpos[qr] * rec_cap + (rho - sm.rpre[qr])];
-        }
-        const int p = __popc((unsigned)rec.y);
-        int incl = p;
+    for (int j = 0; j < nval; ++j) {
+        const int nej = __shfl_sync(FULL, ne, j);
+        if (nej == 0) continue;  // warp-uniform
+        const int nrj = __shfl_sync(FULL, nr, j);
+        const long long kj = __shfl_sync(FULL, k0, j);
+        const int32_t qpj = __shfl_sync(FULL, qp, j);
+        const int32_t bj = __shfl_sync(FULL, base, j);
+        const int32_t qij = __shfl_sync(FULL, q.idx, j) - bj + 1;
+        const T irj = __shfl_sync(FULL, ir, j);
+        T px[D];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int a = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += a;
-        }
-        // Stage the round's records in parts that fit the free positions,
-        // writing the staged edges out whenever the next record does not fit.
-        int lo = 0, base_incl = 0;  // lanes below `lo` are staged (warp-uniform)
-        while (lo < 32) {
-            const bool fits = lane >= lo && incl - base_incl <= kExpandCap - used;
-            const int hi = lo + __popc(__ballot_sync(0xffffffffu, fits));
-            if (hi == lo) {
-                write_batch(used);
-                ebase += used;
-                used = 0;
-                continue;
+        for (int d = 0; d < D; ++d) px[d] = __shfl_sync(FULL, q.x[d], j);
+        const int2* rp = recs + (int64_t)qpj * rec_cap;
+        long long kq = kj;  // COO index of the query's next edge
+        for (int r0 = 0; r0 < nrj; r0 += 32) {
+            int2 rec = make_int2(0, 0);
+            if (r0 + lane < nrj) rec = rp[r0 + lane];
+            const int p = __popc((unsigned)rec.y);
+            int incl = p;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
             }
-            if (fits) {
-                int at = used + (incl - p - base_incl);
-                unsigned m = (unsigned)rec.y;
-                while (m) {
-                    const int j = __ffs(m) - 1;
-                    m &= m - 1;
-                    sm.who[at] = (uint8_t)qr;
-                    sm.pos[at++] = rec.x + j;
+            const int tot = __shfl_sync(FULL, incl, 31);
+            const int excl = incl - p;
+            for (int e0 = 0; e0 < tot; e0 += 32) {
+                const int e = e0 + lane;
+                // the record lane holding hit e: the last lane whose first hit is <= e
+                int r = 0;
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const int v = __shfl_sync(FULL, excl, r + st);
+                    if (v <= e) r += st;
+                }
+                const unsigned m = (unsigned)__shfl_sync(FULL, rec.y, r);
+                const int rx = __shfl_sync(FULL, rec.x, r);
+                const int er = __shfl_sync(FULL, excl, r);
+                const int cnt = min(32, tot - e0);
+                const long long kb = kq + e0;  // COO index of lane 0's edge
+                if (bulk) {
+                    const long long c = (kb + cnt - 1 - kbase) / CHUNK;
+                    if (c != cur_chunk) {
+                        // entering chunk c reuses the slots of chunk c - NCH
+                        if (c >= NCH) {
+                            if (lane == 0) bulk_wait_read<NCH - 2>();
+                            __syncwarp();
+                        }
+                        cur_chunk = c;
+                    }
+                }
+                if (lane < cnt) {
+                    const int tpos = rx + kth_set_bit(m, e - er);
+                    const SPt<T, D> t = tpts[tpos];
+                    const long long k = kb + lane;
+                    const int32_t snd = t.idx - bj + 1;
+                    T dv[D], dist = T(0);
+                    if (FEAT) {
+                        T diff[D];
+                        const T d2 = dist2<T, D>(t.x, px, diff);
+                        dist = mul_rn(sqrt_rn(d2), irj);
+#pragma unroll
+                        for (int d = 0; d < D; ++d) dv[d] = mul_rn(-diff[d], irj);
+                    }
+                    int32_t tw = -1;
+                    if (TWIN) {
+                        // the query's place among the target's hits, record by record
+                        const int2* rj = recs + (int64_t)tpos * rec_cap;
+                        const int nrt = rcount[tpos];
+                        int rank = 0;
+                        for (int rr = 0; rr < nrt; ++rr) {
+                            const int2 rc = rj[rr];
+                            const unsigned off = (unsigned)(qpj - rc.x);
+                            if (off < 32u && ((unsigned)rc.y >> off) & 1u) {
+                                tw = (int32_t)(offsets[t.idx] + rank + __popc((unsigned)rc.y & ((1u << off) - 1u)));
+                                break;
+                            }
+                            rank += __popc((unsigned)rc.y);
+                        }
+                        if (tw < 0) atomicOr(status, 4);
+                    }
+                    if (bulk) {
+                        const int sl = (int)((k - kbase) & (RING - 1));
+                        r_snd[sl] = snd;
+                        if (FEAT) {
+                            r_rcv[sl] = qij;
+                            r_dist[sl] = dist;
+#pragma unroll
+                            for (int d = 0; d < D; ++d) r_disp[D * sl + d] = dv[d];
+                        }
+                        if (TWIN) r_twin[sl] = tw;
+                        fence_smem_to_bulk();
+                    } else {
+                        senders[k] = snd;
+                        if (FEAT) {
+                            receivers[k] = qij;
+                            rdist[k] = dist;
+#pragma unroll
+                            for (int d = 0; d < D; ++d) rdisp[(long long)D * k + d] = dv[d];
+                        }
+                        if (TWIN) twins[k] = tw;
+                    }
+                }
+                if (bulk) {
+                    __syncwarp();
+                    flush(kb + cnt, false);
                 }
             }
-            const int hi_incl = __shfl_sync(0xffffffffu, incl, hi - 1);
-            used += hi_incl - base_incl;
-            base_incl = hi_incl;
-            lo = hi;
-            __syncwarp();
+            kq += tot;
         }
     }
-    write_batch(used);
+    if (bulk) {
+        __syncwarp();
+        flush(K1, true);
+        if (lane == 0) bulk_wait_all();
+    }
 }
 
 // Per-thread reference-order DFS for a handful of query points (the
@@ -651,6 +818,8 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
     }
     const T r = (T)t.radius;
     const T r2 = r * r;  // src/cpu/edges_cpu.jl:184
+    const Tuning tn = ctx.tuning_for(t.ndims, t.dtype, nq, q.nbrs_hint);
+    ctx.plan_tuning = tn;
     ctx.rec_cap = 0;
     if (t.n_nodes == 0) {
         if ((err = cudaMemsetAsync(ctx.counts.p, 0, (size_t)nq * 4, s))) return cuda_status(ctx, err, "zero counts");
@@ -671,12 +840,14 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
                 nullptr, nullptr, nullptr, nullptr, (int*)(ctx.total.as<int64_t>() + 1), ctx.recs.as<int2>(),
-                ctx.rec_cap, ctx.rcount.as<uint16_t>(), ctx.gflag.as<uint8_t>(), t.batch());
+                ctx.rec_cap, ctx.rcount.as<uint16_t>(), ctx.gflag.as<uint8_t>(), t.batch(), nullptr, tn.max_seg,
+                tn.multi_pop, tn.sub_boxes);
         else
             k_edges<T, D, EP_COUNT><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
-                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch());
+                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr,
+                tn.max_seg, tn.multi_pop, tn.sub_boxes);
         ctx.kernel_launches += 1;
     }
     {
@@ -688,6 +859,7 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
         (err = wait_stream(s)))
         return cuda_status(ctx, err, "edge count");
     *n_edges = ctx.total_host[0];
+    q.nbrs_hint = (double)*n_edges / (double)std::max<int64_t>(nq, 1);
     ctx.rec_overflow = 0;
     if (ctx.rec_cap) {
         // Size the next count's records for this one's largest query.
@@ -700,20 +872,68 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
     return OK;
 }
 
+// Ring of the fill: kFillRing chunks of CHUNK edges (32, 64 or 128: a tuned shape).
+constexpr int kFillRing = 4;
+
+template <class T, int D, bool FEAT, bool TWIN, int CHUNK>
+cudaError_t launch_expand_shape(Ctx& ctx, const Tree& q, const Tree& t, T inv_r, int32_t* senders, int32_t* receivers,
+                                void* rel_disp, void* rel_dist, int32_t* twins, int bulk_ok) {
+    constexpr size_t smem = kFillWarps * fill_ring_bytes<T, D, FEAT, TWIN>(CHUNK * kFillRing);
+    auto kern = k_expand<T, D, FEAT, TWIN, CHUNK, kFillRing>;
+    if (smem > 48 * 1024) {
+        static bool attr_set = false;  // per instantiation
+        if (!attr_set) {
+            const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
+    }
+    kern<<<div_up(q.n, 32 * kFillWarps), kFillWarps * 32, smem, ctx.stream>>>(
+        q.n, q.iperm.as<int32_t>(), q.spts.as<SPt<T, D>>(), t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
+        ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint16_t>(), inv_r, senders, receivers, (T*)rel_disp,
+        (T*)rel_dist, twins, ctx.dstatus.as<int>() + 1, t.batch(), bulk_ok);
+    return cudaGetLastError();
+}
+
+template <class T, int D, bool FEAT>
+cudaError_t launch_expand(Ctx& ctx, const Tree& q, const Tree& t, T inv_r, int32_t* senders, int32_t* receivers,
+                          void* rel_disp, void* rel_dist, int32_t* twins, int bulk_ok) {
+    if (FEAT && twins)  // the mirror indices of a differentiable fill: one shape
+        return launch_expand_shape<T, D, FEAT, true, 64>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
+                                                         twins, bulk_ok);
+    switch (ctx.plan_tuning.fill_chunk) {
+        case 32:
+            return launch_expand_shape<T, D, FEAT, false, 32>(ctx, q, t, inv_r, senders, receivers, rel_disp,
+                                                              rel_dist, nullptr, bulk_ok);
+        case 128:
+            return launch_expand_shape<T, D, FEAT, false, 128>(ctx, q, t, inv_r, senders, receivers, rel_disp,
+                                                               rel_dist, nullptr, bulk_ok);
+        default:
+            return launch_expand_shape<T, D, FEAT, false, 64>(ctx, q, t, inv_r, senders, receivers, rel_disp,
+                                                              rel_dist, nullptr, bulk_ok);
+    }
+}
+
 template <class T, int D>
 int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* senders, int32_t* receivers,
-               void* rel_disp, void* rel_dist) {
+               void* rel_disp, void* rel_dist, int32_t* twins = nullptr) {
     const T r = (T)t.radius;
     const T r2 = r * r;
     const T inv_r = T(1) / r;  // inv(r), src/cpu/edges_cpu.jl:185
     cudaStream_t s = ctx.stream;
+    const Tuning& tn = ctx.plan_tuning;  // the shapes of the count this fill follows
     PhaseTimer pt_(ctx, PH_FILL);
     const int64_t ng = q.n_groups;
     if (ctx.rec_cap) {
-        k_expand<T, D><<<div_up(q.n, 32 * kExpandWarps), kExpandWarps * 32, 0, s>>>(
-            q.n, q.iperm.as<int32_t>(), q.spts.as<SPt<T, D>>(), t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
-            ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint16_t>(), inv_r, senders, receivers, (T*)rel_disp,
-            (T*)rel_dist, t.batch());
+        const bool feat = rel_disp != nullptr;
+        auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+        const int bulk_ok = aligned(senders) && (!feat || (aligned(receivers) && aligned(rel_disp) && aligned(rel_dist))) &&
+                            (!twins || aligned(twins));
+        cudaError_t err = feat ? launch_expand<T, D, true>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
+                                                           twins, bulk_ok)
+                               : launch_expand<T, D, false>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
+                                                            nullptr, bulk_ok);
+        if (err != cudaSuccess) return cuda_status(ctx, err, "edge fill launch");
         ctx.kernel_launches += 1;
     }
     if (!ctx.rec_cap || ctx.rec_overflow) {
@@ -722,7 +942,8 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
             q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
             t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r, exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(),
             senders, receivers, (T*)rel_disp, (T*)rel_dist, ctx.dstatus.as<int>(),
-            ctx.rec_cap ? ctx.recs.as<int2>() : nullptr, ctx.rec_cap, nullptr, ctx.gflag.as<uint8_t>(), t.batch());
+            ctx.rec_cap ? ctx.recs.as<int2>() : nullptr, ctx.rec_cap, nullptr, ctx.gflag.as<uint8_t>(), t.batch(),
+            nullptr, tn.max_seg, tn.multi_pop, tn.sub_boxes);
         ctx.kernel_launches += 1;
     }
     return cuda_status(ctx, cudaGetLastError(), "edge fill launch");
@@ -747,8 +968,22 @@ cudaError_t count_into_typed(const Tree& q, const Tree& t, bool exclude_self, in
     k_edges<T, D, EP_COUNT><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
         q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
         t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch());
+        nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr, kMaxSeg, kMultiPop, 1);
     return cudaGetLastError();
+}
+
+template <class T, int D>
+int stats_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, unsigned long long* stats_dev) {
+    const T r = (T)t.radius;
+    const T r2 = r * r;
+    const Tuning tn = ctx.tuning_for(t.ndims, t.dtype, q.n, q.nbrs_hint);
+    k_edges<T, D, EP_STATS><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, ctx.stream>>>(
+        q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
+        t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr,
+        nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), stats_dev, tn.max_seg,
+        tn.multi_pop, tn.sub_boxes);
+    ctx.kernel_launches += 1;
+    return cuda_status(ctx, cudaGetLastError(), "traversal statistics launch");
 }
 
 }  // namespace
@@ -763,6 +998,29 @@ cudaError_t count_into(const Tree& q, const Tree& t, bool exclude_self, int32_t*
                             : count_into_typed<float, 2>(q, t, exclude_self, counts, s);
     return t.ndims == 3 ? count_into_typed<double, 3>(q, t, exclude_self, counts, s)
                         : count_into_typed<double, 2>(q, t, exclude_self, counts, s);
+}
+
+int traversal_stats(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, uint64_t* out, int n_out) {
+    cudaError_t err;
+    if ((err = ensure(ctx.counts, (size_t)std::max<int64_t>(q.n, 1) * 4)) || (err = ensure(ctx.tstats, TS_NUM * 8)))
+        return cuda_status(ctx, err, "allocating statistics");
+    if ((err = cudaMemsetAsync(ctx.tstats.p, 0, TS_NUM * 8, ctx.stream))) return cuda_status(ctx, err, "statistics");
+    ctx.plan_query = nullptr;  // the counts buffer is reused: no fill may follow
+    if (q.n > 0 && t.n_nodes > 0) {
+        unsigned long long* sd = ctx.tstats.as<unsigned long long>();
+        const int st = t.dtype == 0 ? (t.ndims == 3 ? stats_typed<float, 3>(ctx, q, t, exclude_self, sd)
+                                                    : stats_typed<float, 2>(ctx, q, t, exclude_self, sd))
+                                    : (t.ndims == 3 ? stats_typed<double, 3>(ctx, q, t, exclude_self, sd)
+                                                    : stats_typed<double, 2>(ctx, q, t, exclude_self, sd));
+        if (st != OK) return st;
+    }
+    uint64_t host[TS_NUM];
+    if ((err = cudaMemcpyAsync(host, ctx.tstats.p, TS_NUM * 8, cudaMemcpyDeviceToHost, ctx.stream)) ||
+        (err = cudaStreamSynchronize(ctx.stream)))
+        return cuda_status(ctx, err, "statistics read");
+    for (int k = 0; k < n_out && k < TS_NUM; ++k) out[k] = host[k];
+    for (int k = TS_NUM; k < n_out; ++k) out[k] = 0;
+    return OK;
 }
 
 int edges_count(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64_t* n_edges) {
@@ -800,6 +1058,33 @@ int edges_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
                             : fill_typed<float, 2>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist);
     return t.ndims == 3 ? fill_typed<double, 3>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist)
                         : fill_typed<double, 2>(ctx, q, t, exclude_self, senders, receivers, rel_disp, rel_dist);
+}
+
+int edges_fill_diff(Ctx& ctx, const Tree& t, int32_t* senders, int32_t* receivers, void* rel_disp, void* rel_dist,
+                    int32_t* mirror, int64_t n_edges) {
+    if (ctx.plan_query != &t || ctx.plan_target != &t || ctx.plan_qgen != t.generation ||
+        ctx.plan_tgen != t.generation || ctx.plan_exclude != 1)
+        return set_error(ctx, ERR_STATE, "oct_edges_fill_diff: no matching self-pair oct_edges_count for this build");
+    if (t.n_clouds) return set_error(ctx, ERR_ARGUMENT, "oct_edges_fill_diff: not defined for a batched tree");
+    if (n_edges < ctx.plan_edges)
+        return set_error(ctx, ERR_CAPACITY, "oct_edges_fill_diff: output capacity is smaller than the edge count");
+    if (ctx.plan_edges > INT32_MAX)
+        return set_error(ctx, ERR_OVERFLOW, "oct_edges_fill_diff: more than 2^31 - 1 edges overflow the Int32 mirrors");
+    if (ctx.plan_edges == 0 || t.n == 0 || t.n_nodes == 0) return OK;
+    // From the hit records when every query's records are complete (the
+    // mirror of an edge is read off its target's records); otherwise after
+    // the fill, by scanning the senders' segments.
+    const bool from_records = ctx.rec_cap > 0 && ctx.rec_overflow == 0;
+    int32_t* tw = from_records ? mirror : nullptr;
+    int st;
+    if (t.dtype == 0)
+        st = t.ndims == 3 ? fill_typed<float, 3>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist, tw)
+                          : fill_typed<float, 2>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist, tw);
+    else
+        st = t.ndims == 3 ? fill_typed<double, 3>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist, tw)
+                          : fill_typed<double, 2>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist, tw);
+    if (st != OK || from_records) return st;
+    return edges_mirror_scan(ctx, senders, receivers, ctx.plan_edges, t.n, ctx.offsets.as<int64_t>(), mirror);
 }
 
 namespace {

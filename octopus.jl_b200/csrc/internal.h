@@ -23,6 +23,33 @@ void release(DevBuf& b);
 
 struct Ctx;
 
+// Kernel shapes chosen per workload by the autotuner (octopus.jl_b200/tune.py).
+// No result depends on them: they change how the work is cut, not what is
+// computed.
+struct Tuning {
+    int max_seg = 16;     // leaves sharing one staged chunk of the traversal (1..16)
+    int multi_pop = 4;    // internal nodes expanded together by the traversal (1..4)
+    int fill_chunk = 64;  // edges per bulk-copy chunk of the fill (32, 64 or 128)
+    int group_cap = 32;   // query points per traversal group, set at the build (8..32)
+    int sub_boxes = 1;    // boxes a group's queries are split into for the target test (1, 2 or 4)
+};
+
+// One row of a tuning table: the shapes measured best for point sets of
+// about 2^nlog2 points with about 2^nbr_log2 - 1 neighbors per point.
+struct TuneRow {
+    int ndims, dtype, nlog2, nbr_log2;
+    Tuning tn;
+};
+
+// Parses a tuning table (one row per line: ndims dtype nlog2 nbr_log2 max_seg
+// multi_pop fill_chunk group_cap [sub_boxes]; '#' starts a comment).  Returns false when
+// the file cannot be read or a row is malformed.  A ninth value, sub_boxes,
+// is optional (1 when absent).
+bool parse_tuning(const char* path, std::vector<TuneRow>& rows, std::string& err);
+// The row nearest to (n, neighbors per point) among those of the same ndims
+// and dtype (index into rows, -1 when none), and its shapes (defaults when none).
+int select_tuning(const std::vector<TuneRow>& rows, int ndims, int dtype, int64_t n, double nbrs, Tuning& out);
+
 // Phases timed by the optional CUDA-event profiler (oct_profile_*).
 enum Phase : int {
     PH_BOUNDS = 0, PH_ENCODE, PH_SORT, PH_GATHER, PH_TOPOLOGY, PH_REFIT,
@@ -52,6 +79,7 @@ struct Tree {
     int64_t n = 0;
     double radius = 0.0;
     int32_t leaf_size = kLeafSize;
+    int32_t group_cap = 32;  // query points per traversal group of the last build
     bool built = false;
     bool keep_morton = false;
     uint64_t generation = 0;
@@ -71,6 +99,7 @@ struct Tree {
     DevBuf sort_tmp;             // int64 tile sums of the histogram scan
     DevBuf look;                 // one-pass-per-digit sort: digit counts and tile look-back words
     DevBuf spts;                 // SPt<T,D>[n] in Morton order
+    DevBuf spts_tmp;             // SPt<T,D>[n]: the key sort's intermediate passes
     DevBuf iperm;                // int32 [n]: sorted position of each original point
     const int32_t* perm_dev = nullptr;  // original index of each sorted position (null: identity)
     const void* skeys_dev = nullptr;    // sorted keys of the last build (key_bytes wide)
@@ -107,6 +136,9 @@ struct Tree {
     // Batched build (many clouds in one forest); n_clouds == 0 otherwise.
     int32_t n_clouds = 0;
     int32_t kbits = 0;
+    // Neighbors per point of this tree's last count as a query set (-1 before
+    // the first), which keys the tuning table.
+    mutable double nbrs_hint = -1.0;
     DevBuf b_coff;               // int64 [n_clouds + 1]
     DevBuf b_cparam;             // double [n_clouds * kCloudParams]
     DevBuf b_croot, b_cstart;    // int32 [n_clouds]
@@ -160,6 +192,7 @@ struct Ctx {
     DevBuf dredge;       // edges ordered by receiver (adjoint of a COO not grouped by receiver)
     DevBuf dterm;        // per-edge cotangent term of the self-pair adjoint (4 values)
     DevBuf dseg;         // per-point {first, end} edge of the self-pair adjoint
+    DevBuf tstats;       // traversal statistics (oct_edges_traversal_stats)
     // Options (oct_ctx_set_option): the polling rounds of a bounded device
     // wait; a node capacity for each build's first topology attempt (0 =
     // estimate); hit records per query point (0 = automatic); canary regions
@@ -171,6 +204,14 @@ struct Ctx {
     bool guard_check = false;
     int32_t withhold_tile = -1;
     int32_t last_attempts = 0;    // topology attempts of the last build
+    // Tuning: the table (oct_ctx_load_tuning), shapes forced by options
+    // (0 = from the table), the shapes of the last count (used by its fill)
+    // and the table row they came from (-1 = defaults).
+    std::vector<TuneRow> tune_table;
+    Tuning tune_force{0, 0, 0, 0, 0};
+    Tuning plan_tuning;
+    int last_tune_row = -1;
+    Tuning tuning_for(int ndims, int dtype, int64_t n, double nbrs);
     // Profiler.
     int64_t kernel_launches = 0;  // every kernel this context has launched
     bool profiling = false;
@@ -203,6 +244,11 @@ int materialize_view(Ctx& ctx, Tree& t);
 int edges_count(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64_t* n_edges);
 int edges_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* senders,
                int32_t* receivers, void* rel_disp, void* rel_dist, int64_t n_edges);
+int edges_fill_diff(Ctx& ctx, const Tree& t, int32_t* senders, int32_t* receivers, void* rel_disp, void* rel_dist,
+                    int32_t* mirror, int64_t n_edges);
+int edges_mirror_scan(Ctx& ctx, const int32_t* snd, const int32_t* rcv, int64_t m, int64_t n, const int64_t* off,
+                      int32_t* mirror);
+int traversal_stats(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, uint64_t* out, int n_out);
 int neighbors_of(Ctx& ctx, const Tree& t, const void* qcoords, int64_t nsel, int32_t* out_counts,
                  int32_t* out_idx, int64_t cap);
 cudaError_t count_into(const Tree& q, const Tree& t, bool exclude_self, int32_t* counts, cudaStream_t s);
@@ -211,12 +257,18 @@ int csr_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t*
 
 // Permutation of user arrays by a built tree (zsort.cu).
 int zsort_apply(Ctx& ctx, const Tree& t, const void* in, void* out, int64_t n, int64_t row_bytes, int direction);
+int permute_rows(Ctx& ctx, const int32_t* perm, int64_t n, const void* in, void* out, int64_t row_bytes,
+                 int direction);
 
 // Adjoint (diff.cu).
 int diff_backward(Ctx& ctx, int ndims, int dtype, int64_t n_points, int64_t n_edges,
                   const int32_t* senders, const int32_t* receivers, const void* rel_disp,
                   const void* rel_dist, const void* d_disp, const void* d_dist, double radius,
                   void* grad, const void* coords, const int32_t* order);
+int diff_backward_mirror(Ctx& ctx, int ndims, int dtype, int64_t n, int64_t m, const int32_t* snd,
+                         const int32_t* rcv, const int32_t* mirror, const void* rel_disp, const void* rel_dist,
+                         const void* coords, const void* d_disp, const void* d_dist, double radius, void* grad,
+                         const int32_t* order);
 int diff_backward_pair(Ctx& ctx, int ndims, int dtype, int64_t nq, int64_t nt, int64_t m, const int32_t* snd,
                        const int32_t* rcv, const void* rel_disp, const void* rel_dist, const void* d_disp,
                        const void* d_dist, double radius, void* grad_q, void* grad_t);

@@ -4,7 +4,8 @@ and a small runner used for device profiling.
     python octopus.jl_b200/workloads.py <workload> [--steps S] [--scale F]
 
 runs S time steps of run! + build_edges on cuda:0 (used as the target of
-ncu captures; it prints the edge count per step).
+ncu captures; it prints the edge count per step; ``--stats`` adds the count
+pass's traversal statistics).
 
 Workloads (float32):
   uniform100k  3D, 100,000 points U[0,1)^3, r = 0.04
@@ -65,7 +66,29 @@ def gaussian_mixture_2d(n: int, k: int, seed: int) -> np.ndarray:
     return np.concatenate([pts, rng.random((nb, 2))]).astype(np.float32)
 
 
-def _run(name: str, steps: int, scale: float):
+def traversal_stats(ob, tns, sid) -> dict:
+    """The count pass's traversal statistics for the self pair of set `sid`
+    (oct_edges_traversal_stats), with the derived ratios."""
+    import ctypes as C
+    names = ob._lib.TRAVERSAL_STATS
+    buf = (C.c_uint64 * len(names))()
+    ctx = tns._ctx
+    ctx.bind_stream()
+    h = tns.trees[sid - 1].handle
+    ctx.check(ctx.lib.oct_edges_traversal_stats(ctx.handle, h, h, 1, buf, len(names)), "traversal stats")
+    st = {k: int(v) for k, v in zip(names, buf)}
+    hits = max(st["hits"], 1)
+    st["pair_tests_per_hit"] = st["pair_tests"] / hits
+    st["targets_per_chunk"] = st["targets_staged"] / max(st["leaf_chunks"], 1)
+    st["steps_per_chunk"] = st["pair_steps"] / max(st["leaf_chunks"], 1)
+    st["chunks_per_group"] = st["leaf_chunks"] / max(st["groups"], 1)
+    st["expansions_per_group"] = st["expansions"] / max(st["groups"], 1)
+    st["cycle_share_leaf"] = st["cycles_leaf"] / max(st["cycles_total"], 1)
+    st["cycle_share_pairs"] = st["cycles_pairs"] / max(st["cycles_total"], 1)
+    return st
+
+
+def _run(name: str, steps: int, scale: float, stats: bool = False):
     import torch
     here = os.path.dirname(os.path.abspath(__file__))
     sys.path.insert(0, os.path.dirname(here))
@@ -105,6 +128,9 @@ def _run(name: str, steps: int, scale: float):
         e = ob.build_edges(tns, sid, sid)
         ob.synchronize(tns)
         print(f"{name}: n={x.shape[1]} edges={e.senders.numel()}")
+    if stats:
+        import json
+        print(json.dumps(traversal_stats(ob, tns, sid)))
 
 
 def _run_build(ob, torch, x, r, steps):
@@ -178,5 +204,6 @@ if __name__ == "__main__":
     ap.add_argument("workload")
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--stats", action="store_true", help="print the count pass's traversal statistics")
     a = ap.parse_args()
-    _run(a.workload, a.steps, a.scale)
+    _run(a.workload, a.steps, a.scale, a.stats)

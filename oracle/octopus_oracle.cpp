@@ -387,20 +387,31 @@ template <> std::vector<double>& rdistv<double>(Edges& e) { return e.rdist_d; }
 // src/cpu/edges_cpu.jl:172-247 (build_edges_cpu!) with the count and fill
 // workers of :36-168.  The scan is carried in int64: the reference's Int32
 // scan cannot represent 2^31 or more edges.
+//
+// q_first / q_last (1-based, inclusive) restrict the queries to a range: the
+// result is then the slice of the full COO that those queries own (the COO
+// lists each query's edges contiguously, in query order), with offsets
+// relative to the slice's first edge.  The whole set is q_first = 1,
+// q_last = n_q.
 template <class T, int D>
 void build_edges(Edges& e, Tree& t, const T* coords_q, int64_t n_q, const T* coords_t,
-                 T r, bool exclude_self, int nthreads) {
+                 T r, bool exclude_self, int nthreads, int64_t q_first = 1, int64_t q_last = -1) {
+    if (q_last < 0) q_last = n_q;
+    const int64_t m_q = q_last - q_first + 1;  // queries in the range
     const T r_sq = r * r;
     const T inv_r = T(1) / r;
     const T* bmin = bmin_of<T>(t);
     const T* bmax = bmax_of<T>(t);
     const int depth = 1 + ((1 << D) - 1) * bits_per_axis<D>();
-    std::vector<int64_t> counts(n_q + 1, 0);
-    const int64_t nchunks = n_query_chunks(n_q, nthreads, nthreads);
+    // counts[i - q_first + 1] for query i of the range
+    std::vector<int64_t> counts(m_q + 1, 0);
+    const int64_t nchunks = n_query_chunks(m_q, nthreads, nthreads);
 #pragma omp parallel for schedule(static, 1) num_threads(nthreads)
     for (int64_t c = 1; c <= nchunks; ++c) {
         int64_t lo, hi;
-        chunk_bounds(n_q, nchunks, c, lo, hi);
+        chunk_bounds(m_q, nchunks, c, lo, hi);
+        lo += q_first - 1;
+        hi += q_first - 1;
         std::vector<int32_t> stack(depth + 8);
         for (int64_t i = lo; i <= hi; ++i) {
             const T* p = coords_q + D * (i - 1);
@@ -410,11 +421,11 @@ void build_edges(Edges& e, Tree& t, const T* coords_q, int64_t n_q, const T* coo
                            [&](int32_t j, const T*, T) {
                                if (!exclude_self || j != i32) ++cnt;
                            });
-            counts[i] = cnt;
+            counts[i - q_first + 1] = cnt;
         }
     }
-    for (int64_t i = 1; i <= n_q; ++i) counts[i] += counts[i - 1];
-    e.n_edges = counts[n_q];
+    for (int64_t i = 1; i <= m_q; ++i) counts[i] += counts[i - 1];
+    e.n_edges = counts[m_q];
     e.offsets = counts;
     e.senders.assign(e.n_edges, 0);
     e.receivers.assign(e.n_edges, 0);
@@ -427,11 +438,13 @@ void build_edges(Edges& e, Tree& t, const T* coords_q, int64_t n_q, const T* coo
 #pragma omp parallel for schedule(static, 1) num_threads(nthreads)
     for (int64_t c = 1; c <= nchunks; ++c) {
         int64_t lo, hi;
-        chunk_bounds(n_q, nchunks, c, lo, hi);
+        chunk_bounds(m_q, nchunks, c, lo, hi);
+        lo += q_first - 1;
+        hi += q_first - 1;
         std::vector<int32_t> stack(depth + 8);
         for (int64_t i = lo; i <= hi; ++i) {
             const T* p = coords_q + D * (i - 1);
-            int64_t cur = counts[i - 1];
+            int64_t cur = counts[i - q_first];
             const int32_t i32 = (int32_t)i;
             traverse<T, D>(t, bmin, bmax, coords_t, p, r_sq, stack.data(),
                            [&](int32_t j, const T* diff, T d2) {
@@ -564,24 +577,35 @@ void oracle_tree_copy(void* h, int32_t* node_first, int32_t* node_last, int32_t*
 
 void oracle_tree_free(void* h) { delete (Tree*)h; }
 
-// build_edges for the pair (query coords, target tree).
-void* oracle_edges_build(void* tree_t, const void* coords_q, int64_t n_q, const void* coords_t,
-                         double radius, int exclude_self, int nthreads) {
+// build_edges for the pair (query coords, target tree), restricted to the
+// queries q_first..q_last (1-based, inclusive; q_last < 0: all of them).
+void* oracle_edges_build_range(void* tree_t, const void* coords_q, int64_t n_q, const void* coords_t,
+                               double radius, int exclude_self, int nthreads, int64_t q_first, int64_t q_last) {
     Tree* t = (Tree*)tree_t;
     Edges* e = new Edges();
+    if (q_last < 0) q_last = n_q;
     if (t->dtype == 0) {
         const float r = (float)radius;
         if (t->ndims == 3)
-            build_edges<float, 3>(*e, *t, (const float*)coords_q, n_q, (const float*)coords_t, r, exclude_self, nthreads);
+            build_edges<float, 3>(*e, *t, (const float*)coords_q, n_q, (const float*)coords_t, r, exclude_self, nthreads,
+                                  q_first, q_last);
         else
-            build_edges<float, 2>(*e, *t, (const float*)coords_q, n_q, (const float*)coords_t, r, exclude_self, nthreads);
+            build_edges<float, 2>(*e, *t, (const float*)coords_q, n_q, (const float*)coords_t, r, exclude_self, nthreads,
+                                  q_first, q_last);
     } else {
         if (t->ndims == 3)
-            build_edges<double, 3>(*e, *t, (const double*)coords_q, n_q, (const double*)coords_t, radius, exclude_self, nthreads);
+            build_edges<double, 3>(*e, *t, (const double*)coords_q, n_q, (const double*)coords_t, radius, exclude_self,
+                                   nthreads, q_first, q_last);
         else
-            build_edges<double, 2>(*e, *t, (const double*)coords_q, n_q, (const double*)coords_t, radius, exclude_self, nthreads);
+            build_edges<double, 2>(*e, *t, (const double*)coords_q, n_q, (const double*)coords_t, radius, exclude_self,
+                                   nthreads, q_first, q_last);
     }
     return e;
+}
+
+void* oracle_edges_build(void* tree_t, const void* coords_q, int64_t n_q, const void* coords_t,
+                         double radius, int exclude_self, int nthreads) {
+    return oracle_edges_build_range(tree_t, coords_q, n_q, coords_t, radius, exclude_self, nthreads, 1, -1);
 }
 
 int64_t oracle_edges_n(void* h) { return ((Edges*)h)->n_edges; }

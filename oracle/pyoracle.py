@@ -52,6 +52,8 @@ def load():
         lib.oracle_tree_free.argtypes = [P]
         lib.oracle_edges_build.restype = P
         lib.oracle_edges_build.argtypes = [P, P, i64, P, C.c_double, C.c_int, C.c_int]
+        lib.oracle_edges_build_range.restype = P
+        lib.oracle_edges_build_range.argtypes = [P, P, i64, P, C.c_double, C.c_int, C.c_int, i64, i64]
         lib.oracle_edges_n.restype = i64
         lib.oracle_edges_n.argtypes = [P]
         lib.oracle_edges_copy.argtypes = [P, C.c_int, C.c_int, P, P, P, P, P, i64]
@@ -159,17 +161,25 @@ def build_tree(coords, radius, leaf_size=32, nthreads=0) -> OracleTree:
 
 
 def build_edges(tree: OracleTree, coords_q: np.ndarray, radius=None, exclude_self=None,
-                nthreads: int = 0):
+                nthreads: int = 0, query_range=None):
     """build_edges_cpu! (src/cpu/edges_cpu.jl:172-247) for query coords against
-    ``tree``.  Returns a dict of numpy arrays in the reference's COO order."""
+    ``tree``.  Returns a dict of numpy arrays in the reference's COO order.
+
+    ``query_range = (lo, hi)`` (0-based, half-open) returns only the edges of
+    queries lo..hi-1: the slice of the full COO that those queries own, with
+    ``offsets`` (hi - lo + 1 entries) counted from the slice's first edge."""
     lib = load()
     coords_q = np.ascontiguousarray(coords_q, tree.dtype)
     radius = tree.radius if radius is None else float(radius)
     if exclude_self is None:
         exclude_self = coords_q is tree.coords
     nthreads = nthreads or max_threads()
-    h = lib.oracle_edges_build(tree._h, _ptr(coords_q), coords_q.shape[0], _ptr(tree.coords),
-                               radius, int(bool(exclude_self)), nthreads)
+    nq = coords_q.shape[0]
+    lo, hi = (0, nq) if query_range is None else (int(query_range[0]), int(query_range[1]))
+    if not 0 <= lo <= hi <= nq:
+        raise ValueError("query_range out of bounds")
+    h = lib.oracle_edges_build_range(tree._h, _ptr(coords_q), nq, _ptr(tree.coords), radius,
+                                     int(bool(exclude_self)), nthreads, lo + 1, hi)
     try:
         m = int(lib.oracle_edges_n(h))
         d = tree.ndims
@@ -178,11 +188,11 @@ def build_edges(tree: OracleTree, coords_q: np.ndarray, radius=None, exclude_sel
             "receivers": np.zeros(m, np.int32),
             "rel_displacement": np.zeros((m, d), tree.dtype),
             "rel_dist_norm": np.zeros(m, tree.dtype),
-            "offsets": np.zeros(coords_q.shape[0] + 1, np.int64),
+            "offsets": np.zeros(hi - lo + 1, np.int64),
         }
         lib.oracle_edges_copy(h, d, _dtype_code(coords_q), _ptr(out["senders"]),
                               _ptr(out["receivers"]), _ptr(out["rel_displacement"]),
-                              _ptr(out["rel_dist_norm"]), _ptr(out["offsets"]), coords_q.shape[0])
+                              _ptr(out["rel_dist_norm"]), _ptr(out["offsets"]), hi - lo)
     finally:
         lib.oracle_edges_free(h)
     return out

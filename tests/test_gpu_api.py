@@ -216,3 +216,31 @@ def test_two_tns_independent(ob):
     ob.run_(t2)
     assert t1.point_sets[0].n == 80 and t2.point_sets[0].n == 120
     assert t1.radius == float(np.float32(0.1)) and t2.radius == float(np.float32(0.2))
+
+
+def test_traversal_statistics_are_consistent(ob):
+    """oct_edges_traversal_stats: the diagnostic count pass counts exactly the
+    edges of build_edges, and every hit is one of the pair tests issued."""
+    import ctypes as C
+    rng = np.random.default_rng(401)
+    x = rng.random((30000, 3)).astype(np.float32)
+    tns = ob.TNS(torch.float32)
+    ob.set_search_radius_(tns, 0.05)
+    sid = ob.add_point_set_(tns, torch.from_numpy(x).cuda().t())
+    ob.set_active_search_(tns, sid, sid)
+    ob.run_(tns)
+    e = ob.build_edges(tns, sid, sid)
+    snd = e.senders.clone()
+    names = ob._lib.TRAVERSAL_STATS
+    buf = (C.c_uint64 * len(names))()
+    ctx = tns._ctx
+    h = tns.trees[sid - 1].handle
+    ctx.check(ctx.lib.oct_edges_traversal_stats(ctx.handle, h, h, 1, buf, len(names)), "stats")
+    st = dict(zip(names, (int(v) for v in buf)))
+    assert st["hits"] == snd.numel()
+    assert st["queries"] == len(x)
+    assert st["pair_tests"] >= st["hits"] > 0
+    assert st["cycles_total"] >= st["cycles_leaf"] >= st["cycles_pairs"] > 0
+    # the counts buffer was reused: a fill needs a new count
+    e2 = ob.build_edges(tns, sid, sid)
+    assert torch.equal(e2.senders, snd)

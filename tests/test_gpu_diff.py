@@ -347,3 +347,95 @@ def test_cross_pair_adjoint_ungrouped(ob):
         res.append((gq, gt))
     for u, v in zip(res[0], res[1]):
         assert torch.allclose(u, v, rtol=1e-5, atol=1e-6 * float(u.abs().max()))
+
+
+def _fill_diff(ob, tns, sid):
+    """oct_edges_count + oct_edges_fill_diff: the COO and each edge's mirror."""
+    import ctypes as C
+    ctx = tns._ctx
+    ctx.bind_stream()
+    h = tns.trees[sid - 1].handle
+    ne = C.c_int64()
+    ctx.check(ctx.lib.oct_edges_count(ctx.handle, h, h, 1, C.byref(ne)), "count")
+    m = int(ne.value)
+    T = tns.T
+    snd = torch.empty(m, dtype=torch.int32, device="cuda")
+    rcv = torch.empty(m, dtype=torch.int32, device="cuda")
+    disp = torch.empty((m, tns.ndims), dtype=T, device="cuda")
+    dist = torch.empty(m, dtype=T, device="cuda")
+    mir = torch.full((m,), -5, dtype=torch.int32, device="cuda")
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    ctx.check(ctx.lib.oct_edges_fill_diff(ctx.handle, h, ptr(snd), ptr(rcv), ptr(disp), ptr(dist), ptr(mir), m),
+              "fill_diff")
+    torch.cuda.synchronize()
+    return snd, rcv, disp, dist, mir
+
+
+@pytest.mark.parametrize("d,dtype", [(3, np.float32), (2, np.float32), (3, np.float64)])
+def test_mirror_indices_from_records_and_from_the_scan(ob, d, dtype):
+    """Every edge's mirror: senders[mirror[k]] = receivers[k] and back; the
+    records path and the segment-scan path (records forced to overflow) give
+    the same indices, and the same COO as build_edges."""
+    x = uniform(30000, d, 8300 + d, dtype=dtype)
+    r = dtype(0.05 if d == 3 else 0.01)
+    tns, sid, c = setup(ob, x, r)
+    snd, rcv, disp, dist, mir = _fill_diff(ob, tns, sid)
+    e = ob.build_edges(tns, sid, sid)
+    assert torch.equal(snd, e.senders) and torch.equal(rcv, e.receivers)
+    assert torch.equal(disp, e.rel_displacement.t()) and torch.equal(dist, e.rel_dist_norm.reshape(-1))
+    m = snd.numel()
+    assert int(mir.min()) >= 0 and int(mir.max()) < m
+    ml = mir.long()
+    assert torch.equal(snd[ml], rcv) and torch.equal(rcv[ml], snd)
+    assert torch.equal(ml[ml], torch.arange(m, device="cuda"))
+    ctx = tns._ctx
+    ctx.check(ctx.lib.oct_ctx_set_option(ctx.handle, ob._lib.OPT_RECORD_CAP, 1), "record cap")
+    try:
+        _, _, _, _, mir2 = _fill_diff(ob, tns, sid)
+        import ctypes as C
+        ov = C.c_int64()
+        ctx.lib.oct_ctx_get_option(ctx.handle, ob._lib.STAT_RECORD_OVERFLOW, C.byref(ov))
+        assert ov.value > 0
+    finally:
+        ctx.check(ctx.lib.oct_ctx_set_option(ctx.handle, ob._lib.OPT_RECORD_CAP, 0), "record cap")
+    assert torch.equal(mir2, mir)
+
+
+@pytest.mark.parametrize("recompute", [False, True])
+def test_mirror_backward_equals_the_searching_backward(ob, recompute):
+    """oct_edges_diff_backward_mirror gives the bits of
+    oct_edges_diff_backward_ordered; corrupt mirror indices fall back to the
+    checked path and still give them."""
+    import ctypes as C
+    x = uniform(50000, 3, 8401)
+    r = np.float32(0.03)
+    tns, sid, c = setup(ob, x, r)
+    snd, rcv, disp, dist, mir = _fill_diff(ob, tns, sid)
+    m, n = snd.numel(), len(x)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    dd = torch.randn((m, 3), generator=gen, device="cuda")
+    dn = torch.randn(m, generator=gen, device="cuda")
+    xc = torch.from_numpy(x).cuda()
+    order = tns.trees[sid - 1].arrays()["perm"].clone()
+    ctx = tns._ctx
+    ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)  # noqa: E731
+    fp = None if recompute else disp
+    fd = None if recompute else dist
+    xp = xc if recompute else None
+    want = torch.empty((n, 3), device="cuda")
+    ctx.check(ctx.lib.oct_edges_diff_backward_ordered(ctx.handle, 3, 0, n, m, ptr(snd), ptr(rcv), ptr(fp), ptr(fd),
+                                                      ptr(xp), ptr(dd), ptr(dn), float(r), ptr(want), ptr(order)),
+              "ordered")
+    got = torch.empty((n, 3), device="cuda")
+    ctx.check(ctx.lib.oct_edges_diff_backward_mirror(ctx.handle, 3, 0, n, m, ptr(snd), ptr(rcv), ptr(mir), ptr(fp),
+                                                     ptr(fd), ptr(xp), ptr(dd), ptr(dn), float(r), ptr(got),
+                                                     ptr(order)), "mirror")
+    assert torch.equal(got, want)
+    bad = mir.clone()
+    bad[m // 2] = -1
+    bad[m // 3] = m + 7
+    got2 = torch.empty((n, 3), device="cuda")
+    ctx.check(ctx.lib.oct_edges_diff_backward_mirror(ctx.handle, 3, 0, n, m, ptr(snd), ptr(rcv), ptr(bad), ptr(fp),
+                                                     ptr(fd), ptr(xp), ptr(dd), ptr(dn), float(r), ptr(got2),
+                                                     ptr(order)), "mirror fallback")
+    assert torch.equal(got2, want)

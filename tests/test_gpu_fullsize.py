@@ -2,11 +2,9 @@
 
 The 1M-point SPH time step and the 2M-point differentiable configuration are
 compared with the oracle array for array.  The 4M-point nonuniform 2D
-configuration (1.55 G edges, ~37 GB of COO) is beyond the oracle's host
-memory, so it is checked through size-independent properties: the neighbor
-sets of sampled queries against a brute force in the reference's FP32
-operation order (d2 = dx*dx + dy*dy, dx = x_t - x_q), the offsets against
-the segment lengths, and the symmetry of the self-pair COO on the sample."""
+configuration (1.55 G edges, ~31 GB of COO) is compared with the oracle in
+slices of queries, each slice the part of the COO those queries own; the
+same shape at a larger radius runs past 2^31 edges."""
 import os
 import sys
 
@@ -53,50 +51,87 @@ def test_uniform_2m(ob, oracle_mod):
     assert_edges_equal(e, oracle_mod.build_edges(oracle_mod.build_tree(x, r), x, exclude_self=True), tns)
 
 
-def test_nonuniform_2d_4m_properties(ob):
-    x = wl.gaussian_mixture_2d(4_000_000, 64, 2026)
-    r = np.float32(0.002)
+def _assert_slices_equal(e, ot, x, lo, hi, oracle_mod, nthreads=0):
+    """Queries lo..hi-1 (0-based) own one contiguous slice of the GPU COO; it
+    must equal the oracle's COO for those queries, array for array."""
+    part = oracle_mod.build_edges(ot, x, exclude_self=True, query_range=(lo, hi), nthreads=nthreads)
+    q = torch.tensor([lo + 1, hi + 1], dtype=torch.int32, device="cuda")
+    a, b = (int(v) for v in torch.searchsorted(e.receivers, q))
+    assert b - a == len(part["senders"]), f"queries [{lo}, {hi}): {b - a} edges, oracle {len(part['senders'])}"
+    assert np.array_equal(e.senders[a:b].cpu().numpy(), part["senders"]), f"senders of queries [{lo}, {hi})"
+    assert np.array_equal(e.receivers[a:b].cpu().numpy(), part["receivers"]), f"receivers of queries [{lo}, {hi})"
+    assert np.array_equal(e.rel_displacement[:, a:b].t().cpu().numpy(), part["rel_displacement"]), \
+        f"rel_displacement of queries [{lo}, {hi})"
+    assert np.array_equal(e.rel_dist_norm[0, a:b].cpu().numpy(), part["rel_dist_norm"]), \
+        f"rel_dist_norm of queries [{lo}, {hi})"
+    return a, b
+
+
+def _nonuniform_2d_run(ob, x, r):
     tns = ob.TNS(torch.float32, ndims=2)
     ob.set_search_radius_(tns, r)
-    xd = torch.from_numpy(x).cuda()
-    sid = ob.add_point_set_(tns, xd.t())
+    sid = ob.add_point_set_(tns, torch.from_numpy(x).cuda().t())
     ob.set_active_search_(tns, sid, sid)
     ob.run_(tns)
     e = ob.build_edges(tns, sid, sid)
     ob.synchronize(tns)
+    return tns, sid, e
+
+
+def test_nonuniform_2d_4m_bit_exact(ob, oracle_mod):
+    """The 4M-point nonuniform 2D configuration (seed 2026, r = 0.002): the
+    tree and all 1,547,624,876 edges -- senders, receivers, rel_displacement
+    and rel_dist_norm, in order -- equal the oracle's.  The COO (~31 GB) is
+    compared in slices of 250,000 queries, which the oracle emits one at a
+    time against the same tree."""
+    x = wl.gaussian_mixture_2d(4_000_000, 64, 2026)
+    r = np.float32(0.002)
+    tns, sid, e = _nonuniform_2d_run(ob, x, r)
     E = e.senders.numel()
     assert E == 1_547_624_876
+    ot = oracle_mod.build_tree(x, r)
+    assert_tree_equal(tns.trees[sid - 1], ot)
+    covered = 0
+    for lo in range(0, len(x), 250_000):
+        a, b = _assert_slices_equal(e, ot, x, lo, min(len(x), lo + 250_000), oracle_mod)
+        assert a == covered
+        covered = b
+    assert covered == E
+    del e, tns
+    torch.cuda.empty_cache()
+
+
+def test_nonuniform_2d_above_2_31_edges(ob, oracle_mod):
+    """The same 4M-point shape at r = 0.0025: more than 2^31 - 1 edges, which
+    the reference's Int32 edge count and scan cannot represent
+    (src/types.jl:89, src/cpu/edges_cpu.jl:209-212).  The int64 offsets must
+    place every query's edges contiguously and in query order across edge
+    index 2^31; the slices at the start, around edge 2^31 and at the end equal
+    the oracle's."""
+    x = wl.gaussian_mixture_2d(4_000_000, 64, 2026)
+    r = np.float32(0.0025)
+    tns, sid, e = _nonuniform_2d_run(ob, x, r)
+    E = e.senders.numel()
+    assert E > 2**31
     rcv = e.receivers
-    # segment starts of sampled receivers, by binary search on the sorted receivers
-    rng = np.random.default_rng(7)
-    qs = torch.from_numpy(np.sort(rng.choice(len(x), 256, replace=False)) + 1).int().cuda()
-    lo = torch.searchsorted(rcv, qs, right=False)
-    hi = torch.searchsorted(rcv, qs, right=True)
-    assert torch.all(rcv[:-1] <= rcv[1:]) if E < 2**31 else True
-    r2 = torch.tensor(r * r, dtype=torch.float32, device="cuda")
-    for k in range(len(qs)):
-        i = int(qs[k]) - 1
-        dx = xd[:, 0] - xd[i, 0]  # x_t - x_q, FP32
-        dy = xd[:, 1] - xd[i, 1]
-        d2 = dx * dx + dy * dy
-        want = torch.nonzero(d2 <= r2).reshape(-1) + 1
-        want = want[want != i + 1]
-        got = e.senders[int(lo[k]):int(hi[k])]
-        assert got.numel() == want.numel(), f"query {i + 1}"
-        assert torch.equal(torch.sort(got).values, want.int()), f"query {i + 1}"
-        # symmetry: every neighbor j lists i
-        js = got[:64].long()
-        jl = torch.searchsorted(rcv, js.int(), right=False)
-        jh = torch.searchsorted(rcv, js.int(), right=True)
-        for a, b in zip(jl.tolist(), jh.tolist()):
-            assert bool((e.senders[a:b] == i + 1).any())
-    # features of one segment equal their FP32 definition
-    k = 0
-    i = int(qs[k]) - 1
-    seg = slice(int(lo[k]), int(hi[k]))
-    j = e.senders[seg].long() - 1
-    inv = torch.tensor(1, dtype=torch.float32, device="cuda") / torch.tensor(r, device="cuda")
-    dx = xd[j] - xd[i]
-    assert torch.equal(e.rel_displacement[:, seg].t(), (-dx) * inv)
-    d2 = dx[:, 0] * dx[:, 0] + dx[:, 1] * dx[:, 1]
-    assert torch.equal(e.rel_dist_norm[0, seg], torch.sqrt(d2) * inv)
+    n = len(x)
+    # receivers never decrease: each query's edges contiguous, in query order
+    step = 1 << 28
+    for a in range(0, E - 1, step):
+        b = min(E, a + step + 1)
+        assert bool((rcv[a + 1:b] >= rcv[a:b - 1]).all()), f"receivers decrease in [{a}, {b})"
+    assert int(rcv[0]) >= 1 and int(rcv[-1]) <= n
+    # edge counts per query agree with the senders' own per-query totals
+    counts = torch.bincount(rcv.long() - 1, minlength=n)
+    assert int(counts.sum()) == E
+    ot = oracle_mod.build_tree(x, r)
+    q_mid = int(rcv[2**31]) - 1  # the query owning edge 2^31
+    spans = [(0, 100_000), (max(0, q_mid - 50_000), min(n, q_mid + 50_000)), (n - 100_000, n)]
+    for lo, hi in spans:
+        a, b = _assert_slices_equal(e, ot, x, lo, hi, oracle_mod)
+        if lo == spans[1][0]:
+            assert a < 2**31 < b
+        if hi == n:
+            assert b == E
+    del e, tns, counts
+    torch.cuda.empty_cache()

@@ -213,3 +213,24 @@ def test_rrule_matches_central_differences(oracle_mod):
             return loss(c)
         fd.flat[k] = (-f(2 * eps) + 8 * f(eps) - 8 * f(-eps) + f(-2 * eps)) / (12 * eps)
     np.testing.assert_allclose(g, fd, rtol=1e-4, atol=1e-7)
+
+
+@pytest.mark.parametrize("ndims,r", [(3, 0.06), (2, 0.02)])
+def test_query_range_is_the_slice_of_the_full_coo(oracle_mod, ndims, r):
+    """The oracle's query-range COO (used to compare COOs too large for host
+    memory slice by slice) equals the slice of the whole COO those queries
+    own, offsets included."""
+    rng = np.random.default_rng(500 + ndims)
+    x = rng.random((6000, ndims)).astype(np.float32)
+    r = np.float32(r)
+    t = oracle_mod.build_tree(x, r)
+    full = oracle_mod.build_edges(t, x, exclude_self=True)
+    off = full["offsets"]
+    for lo, hi in [(0, 6000), (0, 1), (17, 1033), (2500, 2500), (5999, 6000), (1234, 5000)]:
+        part = oracle_mod.build_edges(t, x, exclude_self=True, query_range=(lo, hi))
+        a, b = off[lo], off[hi]
+        for k in ("senders", "receivers", "rel_displacement", "rel_dist_norm"):
+            assert np.array_equal(part[k], full[k][a:b]), (lo, hi, k)
+        assert np.array_equal(part["offsets"], off[lo:hi + 1] - a)
+    with pytest.raises(ValueError):
+        oracle_mod.build_edges(t, x, query_range=(10, 6001))
