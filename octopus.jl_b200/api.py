@@ -574,6 +574,7 @@ class _EdgesDiff(torch.autograd.Function):
         # buffer, ext/OctopusCUDAChainRulesCoreExt.jl:21-32) together with
         # each edge's mirror index, which the backward pass uses.
         n_edges = 0
+        _pair_index(tns, set_id, set_id)  # the pair must be registered, as for build_edges
         got = _count_pair(tns, set_id, set_id, "build_edges_diff")
         if got is not None:
             lc, qtree, ttree, excl, n_edges = got
