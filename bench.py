@@ -211,11 +211,11 @@ def tuning_used(ob, lib, ctx, ndims, n, nbrs):
     row = C.c_int64(-1)
     lib.oct_ctx_get_option(ctx.handle, ob._lib.STAT_TUNING_ROW, C.byref(row))
     table = os.environ.get("OCTOPUS_B200_TUNING", ob.api.TUNING_TABLE)
-    shapes = (C.c_int32 * 5)()
+    shapes = (C.c_int32 * 6)()
     r2 = C.c_int32(-1)
     st = lib.oct_tuning_select((table if table and os.path.exists(table) else "").encode(), ndims, 0, int(n),
                                float(nbrs), shapes, C.byref(r2))
-    names = ("max_seg", "multi_pop", "fill_chunk", "group_cap", "sub_boxes")
+    names = ("max_seg", "multi_pop", "fill_chunk", "group_cap", "sub_boxes", "prefetch")
     return {"table": os.path.relpath(table, ROOT) if table and os.path.exists(table) else None,
             "row": int(row.value), "shapes": dict(zip(names, list(shapes))) if st == 0 else None}
 

@@ -345,6 +345,8 @@ OCT_API int oct_edges_count_noalloc(oct_ctx* ctx, const oct_tree* query, const o
  *   OCT_OPT_GROUP_CAP      query points per traversal group, 8..32 (32), set at the build
  *   OCT_OPT_SUB_BOXES      boxes a group's queries are split into (runs of 32/k lanes)
  *                          for the test that skips distant target points: 1, 2 or 4 (1)
+ *   OCT_OPT_PREFETCH       the traversal prefetches into L1 what it reads next (the next
+ *                          leaf chunk's points, the next node's children): 1 off, 2 on (off)
  * Read-only (oct_ctx_get_option):
  *   OCT_STAT_TUNING_ROW       tuning-table row the last count or build used (-1 = defaults)
  *   OCT_STAT_BUILD_ATTEMPTS   topology attempts of the last build (1 = none retried)
@@ -361,6 +363,7 @@ enum {
     OCT_OPT_FILL_CHUNK = 8,
     OCT_OPT_GROUP_CAP = 9,
     OCT_OPT_SUB_BOXES = 10,
+    OCT_OPT_PREFETCH = 11,
     OCT_STAT_TUNING_ROW = 99,
     OCT_STAT_BUILD_ATTEMPTS = 100,
     OCT_STAT_RECORD_OVERFLOW = 101,
@@ -372,7 +375,7 @@ OCT_API int oct_ctx_get_option(const oct_ctx* ctx, int option, int64_t* value);
 /* Load the kernel-shape table written by the autotuner
  * (octopus.jl_b200/tune.py; the package ships octopus.jl_b200/tuning.tsv):
  * one row per line, "ndims dtype nlog2 nbr_log2 max_seg multi_pop fill_chunk
- * group_cap [sub_boxes]", '#' comments.  Each count (and each build, for group_cap) then
+ * group_cap [sub_boxes [prefetch]]", '#' comments.  Each count (and each build, for group_cap) then
  * uses the row of the same ndims and dtype nearest to its point count
  * (log2) and neighbors per point (log2 of 1 + the last count's average),
  * unless an option forces a shape.  NULL or "" unloads the table.  No
@@ -381,8 +384,8 @@ OCT_API int oct_ctx_get_option(const oct_ctx* ctx, int option, int64_t* value);
 OCT_API int oct_ctx_load_tuning(oct_ctx* ctx, const char* path);
 
 /* The selection of oct_ctx_load_tuning without a context or a device: the
- * shapes {max_seg, multi_pop, fill_chunk, group_cap, sub_boxes} the table at
- * `path` ("" = no table) gives a set of n points with nbrs_per_point neighbors per point
+ * shapes {max_seg, multi_pop, fill_chunk, group_cap, sub_boxes, prefetch} (six
+ * entries) the table at `path` ("" = no table) gives a set of n points with nbrs_per_point neighbors per point
  * (< 0: not known yet), and the row (-1 = defaults). */
 OCT_API int oct_tuning_select(const char* path, int ndims, int dtype, int64_t n, double nbrs_per_point,
                               int32_t* shapes, int32_t* row);

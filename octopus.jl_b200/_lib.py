@@ -33,6 +33,7 @@ OPT_MULTI_POP = 7
 OPT_FILL_CHUNK = 8
 OPT_GROUP_CAP = 9
 OPT_SUB_BOXES = 10
+OPT_PREFETCH = 11
 STAT_TUNING_ROW = 99
 STAT_BUILD_ATTEMPTS = 100
 STAT_RECORD_OVERFLOW = 101

@@ -74,16 +74,17 @@ bool parse_tuning(const char* path, std::vector<TuneRow>& rows, std::string& err
     while (std::fgets(line, sizeof line, f)) {
         ++lineno;
         if (char* h = std::strchr(line, '#')) *h = '\0';
-        int v[9];
+        int v[10];
         v[8] = 1;
+        v[9] = 0;
         char extra[2];
-        const int got = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %1s", &v[0], &v[1], &v[2], &v[3], &v[4],
-                                    &v[5], &v[6], &v[7], &v[8], extra);
+        const int got = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %1s", &v[0], &v[1], &v[2], &v[3], &v[4],
+                                    &v[5], &v[6], &v[7], &v[8], &v[9], extra);
         if (got <= 0) continue;  // blank or comment
-        const bool valid = (got == 8 || got == 9) && (v[0] == 2 || v[0] == 3) && (v[1] == 0 || v[1] == 1) &&
+        const bool valid = got >= 8 && got <= 10 && (v[0] == 2 || v[0] == 3) && (v[1] == 0 || v[1] == 1) &&
                            v[2] >= 0 && v[2] <= 40 && v[3] >= 0 && v[3] <= 40 && v[4] >= 1 && v[4] <= 16 &&
                            v[5] >= 1 && v[5] <= 4 && (v[6] == 32 || v[6] == 64 || v[6] == 128) && v[7] >= 8 &&
-                           v[7] <= 32 && (v[8] == 1 || v[8] == 2 || v[8] == 4);
+                           v[7] <= 32 && (v[8] == 1 || v[8] == 2 || v[8] == 4) && (v[9] == 0 || v[9] == 1);
         if (!valid) {
             err = std::string("tuning table ") + path + ": bad row at line " + std::to_string(lineno);
             ok = false;
@@ -99,6 +100,7 @@ bool parse_tuning(const char* path, std::vector<TuneRow>& rows, std::string& err
         r.tn.fill_chunk = v[6];
         r.tn.group_cap = v[7];
         r.tn.sub_boxes = v[8];
+        r.tn.prefetch = v[9];
         rows.push_back(r);
     }
     std::fclose(f);
@@ -138,6 +140,7 @@ Tuning Ctx::tuning_for(int ndims, int dtype, int64_t n, double nbrs) {
     if (tune_force.fill_chunk) tn.fill_chunk = tune_force.fill_chunk;
     if (tune_force.group_cap) tn.group_cap = tune_force.group_cap;
     if (tune_force.sub_boxes) tn.sub_boxes = tune_force.sub_boxes;
+    if (tune_force.prefetch) tn.prefetch = tune_force.prefetch - 1;
     return tn;
 }
 
@@ -607,6 +610,10 @@ OCT_API int oct_ctx_set_option(oct_ctx* ctx, int option, int64_t value) {
                 return oct::set_error(c, OCT_ERR_ARGUMENT, "sub_boxes must be 0, 1, 2 or 4");
             c.tune_force.sub_boxes = (int)value;
             return OCT_OK;
+        case OCT_OPT_PREFETCH:  // 0 = table, 1 = off, 2 = on
+            if (value < 0 || value > 2) return oct::set_error(c, OCT_ERR_ARGUMENT, "prefetch must be 0, 1 or 2");
+            c.tune_force.prefetch = (int)value;
+            return OCT_OK;
         default:
             return oct::set_error(c, OCT_ERR_ARGUMENT, "unknown or read-only option");
     }
@@ -626,6 +633,7 @@ OCT_API int oct_ctx_get_option(const oct_ctx* ctx, int option, int64_t* value) {
         case OCT_OPT_FILL_CHUNK: *value = c.tune_force.fill_chunk; return OCT_OK;
         case OCT_OPT_GROUP_CAP: *value = c.tune_force.group_cap; return OCT_OK;
         case OCT_OPT_SUB_BOXES: *value = c.tune_force.sub_boxes; return OCT_OK;
+        case OCT_OPT_PREFETCH: *value = c.tune_force.prefetch; return OCT_OK;
         case OCT_STAT_TUNING_ROW: *value = c.last_tune_row; return OCT_OK;
         case OCT_STAT_BUILD_ATTEMPTS: *value = c.last_attempts; return OCT_OK;
         case OCT_STAT_RECORD_OVERFLOW: *value = c.rec_overflow; return OCT_OK;
@@ -661,6 +669,7 @@ OCT_API int oct_tuning_select(const char* path, int ndims, int dtype, int64_t n,
     shapes[2] = tn.fill_chunk;
     shapes[3] = tn.group_cap;
     shapes[4] = tn.sub_boxes;
+    shapes[5] = tn.prefetch;
     return OCT_OK;
 }
 

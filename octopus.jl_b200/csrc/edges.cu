@@ -86,6 +86,10 @@ __device__ __forceinline__ void write_edge(int64_t k, const SPt<T, D>& t, const 
     rdist[k] = mul_rn(sqrt_rn(d2), inv_r);
 }
 
+// Starts moving the line holding p into L1 (no value is returned; p must lie
+// inside an allocation).
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 // Radius and index base of the point set (cloud) holding sorted position p.
 template <class T>
 __device__ __forceinline__ void cloud_params(const Batch& bt, int64_t p, T& r2, T& inv_r, int32_t& start_node,
@@ -114,7 +118,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ ocount,
     int2* __restrict__ recs, int64_t rec_cap, uint16_t* __restrict__ rcount, uint8_t* __restrict__ gflag, Batch bt,
-    unsigned long long* __restrict__ stats, int max_seg, int multi_pop, int nbox) {
+    unsigned long long* __restrict__ stats, int max_seg, int multi_pop, int nbox, int prefetch) {
     constexpr bool STAGE = PASS == EP_FILL;
     constexpr bool STATS = PASS == EP_STATS;
     long long st_t0 = 0, st_leaf = 0, st_pairs = 0;
@@ -291,6 +295,18 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
                 }
                 const unsigned keep = __ballot_sync(0xffffffffu, near);
                 __syncwarp();
+                if (prefetch && c0 + kStage >= nb) {
+                    // The next chunk's points (the leaves now at the stack top)
+                    // start their way into L1 while this chunk's pairs are tested.
+                    int acc = 0, ppos = -1;
+                    for (int j = sp - 1; j >= 0 && acc < 32; --j) {
+                        const int2 nx = stack[w][j];
+                        if (nx.y <= 0) break;
+                        if (lane >= acc && lane < acc + nx.y) ppos = (nx.x & 0x7fffffff) + (lane - acc);
+                        acc += nx.y;
+                    }
+                    if (ppos >= 0) prefetch_l1(tpts + ppos);
+                }
                 unsigned hm = 0;
                 long long st_p0 = 0;
                 if constexpr (STATS) {
@@ -432,6 +448,16 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
             }
             sp += __popc(m);
             __syncwarp();
+            if (prefetch && sp > 0) {
+                // what the next pop reads: an internal node's children, or a leaf's points
+                const int2 nx = stack[w][sp - 1];
+                const int32_t a = nx.x & 0x7fffffff;
+                if (nx.y <= 0) {
+                    if (lane < __popc((unsigned)(-nx.y))) prefetch_l1(tnode + a + lane);
+                } else if (lane < nx.y) {
+                    prefetch_l1(tpts + a + lane);
+                }
+            }
         }
     }
     if (STAGE) flush(true);
@@ -841,13 +867,13 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
                 nullptr, nullptr, nullptr, nullptr, (int*)(ctx.total.as<int64_t>() + 1), ctx.recs.as<int2>(),
                 ctx.rec_cap, ctx.rcount.as<uint16_t>(), ctx.gflag.as<uint8_t>(), t.batch(), nullptr, tn.max_seg,
-                tn.multi_pop, tn.sub_boxes);
+                tn.multi_pop, tn.sub_boxes, tn.prefetch);
         else
             k_edges<T, D, EP_COUNT><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
                 nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr,
-                tn.max_seg, tn.multi_pop, tn.sub_boxes);
+                tn.max_seg, tn.multi_pop, tn.sub_boxes, tn.prefetch);
         ctx.kernel_launches += 1;
     }
     {
@@ -943,7 +969,7 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
             t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r, exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(),
             senders, receivers, (T*)rel_disp, (T*)rel_dist, ctx.dstatus.as<int>(),
             ctx.rec_cap ? ctx.recs.as<int2>() : nullptr, ctx.rec_cap, nullptr, ctx.gflag.as<uint8_t>(), t.batch(),
-            nullptr, tn.max_seg, tn.multi_pop, tn.sub_boxes);
+            nullptr, tn.max_seg, tn.multi_pop, tn.sub_boxes, tn.prefetch);
         ctx.kernel_launches += 1;
     }
     return cuda_status(ctx, cudaGetLastError(), "edge fill launch");
@@ -968,7 +994,7 @@ cudaError_t count_into_typed(const Tree& q, const Tree& t, bool exclude_self, in
     k_edges<T, D, EP_COUNT><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
         q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
         t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr, kMaxSeg, kMultiPop, 1);
+        nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr, kMaxSeg, kMultiPop, 1, 0);
     return cudaGetLastError();
 }
 
@@ -981,7 +1007,7 @@ int stats_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, unsig
         q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
         t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr,
         nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), stats_dev, tn.max_seg,
-        tn.multi_pop, tn.sub_boxes);
+        tn.multi_pop, tn.sub_boxes, tn.prefetch);
     ctx.kernel_launches += 1;
     return cuda_status(ctx, cudaGetLastError(), "traversal statistics launch");
 }

@@ -32,6 +32,7 @@ struct Tuning {
     int fill_chunk = 64;  // edges per bulk-copy chunk of the fill (32, 64 or 128)
     int group_cap = 32;   // query points per traversal group, set at the build (8..32)
     int sub_boxes = 1;    // boxes a group's queries are split into for the target test (1, 2 or 4)
+    int prefetch = 0;     // 1: the traversal prefetches the next chunk's points / children into L1
 };
 
 // One row of a tuning table: the shapes measured best for point sets of
@@ -42,9 +43,9 @@ struct TuneRow {
 };
 
 // Parses a tuning table (one row per line: ndims dtype nlog2 nbr_log2 max_seg
-// multi_pop fill_chunk group_cap [sub_boxes]; '#' starts a comment).  Returns false when
+// multi_pop fill_chunk group_cap [sub_boxes [prefetch]]; '#' starts a comment).  Returns false when
 // the file cannot be read or a row is malformed.  A ninth value, sub_boxes,
-// is optional (1 when absent).
+// and a tenth, prefetch, are optional (1 and 0 when absent).
 bool parse_tuning(const char* path, std::vector<TuneRow>& rows, std::string& err);
 // The row nearest to (n, neighbors per point) among those of the same ndims
 // and dtype (index into rows, -1 when none), and its shapes (defaults when none).
@@ -208,7 +209,7 @@ struct Ctx {
     // (0 = from the table), the shapes of the last count (used by its fill)
     // and the table row they came from (-1 = defaults).
     std::vector<TuneRow> tune_table;
-    Tuning tune_force{0, 0, 0, 0, 0};
+    Tuning tune_force{0, 0, 0, 0, 0, 0};
     Tuning plan_tuning;
     int last_tune_row = -1;
     Tuning tuning_for(int ndims, int dtype, int64_t n, double nbrs);

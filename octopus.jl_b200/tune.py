@@ -1,6 +1,7 @@
 """Autotuner of the kernel shapes (leaf chunks per traversal step, internal
 nodes expanded together, fill staging depth, query points per traversal
-group, sub-boxes of a group for the target test).
+group, sub-boxes of a group for the target test, L1 prefetch in the
+traversal).
 
     python octopus.jl_b200/tune.py [--out PATH] [--steps K] [--rounds R]
 
@@ -10,7 +11,7 @@ while the others are held, keeps the fastest (coordinate descent, R rounds),
 and writes one row per configuration to the table (default
 ``octopus.jl_b200/tuning.tsv``):
 
-    ndims dtype nlog2 nbr_log2 max_seg multi_pop fill_chunk group_cap sub_boxes
+    ndims dtype nlog2 nbr_log2 max_seg multi_pop fill_chunk group_cap sub_boxes prefetch
 
 keyed by the configuration's point count (log2) and neighbors per point
 (log2 of 1 + the average), the key the library uses to pick a row
@@ -25,8 +26,6 @@ import os
 import sys
 import time
 
-import numpy as np
-
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_TABLE = os.path.join(HERE, "tuning.tsv")
 
@@ -37,8 +36,9 @@ SHAPES = [
     ("multi_pop", 7, (1, 2, 4)),
     ("fill_chunk", 8, (32, 64, 128)),
     ("sub_boxes", 10, (1, 2, 4)),
+    ("prefetch", 11, (0, 1)),
 ]
-DEFAULTS = {"group_cap": 32, "max_seg": 16, "multi_pop": 4, "fill_chunk": 64, "sub_boxes": 1}
+DEFAULTS = {"group_cap": 32, "max_seg": 16, "multi_pop": 4, "fill_chunk": 64, "sub_boxes": 1, "prefetch": 0}
 
 
 def _package():
@@ -89,7 +89,10 @@ class Runner:
 
     def force(self, shapes):
         for name, opt, _ in SHAPES:
-            self.ctx.check(self.ctx.lib.oct_ctx_set_option(self.ctx.handle, opt, int(shapes.get(name, 0))), name)
+            v = shapes.get(name)
+            # 0 hands a shape back to the table; prefetch is forced as 1 (off) / 2 (on)
+            v = 0 if v is None else (v + 1 if name == "prefetch" else v)
+            self.ctx.check(self.ctx.lib.oct_ctx_set_option(self.ctx.handle, opt, int(v)), name)
 
     def step(self):
         x = self.xs[self.k % len(self.xs)]
@@ -150,23 +153,23 @@ def write_table(path, rows, device):
     with open(path, "w") as f:
         f.write("# Kernel shapes per workload, measured by octopus.jl_b200/tune.py on " + device + " "
                 + time.strftime("%Y-%m-%d") + "\n")
-        f.write("# ndims dtype nlog2 nbr_log2 max_seg multi_pop fill_chunk group_cap sub_boxes"
+        f.write("# ndims dtype nlog2 nbr_log2 max_seg multi_pop fill_chunk group_cap sub_boxes prefetch"
                 "   # configuration: step ms with these shapes / with the defaults\n")
         for (ndims, dtype, nlog2, nbr), s, name, base_ms, ms in rows:
             f.write(f"{ndims} {dtype} {nlog2} {nbr} {s['max_seg']} {s['multi_pop']} {s['fill_chunk']} "
-                    f"{s['group_cap']} {s['sub_boxes']}   # {name}: {ms:.4f} / {base_ms:.4f} ms\n")
+                    f"{s['group_cap']} {s['sub_boxes']} {s['prefetch']}   # {name}: {ms:.4f} / {base_ms:.4f} ms\n")
 
 
 def select(path, ndims, dtype, n, nbrs_per_point):
     """The shapes and row the library would pick from the table at `path`."""
     ob = _package()
     lib = ob._lib.load()
-    shapes = (C.c_int32 * 5)()
+    shapes = (C.c_int32 * 6)()
     row = C.c_int32(-2)
     st = lib.oct_tuning_select((path or "").encode(), ndims, dtype, n, float(nbrs_per_point), shapes, C.byref(row))
     if st != 0:
         raise ValueError(f"tuning table {path} could not be read")
-    return dict(zip(("max_seg", "multi_pop", "fill_chunk", "group_cap", "sub_boxes"), list(shapes))), int(row.value)
+    return dict(zip(("max_seg", "multi_pop", "fill_chunk", "group_cap", "sub_boxes", "prefetch"), list(shapes))), int(row.value)
 
 
 if __name__ == "__main__":

@@ -8,8 +8,8 @@ import pytest
 
 from conftest import ROOT
 
-TABLE = """# ndims dtype nlog2 nbr_log2 max_seg multi_pop fill_chunk group_cap [sub_boxes]
-3 0 16 4 8 2 32 24 2  # 100k points, ~25 neighbors
+TABLE = """# ndims dtype nlog2 nbr_log2 max_seg multi_pop fill_chunk group_cap [sub_boxes [prefetch]]
+3 0 16 4 8 2 32 24 2 1  # 100k points, ~25 neighbors
 3 0 19 5 16 4 64 32   # 1M points, ~33 neighbors (sub_boxes absent: 1)
 2 0 21 8 4 1 128 16 4 # 4M points 2D, ~390 neighbors
 3 1 16 4 1 1 64 8 1   # Float64
@@ -19,7 +19,7 @@ TABLE = """# ndims dtype nlog2 nbr_log2 max_seg multi_pop fill_chunk group_cap [
 def select(ob, path, ndims, dtype, n, nbrs):
     import ctypes as C
     lib = ob._lib.load()
-    shapes = (C.c_int32 * 5)()
+    shapes = (C.c_int32 * 6)()
     row = C.c_int32(-9)
     st = lib.oct_tuning_select(path.encode(), ndims, dtype, n, float(nbrs), shapes, C.byref(row))
     return st, list(shapes), row.value
@@ -28,21 +28,22 @@ def select(ob, path, ndims, dtype, n, nbrs):
 def test_nearest_row_of_the_same_kind(ob, tmp_path):
     p = tmp_path / "t.tsv"
     p.write_text(TABLE)
-    assert select(ob, str(p), 3, 0, 100_000, 25.6) == (0, [8, 2, 32, 24, 2], 0)
-    assert select(ob, str(p), 3, 0, 1_000_000, 28.3) == (0, [16, 4, 64, 32, 1], 1)
-    assert select(ob, str(p), 3, 0, 2_000_000, 14.3) == (0, [16, 4, 64, 32, 1], 1)  # nearer in size than in neighbors
-    assert select(ob, str(p), 2, 0, 4_000_000, 387.0) == (0, [4, 1, 128, 16, 4], 2)
-    assert select(ob, str(p), 3, 1, 5_000, 0.5) == (0, [1, 1, 64, 8, 1], 3)
+    assert select(ob, str(p), 3, 0, 100_000, 25.6) == (0, [8, 2, 32, 24, 2, 1], 0)
+    assert select(ob, str(p), 3, 0, 1_000_000, 28.3) == (0, [16, 4, 64, 32, 1, 0], 1)
+    assert select(ob, str(p), 3, 0, 2_000_000, 14.3) == (0, [16, 4, 64, 32, 1, 0], 1)  # nearer in size than in neighbors
+    assert select(ob, str(p), 2, 0, 4_000_000, 387.0) == (0, [4, 1, 128, 16, 4, 0], 2)
+    assert select(ob, str(p), 3, 1, 5_000, 0.5) == (0, [1, 1, 64, 8, 1, 0], 3)
     # no row of that kind: the built-in defaults
-    assert select(ob, str(p), 2, 1, 1000, 10) == (0, [16, 4, 64, 32, 1], -1)
+    assert select(ob, str(p), 2, 1, 1000, 10) == (0, [16, 4, 64, 32, 1, 0], -1)
     # neighbors not known yet (before a first count): keyed as ~15 per point
-    assert select(ob, str(p), 3, 0, 100_000, -1) == (0, [8, 2, 32, 24, 2], 0)
+    assert select(ob, str(p), 3, 0, 100_000, -1) == (0, [8, 2, 32, 24, 2, 1], 0)
 
 
 def test_no_table_and_bad_tables(ob, tmp_path):
-    assert select(ob, "", 3, 0, 100_000, 25) == (0, [16, 4, 64, 32, 1], -1)
+    assert select(ob, "", 3, 0, 100_000, 25) == (0, [16, 4, 64, 32, 1, 0], -1)
     for bad in ("3 0 16 4 8 2 32\n", "3 0 16 4 8 2 48 24\n", "3 0 16 4 8 9 32 24\n", "4 0 16 4 8 2 32 24\n",
-                "3 0 16 4 8 2 32 24 3\n", "3 0 16 4 8 2 32 24 2 9\n"):
+                "3 0 16 4 8 2 32 24 3\n", "3 0 16 4 8 2 32 24 2 9\n",
+                "3 0 16 4 8 2 32 24 2 0 5\n"):
         p = tmp_path / "bad.tsv"
         p.write_text(bad)
         st, _, _ = select(ob, str(p), 3, 0, 1000, 1)
