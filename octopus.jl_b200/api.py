@@ -571,8 +571,9 @@ class _EdgesDiff(torch.autograd.Function):
     @staticmethod
     def forward(ctx, coords, tns, set_id, radius, recompute):
         # The primal writes fresh arrays (the reference copies build_edges'
-        # buffer, ext/OctopusCUDAChainRulesCoreExt.jl:21-32) together with
-        # each edge's mirror index, which the backward pass uses.
+        # buffer, ext/OctopusCUDAChainRulesCoreExt.jl:21-32).  The backward
+        # pass finds each edge's mirror itself: searching the sender's
+        # segment there costs less than writing mirror indices here.
         n_edges = 0
         _pair_index(tns, set_id, set_id)  # the pair must be registered, as for build_edges
         got = _count_pair(tns, set_id, set_id, "build_edges_diff")
@@ -585,10 +586,9 @@ class _EdgesDiff(torch.autograd.Function):
         rcv = torch.empty(n_edges, dtype=torch.int32, device=dev)
         disp_rows = torch.empty((n_edges, tns.ndims), dtype=tns.T, device=dev)
         dist = torch.empty((1, n_edges), dtype=tns.T, device=dev)
-        mirror = torch.empty(n_edges, dtype=torch.int32, device=dev)
         if n_edges > 0:
-            lc.check(lc.lib.oct_edges_fill_diff(lc.handle, ttree.handle, _ptr(snd), _ptr(rcv), _ptr(disp_rows),
-                                                _ptr(dist), _ptr(mirror), n_edges), "build_edges_diff")
+            lc.check(lc.lib.oct_edges_fill(lc.handle, qtree.handle, ttree.handle, excl, _ptr(snd), _ptr(rcv),
+                                           _ptr(disp_rows), _ptr(dist), n_edges), "build_edges_diff")
         disp = disp_rows.t()  # (D, E) column-major
         ctx.tns = tns
         ctx.radius = float(radius)
@@ -609,9 +609,9 @@ class _EdgesDiff(torch.autograd.Function):
         if ctx.recompute:
             # Keep only the indices and the coordinates: the backward pass
             # recomputes the features (memory-lean mode).
-            ctx.save_for_backward(snd, rcv, mirror, colmajor(coords.detach()), order)
+            ctx.save_for_backward(snd, rcv, colmajor(coords.detach()), order)
         else:
-            ctx.save_for_backward(snd, rcv, mirror, disp, dist, order)
+            ctx.save_for_backward(snd, rcv, disp, dist, order)
         ctx.mark_non_differentiable(snd, rcv)
         return snd, rcv, disp, dist
 
@@ -627,14 +627,14 @@ class _EdgesDiff(torch.autograd.Function):
         lc = tns._ctx
         lc.bind_stream()
         if ctx.recompute:
-            snd, rcv, mirror, xc, order = ctx.saved_tensors
+            snd, rcv, xc, order = ctx.saved_tensors
             disp_p, dist_p, xc_p = None, None, _ptr(xc)
         else:
-            snd, rcv, mirror, disp, dist, order = ctx.saved_tensors
+            snd, rcv, disp, dist, order = ctx.saved_tensors
             disp_p, dist_p, xc_p = _ptr(disp.t()), _ptr(dist), None
-        lc.check(lc.lib.oct_edges_diff_backward_mirror(
-            lc.handle, d, _dtype_code(T), n, snd.numel(), _ptr(snd), _ptr(rcv), _ptr(mirror), disp_p, dist_p, xc_p,
-            _ptr(dd), _ptr(dn), ctx.radius, _ptr(grad), _ptr(order) if order.numel() == n else None),
+        lc.check(lc.lib.oct_edges_diff_backward_ordered(
+            lc.handle, d, _dtype_code(T), n, snd.numel(), _ptr(snd), _ptr(rcv), disp_p, dist_p, xc_p, _ptr(dd),
+            _ptr(dn), ctx.radius, _ptr(grad), _ptr(order) if order.numel() == n else None),
             "build_edges_diff pullback")
         return grad.t(), None, None, None, None
 

@@ -229,7 +229,7 @@ OCT_API int oct_ctx_destroy(oct_ctx* ctx) {
     using oct::release;
     for (auto* b : {&ctx->c.counts, &ctx->c.offsets, &ctx->c.scan_tmp, &ctx->c.total, &ctx->c.dkeys[0],
                     &ctx->c.dkeys[1], &ctx->c.dvals[0], &ctx->c.dvals[1], &ctx->c.dhist, &ctx->c.dsort_tmp, &ctx->c.droff,
-                    &ctx->c.dsoff, &ctx->c.dstatus, &ctx->c.dredge, &ctx->c.dterm, &ctx->c.dseg, &ctx->c.tstats, &ctx->c.recs, &ctx->c.rcount, &ctx->c.gflag})
+                    &ctx->c.dsoff, &ctx->c.dstatus, &ctx->c.dredge, &ctx->c.dseg, &ctx->c.tstats, &ctx->c.recs, &ctx->c.rcount, &ctx->c.gflag})
         release(*b);
     if (ctx->c.total_host) cudaFreeHost(ctx->c.total_host);
     for (auto& r : ctx->c.prof) {

@@ -491,11 +491,14 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
 
 // Fill pass from the records, in original index order.  Warp v writes the
 // edges of queries 32v .. 32v+31, which own one contiguous range [K0, K1) of
-// the COO.  The warp takes its queries one at a time, lanes over the query's
-// edges: a round of up to 32 records is loaded (one per lane) and scanned by
-// hit count, and each lane finds its edge's record by a binary search over the
-// scanned counts (shuffles) and its point as the k-th set bit of the record's
-// mask.  The query's coordinates, index and radius are warp-uniform.
+// the COO, query after query, each query's edges in record order.  The warp
+// takes the records of all its queries as one flat list, 32 per round (one per
+// lane, the record's query found by a binary search of the queries' record
+// counts), scans their hit counts, and then writes the round's hits with the
+// lanes on consecutive hits, two per lane in flight: each lane finds its hit's
+// record by a binary search of the scanned counts (shuffles), its point as the
+// k-th set bit of the record's mask, and its query's coordinates, index and
+// radius by shuffles from the query's lane.
 //
 // Output goes through a per-warp ring of NCH chunks of CHUNK edges in shared
 // memory, one array per COO array, in the COO's own layout; a completed chunk
@@ -559,7 +562,10 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int32_t* __restrict__ twins,
     int* __restrict__ status, Batch bt, int bulk_ok) {
     constexpr int RING = CHUNK * NCH;
-    static_assert(CHUNK % 32 == 0 && (RING & (RING - 1)) == 0 && NCH >= 2, "ring shape");
+    constexpr int U = 2;                                  // hits per lane in flight
+    constexpr int SUB = 32 * U;                           // hits written per sub-round
+    constexpr int SPAN = (SUB - 1 + CHUNK - 1) / CHUNK;   // chunk boundaries a sub-round may cross
+    static_assert(CHUNK % 32 == 0 && (RING & (RING - 1)) == 0 && NCH - 1 - SPAN >= 0, "ring shape");
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ __align__(128) unsigned char fill_smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -590,6 +596,23 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
     T r2 = T(0), ir = inv_r;
     int32_t start_node = 0, base = 0;
     cloud_params<T>(bt, qp, r2, ir, start_node, base);
+    const int32_t qi = q.idx - base + 1;
+    // record and hit prefixes over the queries
+    int rincl = nr, eincl = ne;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int a = __shfl_up_sync(FULL, rincl, o);
+        const int b = __shfl_up_sync(FULL, eincl, o);
+        if (lane >= o) {
+            rincl += a;
+            eincl += b;
+        }
+    }
+    const int rexcl = rincl - nr;
+    const int total_r = __shfl_sync(FULL, rincl, 31);
+    // COO index of this query's flat hit 0 (flat hits count only the queries
+    // written here): hit F of query j is COO edge kq_j + F
+    const long long kq = k0 - (eincl - ne);
     const long long K0 = __shfl_sync(FULL, k0, 0);
     const long long K1 = __shfl_sync(FULL, kn, nval - 1);
     const bool bulk = bulk_ok && !__any_sync(FULL, over) && K1 - K0 >= 32;
@@ -639,116 +662,132 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
         }
     };
 
-    for (int j = 0; j < nval; ++j) {
-        const int nej = __shfl_sync(FULL, ne, j);
-        if (nej == 0) continue;  // warp-uniform
-        const int nrj = __shfl_sync(FULL, nr, j);
-        const long long kj = __shfl_sync(FULL, k0, j);
-        const int32_t qpj = __shfl_sync(FULL, qp, j);
-        const int32_t bj = __shfl_sync(FULL, base, j);
-        const int32_t qij = __shfl_sync(FULL, q.idx, j) - bj + 1;
-        const T irj = __shfl_sync(FULL, ir, j);
-        T px[D];
+    int fbase = 0;  // flat hits of the earlier record rounds
+    for (int r0 = 0; r0 < total_r; r0 += 32) {
+        // record r0 + lane and its query: the last query whose first record is <= it
+        const int rho = r0 + lane;
+        int jr = 0;
 #pragma unroll
-        for (int d = 0; d < D; ++d) px[d] = __shfl_sync(FULL, q.x[d], j);
-        const int2* rp = recs + (int64_t)qpj * rec_cap;
-        long long kq = kj;  // COO index of the query's next edge
-        for (int r0 = 0; r0 < nrj; r0 += 32) {
-            int2 rec = make_int2(0, 0);
-            if (r0 + lane < nrj) rec = rp[r0 + lane];
-            const int p = __popc((unsigned)rec.y);
-            int incl = p;
+        for (int st = 16; st > 0; st >>= 1) {
+            const int v = __shfl_sync(FULL, rexcl, jr + st);
+            if (v <= rho) jr += st;
+        }
+        const int32_t qpr = __shfl_sync(FULL, qp, jr);
+        const int rx0 = __shfl_sync(FULL, rexcl, jr);
+        int2 rec = make_int2(0, 0);
+        if (rho < total_r) rec = recs[(int64_t)qpr * rec_cap + (rho - rx0)];
+        const int p = __popc((unsigned)rec.y);
+        int hincl = p;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(FULL, incl, o);
-                if (lane >= o) incl += v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int a = __shfl_up_sync(FULL, hincl, o);
+            if (lane >= o) hincl += a;
+        }
+        const int hexcl = hincl - p;
+        const int tot = __shfl_sync(FULL, hincl, 31);
+        for (int e0 = 0; e0 < tot; e0 += SUB) {
+            const int cnt = min(SUB, tot - e0);
+            if (bulk) {
+                // the sub-round writes COO edges [K0 + fbase + e0, + cnt): its
+                // last chunk reuses the slots of that chunk minus NCH
+                const long long c = (K0 + fbase + e0 + cnt - 1 - kbase) / CHUNK;
+                if (c > cur_chunk) {
+                    if (c >= NCH) {
+                        if (lane == 0) bulk_wait_read<NCH - 1 - SPAN>();
+                        __syncwarp();
+                    }
+                    cur_chunk = c;
+                }
             }
-            const int tot = __shfl_sync(FULL, incl, 31);
-            const int excl = incl - p;
-            for (int e0 = 0; e0 < tot; e0 += 32) {
-                const int e = e0 + lane;
-                // the record lane holding hit e: the last lane whose first hit is <= e
+            SPt<T, D> tp[U];
+            int jq[U], tpos[U];
+            long long kk[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + 32 * u + lane;
                 int r = 0;
 #pragma unroll
                 for (int st = 16; st > 0; st >>= 1) {
-                    const int v = __shfl_sync(FULL, excl, r + st);
+                    const int v = __shfl_sync(FULL, hexcl, r + st);
                     if (v <= e) r += st;
                 }
                 const unsigned m = (unsigned)__shfl_sync(FULL, rec.y, r);
                 const int rx = __shfl_sync(FULL, rec.x, r);
-                const int er = __shfl_sync(FULL, excl, r);
-                const int cnt = min(32, tot - e0);
-                const long long kb = kq + e0;  // COO index of lane 0's edge
-                if (bulk) {
-                    const long long c = (kb + cnt - 1 - kbase) / CHUNK;
-                    if (c != cur_chunk) {
-                        // entering chunk c reuses the slots of chunk c - NCH
-                        if (c >= NCH) {
-                            if (lane == 0) bulk_wait_read<NCH - 2>();
-                            __syncwarp();
-                        }
-                        cur_chunk = c;
-                    }
-                }
-                if (lane < cnt) {
-                    const int tpos = rx + kth_set_bit(m, e - er);
-                    const SPt<T, D> t = tpts[tpos];
-                    const long long k = kb + lane;
-                    const int32_t snd = t.idx - bj + 1;
-                    T dv[D], dist = T(0);
-                    if (FEAT) {
-                        T diff[D];
-                        const T d2 = dist2<T, D>(t.x, px, diff);
-                        dist = mul_rn(sqrt_rn(d2), irj);
-#pragma unroll
-                        for (int d = 0; d < D; ++d) dv[d] = mul_rn(-diff[d], irj);
-                    }
-                    int32_t tw = -1;
-                    if (TWIN) {
-                        // the query's place among the target's hits, record by record
-                        const int2* rj = recs + (int64_t)tpos * rec_cap;
-                        const int nrt = rcount[tpos];
-                        int rank = 0;
-                        for (int rr = 0; rr < nrt; ++rr) {
-                            const int2 rc = rj[rr];
-                            const unsigned off = (unsigned)(qpj - rc.x);
-                            if (off < 32u && ((unsigned)rc.y >> off) & 1u) {
-                                tw = (int32_t)(offsets[t.idx] + rank + __popc((unsigned)rc.y & ((1u << off) - 1u)));
-                                break;
-                            }
-                            rank += __popc((unsigned)rc.y);
-                        }
-                        if (tw < 0) atomicOr(status, 4);
-                    }
-                    if (bulk) {
-                        const int sl = (int)((k - kbase) & (RING - 1));
-                        r_snd[sl] = snd;
-                        if (FEAT) {
-                            r_rcv[sl] = qij;
-                            r_dist[sl] = dist;
-#pragma unroll
-                            for (int d = 0; d < D; ++d) r_disp[D * sl + d] = dv[d];
-                        }
-                        if (TWIN) r_twin[sl] = tw;
-                        fence_smem_to_bulk();
-                    } else {
-                        senders[k] = snd;
-                        if (FEAT) {
-                            receivers[k] = qij;
-                            rdist[k] = dist;
-#pragma unroll
-                            for (int d = 0; d < D; ++d) rdisp[(long long)D * k + d] = dv[d];
-                        }
-                        if (TWIN) twins[k] = tw;
-                    }
-                }
-                if (bulk) {
-                    __syncwarp();
-                    flush(kb + cnt, false);
+                const int er = __shfl_sync(FULL, hexcl, r);
+                jq[u] = __shfl_sync(FULL, jr, r);
+                kk[u] = __shfl_sync(FULL, kq, jq[u]) + fbase + e;
+                tpos[u] = 0;
+                if (e < tot) {
+                    tpos[u] = rx + kth_set_bit(m, e - er);
+                    tp[u] = tpts[tpos[u]];
                 }
             }
-            kq += tot;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + 32 * u + lane;
+                T px[D];
+#pragma unroll
+                for (int d = 0; d < D; ++d) px[d] = __shfl_sync(FULL, q.x[d], jq[u]);
+                const T irq = __shfl_sync(FULL, ir, jq[u]);
+                const int32_t bq = __shfl_sync(FULL, base, jq[u]);
+                const int32_t qiq = __shfl_sync(FULL, qi, jq[u]);
+                const int32_t qpq = TWIN ? __shfl_sync(FULL, qp, jq[u]) : 0;
+                if (e >= tot) continue;
+                const long long k = kk[u];
+                const int32_t snd = tp[u].idx - bq + 1;
+                T dv[D], dist = T(0);
+                if (FEAT) {
+                    T diff[D];
+                    const T d2 = dist2<T, D>(tp[u].x, px, diff);
+                    dist = mul_rn(sqrt_rn(d2), irq);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) dv[d] = mul_rn(-diff[d], irq);
+                }
+                int32_t tw = -1;
+                if (TWIN) {
+                    // the query's place among the target's hits, record by record
+                    const int2* rj = recs + (int64_t)tpos[u] * rec_cap;
+                    const int nrt = rcount[tpos[u]];
+                    int rank = 0;
+                    for (int rr = 0; rr < nrt; ++rr) {
+                        const int2 rc = rj[rr];
+                        const unsigned off = (unsigned)(qpq - rc.x);
+                        if (off < 32u && ((unsigned)rc.y >> off) & 1u) {
+                            tw = (int32_t)(offsets[tp[u].idx] + rank + __popc((unsigned)rc.y & ((1u << off) - 1u)));
+                            break;
+                        }
+                        rank += __popc((unsigned)rc.y);
+                    }
+                    if (tw < 0) atomicOr(status, 4);
+                }
+                if (bulk) {
+                    const int sl = (int)((k - kbase) & (RING - 1));
+                    r_snd[sl] = snd;
+                    if (FEAT) {
+                        r_rcv[sl] = qiq;
+                        r_dist[sl] = dist;
+#pragma unroll
+                        for (int d = 0; d < D; ++d) r_disp[D * sl + d] = dv[d];
+                    }
+                    if (TWIN) r_twin[sl] = tw;
+                } else {
+                    senders[k] = snd;
+                    if (FEAT) {
+                        receivers[k] = qiq;
+                        rdist[k] = dist;
+#pragma unroll
+                        for (int d = 0; d < D; ++d) rdisp[(long long)D * k + d] = dv[d];
+                    }
+                    if (TWIN) twins[k] = tw;
+                }
+            }
+            if (bulk) {
+                fence_smem_to_bulk();
+                __syncwarp();
+                flush(K0 + fbase + e0 + cnt, false);
+            }
         }
+        fbase += tot;
     }
     if (bulk) {
         __syncwarp();

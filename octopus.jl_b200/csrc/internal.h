@@ -191,7 +191,6 @@ struct Ctx {
     // Adjoint scratch (diff.cu).
     DevBuf dkeys[2], dvals[2], dhist, dsort_tmp, droff, dsoff;
     DevBuf dredge;       // edges ordered by receiver (adjoint of a COO not grouped by receiver)
-    DevBuf dterm;        // per-edge cotangent term of the self-pair adjoint (4 values)
     DevBuf dseg;         // per-point {first, end} edge of the self-pair adjoint
     DevBuf tstats;       // traversal statistics (oct_edges_traversal_stats)
     // Options (oct_ctx_set_option): the polling rounds of a bounded device

@@ -15,8 +15,8 @@
 //                   (bounded waits), stages the tile in shared memory in digit
 //                   order and writes each digit's run contiguously.  The first
 //                   pass encodes from the coordinates; the last writes the
-//                   sorted keys, the sorted points, the permutation and its
-//                   inverse.
+//                   sorted keys, the sorted points and the permutation;
+//   k_inverse_perm  the inverse permutation.
 //
 // Every wait is bounded (spin_limit polling rounds); one that runs out sets
 // DF_TIMEOUT, and every store still stays inside its array.
@@ -115,8 +115,7 @@ constexpr size_t point_pass_smem() { return sizeof(PointPassSmem<T, D, K>); }
 
 // One pass on digit `pass`.  FIRST: the points come from `coords` (key
 // encoded here, value = the point and its index); otherwise from (kin, pin).
-// LAST: writes kout, pout (the sorted points), perm[dst] = original index and
-// iperm[original index] = dst.
+// LAST: writes kout, pout (the sorted points) and perm[dst] = original index.
 template <class T, int D, class K, bool FIRST, bool LAST>
 __global__ void __launch_bounds__(kSortThreads) k_point_pass(
     const T* __restrict__ coords, EncodeParams<T> ep, const K* __restrict__ kin, const SPt<T, D>* __restrict__ pin,
@@ -237,18 +236,27 @@ __global__ void __launch_bounds__(kSortThreads) k_point_pass(
             const SPt<T, D> p = sm.pt[i];
             kout[dst] = k;
             pout[dst] = p;
-            if (LAST) {
-                perm[dst] = p.idx;
-                if ((uint64_t)(uint32_t)p.idx < (uint64_t)n)
-                    iperm[p.idx] = (int32_t)dst;
-                else
-                    timed_out = true;  // a stale record: only after a wait ran out
-            }
+            if (LAST) perm[dst] = p.idx;
         } else {
             timed_out = true;
         }
     }
     if (timed_out) atomicOr(status, (int)DF_TIMEOUT);
+}
+
+// iperm[perm[k]] = k: after the last pass, in a pass of its own, so that the
+// random 4-byte stores land in a 4n-byte target that L2 holds while nothing
+// else streams.  An entry outside [0, n) can only be stale after a look-back
+// wait ran out (DF_TIMEOUT is then set already) and is skipped.
+__global__ void __launch_bounds__(kSortThreads) k_inverse_perm(const int32_t* __restrict__ perm, int64_t n,
+                                                               int32_t* __restrict__ iperm, int* __restrict__ status) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int32_t j = perm[k];
+    if ((uint64_t)(uint32_t)j < (uint64_t)n)
+        iperm[j] = (int32_t)k;
+    else
+        atomicOr(status, (int)DF_TIMEOUT);
 }
 
 template <class T, int D, class K, bool FIRST, bool LAST>
@@ -272,7 +280,7 @@ cudaError_t launch_point_pass(const T* coords, const EncodeParams<T>& ep, const 
 // on return keys_out holds the sorted keys, spts the sorted points, perm the
 // original index of each sorted position and iperm its inverse.  kt and ptmp
 // are scratch of n keys / points (used when passes > 1); `scratch` holds
-// onesweep_words(n, kOnesweepMaxPasses) words.  Launches 1 + passes kernels.
+// onesweep_words(n, kOnesweepMaxPasses) words.  Launches 2 + passes kernels.
 template <class T, int D, class K>
 cudaError_t point_sort(const T* coords, const EncodeParams<T>& ep, int64_t n, int passes, K* keys_out, K* kt,
                        SPt<T, D>* spts, SPt<T, D>* ptmp, int32_t* perm, int32_t* iperm, uint32_t* scratch, int* status,
@@ -288,20 +296,27 @@ cudaError_t point_sort(const T* coords, const EncodeParams<T>& ep, int64_t n, in
     // last pass lands in (keys_out, spts).
     auto kb = [&](int p) { return ((passes - 1 - p) & 1) == 0 ? keys_out : kt; };
     auto pb = [&](int p) { return ((passes - 1 - p) & 1) == 0 ? spts : ptmp; };
-    if (passes == 1)
-        return launch_point_pass<T, D, K, true, true>(coords, ep, nullptr, nullptr, keys_out, spts, perm, iperm, n, 0,
-                                                      ntiles, scratch, status, spin_limit, withhold, s);
-    if ((e = launch_point_pass<T, D, K, true, false>(coords, ep, nullptr, nullptr, kb(0), pb(0), nullptr, nullptr, n, 0,
-                                                     ntiles, scratch, status, spin_limit, withhold, s)))
-        return e;
-    for (int p = 1; p < passes - 1; ++p)
-        if ((e = launch_point_pass<T, D, K, false, false>(coords, ep, kb(p - 1), pb(p - 1), kb(p), pb(p), nullptr,
-                                                          nullptr, n, p, ntiles, scratch, status, spin_limit, withhold,
-                                                          s)))
+    *launches += 1;  // the inverse permutation
+    if (passes == 1) {
+        if ((e = launch_point_pass<T, D, K, true, true>(coords, ep, nullptr, nullptr, keys_out, spts, perm, iperm, n, 0,
+                                                        ntiles, scratch, status, spin_limit, withhold, s)))
             return e;
-    return launch_point_pass<T, D, K, false, true>(coords, ep, kb(passes - 2), pb(passes - 2), keys_out, spts, perm,
-                                                   iperm, n, passes - 1, ntiles, scratch, status, spin_limit, withhold,
-                                                   s);
+    } else {
+        if ((e = launch_point_pass<T, D, K, true, false>(coords, ep, nullptr, nullptr, kb(0), pb(0), nullptr, nullptr,
+                                                         n, 0, ntiles, scratch, status, spin_limit, withhold, s)))
+            return e;
+        for (int p = 1; p < passes - 1; ++p)
+            if ((e = launch_point_pass<T, D, K, false, false>(coords, ep, kb(p - 1), pb(p - 1), kb(p), pb(p), nullptr,
+                                                              nullptr, n, p, ntiles, scratch, status, spin_limit,
+                                                              withhold, s)))
+                return e;
+        if ((e = launch_point_pass<T, D, K, false, true>(coords, ep, kb(passes - 2), pb(passes - 2), keys_out, spts,
+                                                         perm, iperm, n, passes - 1, ntiles, scratch, status,
+                                                         spin_limit, withhold, s)))
+            return e;
+    }
+    k_inverse_perm<<<(unsigned)((n + kSortThreads - 1) / kSortThreads), kSortThreads, 0, s>>>(perm, n, iperm, status);
+    return cudaGetLastError();
 }
 
 }  // namespace oct
