@@ -517,11 +517,33 @@ __global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n,
 // room for its nodes' groups with one atomic on hdr->n_groups, and each node
 // writes its groups there.  The groups' order does not matter: every result
 // is per query point.
-template <class T, int D>
+//
+// Each group also gets the node its traversal may start from (gstart, when
+// given): the deepest strict ancestor S of the group's parent P whose Morton
+// cell contains every cell within kStartMargin cells of P's cell.  The cell
+// size is the radius, so every point within the radius of a point of the group
+// (one cell, plus one for the rounding of the two binnings) lies in S's cell,
+// hence in S's subtree: a search from S meets every neighbor the search from
+// the root meets, and in the same order, since a depth-first search restricted
+// to a subtree visits it in the subtree's own order.  Bit 30 carries the
+// ascending-order flag that S's stack entry has in the search from the root
+// (some strict ancestor with its first child slot empty); -1 = start at the
+// root.  The test reads keys and topology only, so it holds for as long as the
+// keys do (the bounds-only refit keeps it).
+constexpr int kStartMargin = 2;
+
+template <int D, class K>
+__device__ __forceinline__ uint64_t axis_cell(K key, int d) {
+    return D == 3 ? compact_by_3((uint64_t)key >> d) : compact_by_2((uint64_t)key >> d);
+}
+
+template <class T, int D, class K>
 __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restrict__ tnode, int64_t capacity,
                                                      int2* __restrict__ groups, int64_t group_cap,
                                                      const int32_t* __restrict__ chain,
-                                                     const int32_t* __restrict__ parent, OctHeader* hdr, int gmax) {
+                                                     const int32_t* __restrict__ parent, OctHeader* hdr, int gmax,
+                                                     const K* __restrict__ skeys, const int2* __restrict__ nrange,
+                                                     int32_t* __restrict__ gstart) {
     const int64_t nn = hdr->n_nodes;
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id == 0 && nn <= capacity) {
@@ -537,10 +559,50 @@ __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restri
     // pass 0 counts the node's groups, pass 1 writes them from `out`.
     int64_t out = 0;
     int32_t ng = 0;
+    int32_t start = -1;  // the traversal start of this node's groups
     for (int pass = 0; pass < 2; ++pass) {
         ng = 0;
+        if (pass && gstart && live && ng == 0) {
+            const TNode<T, D> nd = tnode[id];
+            if (nd.b <= 0) {
+                // P = this node: its level (depth) and the ancestors' chain
+                constexpr int BITS = Dims<D>::bits;
+                int32_t anc[BITS + 2];
+                int depth = 0;
+                for (int32_t a = (int32_t)id; a >= 0 && depth < BITS + 2; a = parent[a]) anc[depth++] = a;
+                const int lp = depth - 1;  // anc[0] = P at level lp, anc[lp] = root
+                const K kp = skeys[nrange[id].x];
+                constexpr int64_t cmax = (1LL << BITS) - 1;
+                int la = -1;  // deepest level whose cell holds P's cell +- kStartMargin
+                for (int L = lp - 1; L >= 1 && la < 0; --L) {
+                    const int sh = BITS - L;
+                    bool ok = true;
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        const int64_t c = (int64_t)axis_cell<D, K>(kp, d);
+                        const int64_t plo = (c >> (BITS - lp)) << (BITS - lp);
+                        const int64_t phi = plo + (1LL << (BITS - lp)) - 1;
+                        const int64_t slo = (c >> sh) << sh, shi = slo + (1LL << sh) - 1;
+                        int64_t nlo = plo - kStartMargin, nhi = phi + kStartMargin;
+                        nlo = nlo < 0 ? 0 : nlo;
+                        nhi = nhi > cmax ? cmax : nhi;
+                        ok = ok && nlo >= slo && nhi <= shi;
+                    }
+                    if (ok) la = L;
+                }
+                if (la >= 1) {
+                    const int32_t sid = anc[lp - la];
+                    bool casc = false;  // a strict ancestor of S with its first slot empty
+                    for (int j = lp - la + 1; j <= lp; ++j) casc = casc || !(((unsigned)(-tnode[anc[j]].b)) & 1u);
+                    start = sid | (casc ? (1 << 30) : 0);
+                }
+            }
+        }
         auto emit = [&](int32_t first, int32_t count) {
-            if (pass && out + ng < group_cap) groups[out + ng] = make_int2(first, count);
+            if (pass && out + ng < group_cap) {
+                groups[out + ng] = make_int2(first, count);
+                if (gstart) gstart[out + ng] = start;
+            }
             ++ng;
         };
         if (live) {
@@ -1159,7 +1221,8 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             (err = ensure_g(ctx, t.nrange, (size_t)cap * 8)) || (err = ensure_g(ctx, t.parent, (size_t)cap * 4)) ||
             (err = ensure_g(ctx, t.arrive, (size_t)cap * 4)) || (err = ensure_g(ctx, t.fchild, (size_t)cap * 4)) ||
             (err = ensure(t.scan_tmp, (size_t)scan_tmp_elems(nbc) * 8)) ||
-            (err = ensure_g(ctx, t.groups, gcap * 8)) || (err = ensure(t.chain, 64 * 4)))
+            (err = ensure_g(ctx, t.groups, gcap * 8)) || (err = ensure(t.gstart, gcap * 4)) ||
+            (err = ensure(t.chain, 64 * 4)))
             return cuda_status(ctx, err, "allocating node arrays");
         if ((err = cudaMemsetAsync(t.chain.p, 0xff, 64 * 4, s)) ||
             (err = cudaMemsetAsync(&hdr->n_groups, 0, sizeof(int64_t), s)))
@@ -1194,10 +1257,10 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         }
         {
             PhaseTimer pt_(ctx, PH_GROUPS);
-            k_groups<T, D><<<div_up(cap, kThreads), kThreads, 0, s>>>(t.tnode.as<TNode<T, D>>(), cap,
-                                                                     t.groups.as<int2>(), (int64_t)gcap,
-                                                                     t.chain.as<int32_t>(), t.parent.as<int32_t>(),
-                                                                     hdr, gmax);
+            k_groups<T, D, K><<<div_up(cap, kThreads), kThreads, 0, s>>>(
+                t.tnode.as<TNode<T, D>>(), cap, t.groups.as<int2>(), (int64_t)gcap, t.chain.as<int32_t>(),
+                t.parent.as<int32_t>(), hdr, gmax, skeys, t.nrange.as<int2>(),
+                bt.n_clouds ? nullptr : t.gstart.as<int32_t>());
             ctx.kernel_launches += 1;
             if (bt.n_clouds) {
                 k_cloud_start<T, D><<<div_up(bt.n_clouds, 128), 128, 0, s>>>(t.tnode.as<TNode<T, D>>(), bt, cap, hdr);

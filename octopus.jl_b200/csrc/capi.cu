@@ -176,7 +176,7 @@ void release_tree(oct::Tree& t) {
     for (auto* b : {&t.b_coff, &t.b_cparam, &t.b_croot, &t.b_cstart, &t.b_cbounds, &t.b_eoff})
         release(*b);
     for (auto* b : {&t.keys[0], &t.keys[1], &t.vals[0], &t.vals[1], &t.hist, &t.sort_tmp, &t.look, &t.spts, &t.spts_tmp, &t.tnode, &t.nrange,
-                    &t.parent, &t.fchild, &t.arrive, &t.groups, &t.chain, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
+                    &t.parent, &t.fchild, &t.arrive, &t.groups, &t.gstart, &t.chain, &t.lohi, &t.blockcnt, &t.blockoff, &t.scan_tmp, &t.partials, &t.hdr,
                     &t.morton, &t.v_first, &t.v_last, &t.v_children, &t.v_bmin, &t.v_bmax, &t.v_perm, &t.iperm,
                     &t.rflag, &t.rcnt, &t.roff, &t.mkeys, &t.mvals, &t.mkeys2, &t.mvals2})
         release(*b);

@@ -193,6 +193,27 @@ __host__ __device__ __forceinline__ uint64_t split_by_2(uint64_t x) {
     return x;
 }
 
+// Inverses of split_by_3 / split_by_2: the cell index of one axis from a
+// Morton code shifted so that the axis's bits are the lowest of each group.
+__host__ __device__ __forceinline__ uint64_t compact_by_3(uint64_t x) {
+    x &= 0x1249249249249249ULL;
+    x = (x ^ (x >> 2)) & 0x10c30c30c30c30c3ULL;
+    x = (x ^ (x >> 4)) & 0x100f00f00f00f00fULL;
+    x = (x ^ (x >> 8)) & 0x001f0000ff0000ffULL;
+    x = (x ^ (x >> 16)) & 0x001f00000000ffffULL;
+    x = (x ^ (x >> 32)) & 0x00000000001fffffULL;
+    return x;
+}
+__host__ __device__ __forceinline__ uint64_t compact_by_2(uint64_t x) {
+    x &= 0x5555555555555555ULL;
+    x = (x ^ (x >> 1)) & 0x3333333333333333ULL;
+    x = (x ^ (x >> 2)) & 0x0f0f0f0f0f0f0f0fULL;
+    x = (x ^ (x >> 4)) & 0x00ff00ff00ff00ffULL;
+    x = (x ^ (x >> 8)) & 0x0000ffff0000ffffULL;
+    x = (x ^ (x >> 16)) & 0x00000000ffffffffULL;
+    return x;
+}
+
 // ---------------------------------------------------------- warp helpers --
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;

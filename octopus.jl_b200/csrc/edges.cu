@@ -90,6 +90,12 @@ __device__ __forceinline__ void write_edge(int64_t k, const SPt<T, D>& t, const 
 // inside an allocation).
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
+// The per-group traversal starts of a tree searched against itself (not a
+// batch), else null (every group starts at the root).
+__host__ __forceinline__ const int32_t* own_start(const Tree& q, const Tree& t) {
+    return (&q == &t && !t.n_clouds) ? t.gstart.as<int32_t>() : nullptr;
+}
+
 // Radius and index base of the point set (cloud) holding sorted position p.
 template <class T>
 __device__ __forceinline__ void cloud_params(const Batch& bt, int64_t p, T& r2, T& inv_r, int32_t& start_node,
@@ -118,7 +124,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     int32_t* __restrict__ counts, const int64_t* __restrict__ offsets, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int* __restrict__ ocount,
     int2* __restrict__ recs, int64_t rec_cap, uint16_t* __restrict__ rcount, uint8_t* __restrict__ gflag, Batch bt,
-    unsigned long long* __restrict__ stats, int max_seg, int multi_pop, int nbox, int prefetch) {
+    unsigned long long* __restrict__ stats, int max_seg, int multi_pop, int nbox, int prefetch,
+    const int32_t* __restrict__ gstart) {
     constexpr bool STAGE = PASS == EP_FILL;
     constexpr bool STATS = PASS == EP_STATS;
     long long st_t0 = 0, st_leaf = 0, st_pairs = 0;
@@ -229,7 +236,14 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     };
 
     int sp = 0;
-    if (n_tnodes > 0) {
+    const int32_t gs = gstart ? gstart[g] : -1;
+    if (gs >= 0) {
+        // the group's own start node (k_groups): its subtree holds every
+        // neighbor, and the group lies inside it
+        const TNode<T, D> sn = tnode[gs & 0x3fffffff];
+        if (lane == 0) stack[w][0] = make_int2(sn.a | ((gs >> 30) & 1 ? (int32_t)0x80000000 : 0), sn.b);
+        sp = 1;
+    } else if (n_tnodes > 0) {
         const TNode<T, D> root = tnode[start_node];
         if (box_gap2<T, D>(qlo, qhi, root.lo, root.hi) <= r2) {
             if (lane == 0) stack[w][0] = make_int2(root.a, root.b);
@@ -906,13 +920,13 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
                 nullptr, nullptr, nullptr, nullptr, (int*)(ctx.total.as<int64_t>() + 1), ctx.recs.as<int2>(),
                 ctx.rec_cap, ctx.rcount.as<uint16_t>(), ctx.gflag.as<uint8_t>(), t.batch(), nullptr, tn.max_seg,
-                tn.multi_pop, tn.sub_boxes, tn.prefetch);
+                tn.multi_pop, tn.sub_boxes, tn.prefetch, own_start(q, t));
         else
             k_edges<T, D, EP_COUNT><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
                 nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr,
-                tn.max_seg, tn.multi_pop, tn.sub_boxes, tn.prefetch);
+                tn.max_seg, tn.multi_pop, tn.sub_boxes, tn.prefetch, own_start(q, t));
         ctx.kernel_launches += 1;
     }
     {
@@ -1008,7 +1022,7 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
             t.spts.as<SPt<T, D>>(), t.n_nodes, r2, inv_r, exclude_self ? 1 : 0, nullptr, ctx.offsets.as<int64_t>(),
             senders, receivers, (T*)rel_disp, (T*)rel_dist, ctx.dstatus.as<int>(),
             ctx.rec_cap ? ctx.recs.as<int2>() : nullptr, ctx.rec_cap, nullptr, ctx.gflag.as<uint8_t>(), t.batch(),
-            nullptr, tn.max_seg, tn.multi_pop, tn.sub_boxes, tn.prefetch);
+            nullptr, tn.max_seg, tn.multi_pop, tn.sub_boxes, tn.prefetch, own_start(q, t));
         ctx.kernel_launches += 1;
     }
     return cuda_status(ctx, cudaGetLastError(), "edge fill launch");
@@ -1033,7 +1047,7 @@ cudaError_t count_into_typed(const Tree& q, const Tree& t, bool exclude_self, in
     k_edges<T, D, EP_COUNT><<<div_up(q.n_groups, kEdgeWarps), kEdgeThreads, 0, s>>>(
         q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
         t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, counts, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr, kMaxSeg, kMultiPop, 1, 0);
+        nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr, kMaxSeg, kMultiPop, 1, 0, nullptr);
     return cudaGetLastError();
 }
 
@@ -1046,7 +1060,7 @@ int stats_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, unsig
         q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), q.n_groups, t.tnode.as<TNode<T, D>>(), t.dfs_start,
         t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr,
         nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), stats_dev, tn.max_seg,
-        tn.multi_pop, tn.sub_boxes, tn.prefetch);
+        tn.multi_pop, tn.sub_boxes, tn.prefetch, own_start(q, t));
     ctx.kernel_launches += 1;
     return cuda_status(ctx, cudaGetLastError(), "traversal statistics launch");
 }

@@ -117,6 +117,7 @@ struct Tree {
     DevBuf hdr;                  // OctHeader
     DevBuf morton;               // uint64 per original point (refit mode), filled with the views
     DevBuf groups;               // int2 {first position, count <= 32}: query groups
+    DevBuf gstart;               // int32 per group: traversal start node (| 1 << 30: ascending flag), -1 = root
     int64_t n_groups = 0;
     int32_t dfs_start = 0;
     DevBuf chain;                // int32[64]: full-range chain node ids and flags
