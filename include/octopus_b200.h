@@ -341,7 +341,9 @@ OCT_API int oct_edges_count_noalloc(oct_ctx* ctx, const oct_tree* query, const o
  * or the default when no table is loaded, see oct_ctx_load_tuning):
  *   OCT_OPT_MAX_SEG        leaves sharing one staged chunk of the traversal, 1..16 (16)
  *   OCT_OPT_MULTI_POP      internal nodes the traversal expands together, 1..4 (4)
- *   OCT_OPT_FILL_CHUNK     edges per bulk-copy chunk of the fill: 32, 64 or 128 (64)
+ *   OCT_OPT_FILL_CHUNK     the fill's stores: 1 direct (default), or 32, 64 or 128 for
+ *                          bulk copies of that many edges per chunk (a table row says 0
+ *                          for direct)
  *   OCT_OPT_GROUP_CAP      query points per traversal group, 8..32 (32), set at the build
  *   OCT_OPT_SUB_BOXES      boxes a group's queries are split into (runs of 32/k lanes)
  *                          for the test that skips distant target points: 1, 2 or 4 (1)

@@ -83,7 +83,7 @@ bool parse_tuning(const char* path, std::vector<TuneRow>& rows, std::string& err
         if (got <= 0) continue;  // blank or comment
         const bool valid = got >= 8 && got <= 10 && (v[0] == 2 || v[0] == 3) && (v[1] == 0 || v[1] == 1) &&
                            v[2] >= 0 && v[2] <= 40 && v[3] >= 0 && v[3] <= 40 && v[4] >= 1 && v[4] <= 16 &&
-                           v[5] >= 1 && v[5] <= 4 && (v[6] == 32 || v[6] == 64 || v[6] == 128) && v[7] >= 8 &&
+                           v[5] >= 1 && v[5] <= 4 && (v[6] == 0 || v[6] == 32 || v[6] == 64 || v[6] == 128) && v[7] >= 8 &&
                            v[7] <= 32 && (v[8] == 1 || v[8] == 2 || v[8] == 4) && (v[9] == 0 || v[9] == 1);
         if (!valid) {
             err = std::string("tuning table ") + path + ": bad row at line " + std::to_string(lineno);
@@ -137,7 +137,7 @@ Tuning Ctx::tuning_for(int ndims, int dtype, int64_t n, double nbrs) {
     last_tune_row = select_tuning(tune_table, ndims, dtype, n, nbrs, tn);
     if (tune_force.max_seg) tn.max_seg = tune_force.max_seg;
     if (tune_force.multi_pop) tn.multi_pop = tune_force.multi_pop;
-    if (tune_force.fill_chunk) tn.fill_chunk = tune_force.fill_chunk;
+    if (tune_force.fill_chunk) tn.fill_chunk = tune_force.fill_chunk == 1 ? 0 : tune_force.fill_chunk;
     if (tune_force.group_cap) tn.group_cap = tune_force.group_cap;
     if (tune_force.sub_boxes) tn.sub_boxes = tune_force.sub_boxes;
     if (tune_force.prefetch) tn.prefetch = tune_force.prefetch - 1;
@@ -229,7 +229,7 @@ OCT_API int oct_ctx_destroy(oct_ctx* ctx) {
     using oct::release;
     for (auto* b : {&ctx->c.counts, &ctx->c.offsets, &ctx->c.scan_tmp, &ctx->c.total, &ctx->c.dkeys[0],
                     &ctx->c.dkeys[1], &ctx->c.dvals[0], &ctx->c.dvals[1], &ctx->c.dhist, &ctx->c.dsort_tmp, &ctx->c.droff,
-                    &ctx->c.dsoff, &ctx->c.dstatus, &ctx->c.dredge, &ctx->c.dseg, &ctx->c.tstats, &ctx->c.recs, &ctx->c.rcount, &ctx->c.gflag})
+                    &ctx->c.dsoff, &ctx->c.dstatus, &ctx->c.dredge, &ctx->c.dterm, &ctx->c.dseg, &ctx->c.tstats, &ctx->c.recs, &ctx->c.rcount, &ctx->c.gflag})
         release(*b);
     if (ctx->c.total_host) cudaFreeHost(ctx->c.total_host);
     for (auto& r : ctx->c.prof) {
@@ -595,9 +595,9 @@ OCT_API int oct_ctx_set_option(oct_ctx* ctx, int option, int64_t value) {
             if (value < 0 || value > 4) return oct::set_error(c, OCT_ERR_ARGUMENT, "multi_pop must be in [0, 4]");
             c.tune_force.multi_pop = (int)value;
             return OCT_OK;
-        case OCT_OPT_FILL_CHUNK:
-            if (value != 0 && value != 32 && value != 64 && value != 128)
-                return oct::set_error(c, OCT_ERR_ARGUMENT, "fill_chunk must be 0, 32, 64 or 128");
+        case OCT_OPT_FILL_CHUNK:  // 0 = table, 1 = direct stores, else the bulk-copy chunk
+            if (value != 0 && value != 1 && value != 32 && value != 64 && value != 128)
+                return oct::set_error(c, OCT_ERR_ARGUMENT, "fill_chunk must be 0, 1, 32, 64 or 128");
             c.tune_force.fill_chunk = (int)value;
             return OCT_OK;
         case OCT_OPT_GROUP_CAP:

@@ -503,6 +503,187 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     }
 }
 
+// Fill pass from the records with direct stores, in original index order
+// (the default fill; k_expand below writes through bulk copies instead, a
+// tuned alternative): warp v writes the
+// edges of queries 32v .. 32v+31, which the COO stores contiguously, so its
+// stores cover whole sectors.  The warp's edges form one flat list, query
+// ql's first at flat index epre(ql), COO slot kq[ql] + flat index.  Records are expanded into shared memory
+// (lanes over consecutive records, each record's first hit at the running sum
+// of the hit counts before it), then each batch of flat edges is written with
+// lanes on consecutive edges.  Queries of an overflowed group (record count
+// kOverflowMark) are left to the walking fill.
+constexpr int kDirectWarps = 4;
+constexpr int kDirectCap = 512;  // staged positions per warp (at least 32: one record)
+
+template <class T, int D>
+struct DirectSmem {
+    int32_t pos[kDirectCap];
+    uint8_t who[kDirectCap];  // query (lane) of each staged position
+    long long kq[32];    // COO slot of each query's flat edge 0: first slot - epre
+    long long key[32];   // COO slot of each entry of a write batch
+    T qx[D][32];
+    T disp[D * 32];
+    T inv_r[32];
+    int32_t qpos[32];    // sorted position of each query
+    int32_t qi[32];      // 1-based receiver index of each query
+    int32_t base[32];    // index base of each query's point set
+    int32_t rpre[33];    // flat record index where each query starts
+};
+
+template <class T, int D>
+__global__ void __launch_bounds__(kDirectWarps * 32, 8) k_expand_direct(
+    int64_t nq, const int32_t* __restrict__ iperm, const SPt<T, D>* __restrict__ qpts,
+    const SPt<T, D>* __restrict__ tpts, const int64_t* __restrict__ offsets, const int2* __restrict__ recs,
+    int64_t rec_cap, const uint16_t* __restrict__ rcount, T inv_r, int32_t* __restrict__ senders,
+    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, Batch bt) {
+    __shared__ DirectSmem<T, D> sm_all[kDirectWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t i0 = ((int64_t)blockIdx.x * kDirectWarps + w) * 32;
+    if (i0 >= nq) return;  // warp-uniform
+    DirectSmem<T, D>& sm = sm_all[w];
+    const int64_t i = i0 + lane;
+    const bool valid = i < nq;
+    const int32_t qp = valid ? iperm[i] : 0;
+    int nr = valid ? rcount[qp] : 0;
+    long long cur = 0;
+    int ne = 0;
+    if (valid && nr != kOverflowMark) {
+        cur = offsets[i];
+        ne = (int)(offsets[i + 1] - cur);
+    } else {
+        nr = 0;
+    }
+    const SPt<T, D> q = qpts[qp];
+    T r2 = T(0), ir = inv_r;
+    int32_t start_node = 0, base = 0;
+    cloud_params<T>(bt, qp, r2, ir, start_node, base);
+    int ie = ne, irc = nr;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int a = __shfl_up_sync(0xffffffffu, ie, o);
+        const int b = __shfl_up_sync(0xffffffffu, irc, o);
+        if (lane >= o) {
+            ie += a;
+            irc += b;
+        }
+    }
+    sm.kq[lane] = cur - (ie - ne);
+#pragma unroll
+    for (int d = 0; d < D; ++d) sm.qx[d][lane] = q.x[d];
+    sm.inv_r[lane] = ir;
+    sm.qpos[lane] = qp;
+    sm.qi[lane] = q.idx - base + 1;
+    sm.base[lane] = base;
+    sm.rpre[lane + 1] = irc;
+    if (lane == 0) sm.rpre[0] = 0;
+    __syncwarp();
+    const int total_r = __shfl_sync(0xffffffffu, irc, 31);
+    const bool feat = rdisp != nullptr;  // false: neighbor lists (CSR values) only
+    int used = 0;      // positions staged (warp-uniform)
+    int ebase = 0;     // flat edge index of pos[0]
+    int qr = 0;        // this lane's query, for records
+
+    // Writes flat edges [ebase, ebase + cnt) from the staged positions: four
+    // entries per lane in flight, rel_displacement through shared memory so
+    // that each store of the warp covers consecutive values.
+    auto write_batch = [&](int cnt) {
+        for (int f0 = 0; f0 < cnt; f0 += 4 * 32) {
+            int qv[4];
+            long long kv[4];
+            SPt<T, D> tp[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int f = f0 + 32 * u + lane;
+                if (f < cnt) {
+                    const int qe = sm.who[f];
+                    qv[u] = qe;
+                    kv[u] = sm.kq[qe] + (ebase + f);
+                    tp[u] = tpts[sm.pos[f]];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int fb = f0 + 32 * u;
+                if (fb >= cnt) break;
+                const int nb = min(32, cnt - fb);
+                if (lane < nb) {
+                    const int q2 = qv[u];
+                    const long long k = kv[u];
+                    senders[k] = tp[u].idx - sm.base[q2] + 1;
+                    if (feat) {
+                        const T iv = sm.inv_r[q2];
+                        T px[D], diff[D];
+#pragma unroll
+                        for (int d = 0; d < D; ++d) px[d] = sm.qx[d][q2];
+                        const T d2 = dist2<T, D>(tp[u].x, px, diff);
+                        receivers[k] = sm.qi[q2];
+                        rdist[k] = mul_rn(sqrt_rn(d2), iv);
+#pragma unroll
+                        for (int d = 0; d < D; ++d) sm.disp[D * lane + d] = mul_rn(-diff[d], iv);
+                        sm.key[lane] = k;
+                    }
+                }
+                if (feat) {
+                    __syncwarp();
+#pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        const int v = 32 * c + lane;  // value v of the batch: entry v / D, axis v % D
+                        const int ent = v / D;
+                        if (ent < nb) rdisp[D * sm.key[ent] + (v - D * ent)] = sm.disp[v];
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+    };
+
+    for (int r0 = 0; r0 < total_r; r0 += 32) {
+        const int rho = r0 + lane;
+        int2 rec = make_int2(0, 0);
+        if (rho < total_r) {
+            while (sm.rpre[qr + 1] <= rho) ++qr;
+            rec = recs[(int64_t)sm.qpos[qr] * rec_cap + (rho - sm.rpre[qr])];
+        }
+        const int p = __popc((unsigned)rec.y);
+        int incl = p;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int a = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += a;
+        }
+        // Stage the round's records in parts that fit the free positions,
+        // writing the staged edges out whenever the next record does not fit.
+        int lo = 0, base_incl = 0;  // lanes below `lo` are staged (warp-uniform)
+        while (lo < 32) {
+            const bool fits = lane >= lo && incl - base_incl <= kDirectCap - used;
+            const int hi = lo + __popc(__ballot_sync(0xffffffffu, fits));
+            if (hi == lo) {
+                write_batch(used);
+                ebase += used;
+                used = 0;
+                continue;
+            }
+            if (fits) {
+                int at = used + (incl - p - base_incl);
+                unsigned m = (unsigned)rec.y;
+                while (m) {
+                    const int j = __ffs(m) - 1;
+                    m &= m - 1;
+                    sm.who[at] = (uint8_t)qr;
+                    sm.pos[at++] = rec.x + j;
+                }
+            }
+            const int hi_incl = __shfl_sync(0xffffffffu, incl, hi - 1);
+            used += hi_incl - base_incl;
+            base_incl = hi_incl;
+            lo = hi;
+            __syncwarp();
+        }
+    }
+    write_batch(used);
+}
+
 // Fill pass from the records, in original index order.  Warp v writes the
 // edges of queries 32v .. 32v+31, which own one contiguous range [K0, K1) of
 // the COO, query after query, each query's edges in record order.  The warp
@@ -558,23 +739,17 @@ __device__ __forceinline__ int kth_set_bit(unsigned m, int k) {
 }
 
 // Shared-memory bytes of one warp's ring of `ring` edges.
-template <class T, int D, bool FEAT, bool TWIN>
+template <class T, int D, bool FEAT>
 __host__ __device__ constexpr size_t fill_ring_bytes(int ring) {
-    return (FEAT ? (size_t)ring * (8 + (D + 1) * sizeof(T)) : (size_t)ring * 4) + (TWIN ? (size_t)ring * 4 : 0);
+    return FEAT ? (size_t)ring * (8 + (D + 1) * sizeof(T)) : (size_t)ring * 4;
 }
 
-// TWIN (a self pair whose records are complete): also writes, for every edge
-// k = (i <- j), the index of its mirror (j <- i) in the COO: j's first edge
-// plus the number of j's hits before i, counted over j's records in order.
-// A mirror not found there (only for a COO that is not a self pair) is
-// written as -1 and sets bit 2 of *status.
-template <class T, int D, bool FEAT, bool TWIN, int CHUNK, int NCH>
+template <class T, int D, bool FEAT, int CHUNK, int NCH>
 __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
     int64_t nq, const int32_t* __restrict__ iperm, const SPt<T, D>* __restrict__ qpts,
     const SPt<T, D>* __restrict__ tpts, const int64_t* __restrict__ offsets, const int2* __restrict__ recs,
     int64_t rec_cap, const uint16_t* __restrict__ rcount, T inv_r, int32_t* __restrict__ senders,
-    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, int32_t* __restrict__ twins,
-    int* __restrict__ status, Batch bt, int bulk_ok) {
+    int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, Batch bt, int bulk_ok) {
     constexpr int RING = CHUNK * NCH;
     constexpr int U = 2;                                  // hits per lane in flight
     constexpr int SUB = 32 * U;                           // hits written per sub-round
@@ -585,12 +760,11 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t i0 = ((int64_t)blockIdx.x * kFillWarps + w) * 32;
     if (i0 >= nq) return;  // warp-uniform
-    unsigned char* wsm = fill_smem + (size_t)w * fill_ring_bytes<T, D, FEAT, TWIN>(RING);
+    unsigned char* wsm = fill_smem + (size_t)w * fill_ring_bytes<T, D, FEAT>(RING);
     int32_t* r_snd = reinterpret_cast<int32_t*>(wsm);
     int32_t* r_rcv = r_snd + RING;
     T* r_dist = reinterpret_cast<T*>(r_rcv + RING);
     T* r_disp = r_dist + RING;
-    int32_t* r_twin = FEAT ? reinterpret_cast<int32_t*>(r_disp + D * RING) : r_snd + RING;
 
     // Lane j: query i0 + j.
     const int64_t i = i0 + lane;
@@ -655,7 +829,6 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
                         bulk_store(rdist + a, r_dist + sl, (uint32_t)sizeof(T) * m);
                         bulk_store(rdisp + (long long)D * a, r_disp + D * sl, (uint32_t)(D * sizeof(T)) * m);
                     }
-                    if (TWIN) bulk_store(twins + a, r_twin + sl, 4u * m);
                 }
                 bulk_commit();  // one group per chunk, empty or not
             }
@@ -670,7 +843,6 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
 #pragma unroll
                     for (int d = 0; d < D; ++d) rdisp[(long long)D * k + d] = r_disp[D * sl + d];
                 }
-                if (TWIN) twins[k] = r_twin[sl];
             }
             ++next_flush;
         }
@@ -745,7 +917,6 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
                 const T irq = __shfl_sync(FULL, ir, jq[u]);
                 const int32_t bq = __shfl_sync(FULL, base, jq[u]);
                 const int32_t qiq = __shfl_sync(FULL, qi, jq[u]);
-                const int32_t qpq = TWIN ? __shfl_sync(FULL, qp, jq[u]) : 0;
                 if (e >= tot) continue;
                 const long long k = kk[u];
                 const int32_t snd = tp[u].idx - bq + 1;
@@ -757,23 +928,6 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
 #pragma unroll
                     for (int d = 0; d < D; ++d) dv[d] = mul_rn(-diff[d], irq);
                 }
-                int32_t tw = -1;
-                if (TWIN) {
-                    // the query's place among the target's hits, record by record
-                    const int2* rj = recs + (int64_t)tpos[u] * rec_cap;
-                    const int nrt = rcount[tpos[u]];
-                    int rank = 0;
-                    for (int rr = 0; rr < nrt; ++rr) {
-                        const int2 rc = rj[rr];
-                        const unsigned off = (unsigned)(qpq - rc.x);
-                        if (off < 32u && ((unsigned)rc.y >> off) & 1u) {
-                            tw = (int32_t)(offsets[tp[u].idx] + rank + __popc((unsigned)rc.y & ((1u << off) - 1u)));
-                            break;
-                        }
-                        rank += __popc((unsigned)rc.y);
-                    }
-                    if (tw < 0) atomicOr(status, 4);
-                }
                 if (bulk) {
                     const int sl = (int)((k - kbase) & (RING - 1));
                     r_snd[sl] = snd;
@@ -783,7 +937,6 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
 #pragma unroll
                         for (int d = 0; d < D; ++d) r_disp[D * sl + d] = dv[d];
                     }
-                    if (TWIN) r_twin[sl] = tw;
                 } else {
                     senders[k] = snd;
                     if (FEAT) {
@@ -792,7 +945,6 @@ __global__ void __launch_bounds__(kFillWarps * 32) k_expand(
 #pragma unroll
                         for (int d = 0; d < D; ++d) rdisp[(long long)D * k + d] = dv[d];
                     }
-                    if (TWIN) twins[k] = tw;
                 }
             }
             if (bulk) {
@@ -954,11 +1106,11 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
 // Ring of the fill: kFillRing chunks of CHUNK edges (32, 64 or 128: a tuned shape).
 constexpr int kFillRing = 4;
 
-template <class T, int D, bool FEAT, bool TWIN, int CHUNK>
+template <class T, int D, bool FEAT, int CHUNK>
 cudaError_t launch_expand_shape(Ctx& ctx, const Tree& q, const Tree& t, T inv_r, int32_t* senders, int32_t* receivers,
-                                void* rel_disp, void* rel_dist, int32_t* twins, int bulk_ok) {
-    constexpr size_t smem = kFillWarps * fill_ring_bytes<T, D, FEAT, TWIN>(CHUNK * kFillRing);
-    auto kern = k_expand<T, D, FEAT, TWIN, CHUNK, kFillRing>;
+                                void* rel_disp, void* rel_dist, int bulk_ok) {
+    constexpr size_t smem = kFillWarps * fill_ring_bytes<T, D, FEAT>(CHUNK * kFillRing);
+    auto kern = k_expand<T, D, FEAT, CHUNK, kFillRing>;
     if (smem > 48 * 1024) {
         static bool attr_set = false;  // per instantiation
         if (!attr_set) {
@@ -970,32 +1122,37 @@ cudaError_t launch_expand_shape(Ctx& ctx, const Tree& q, const Tree& t, T inv_r,
     kern<<<div_up(q.n, 32 * kFillWarps), kFillWarps * 32, smem, ctx.stream>>>(
         q.n, q.iperm.as<int32_t>(), q.spts.as<SPt<T, D>>(), t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
         ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint16_t>(), inv_r, senders, receivers, (T*)rel_disp,
-        (T*)rel_dist, twins, ctx.dstatus.as<int>() + 1, t.batch(), bulk_ok);
+        (T*)rel_dist, t.batch(), bulk_ok);
     return cudaGetLastError();
 }
 
+// The fill of the last count's records with the tuned stores: direct
+// (k_expand_direct) or bulk copies of 32-, 64- or 128-edge chunks (k_expand).
 template <class T, int D, bool FEAT>
 cudaError_t launch_expand(Ctx& ctx, const Tree& q, const Tree& t, T inv_r, int32_t* senders, int32_t* receivers,
-                          void* rel_disp, void* rel_dist, int32_t* twins, int bulk_ok) {
-    if (FEAT && twins)  // the mirror indices of a differentiable fill: one shape
-        return launch_expand_shape<T, D, FEAT, true, 64>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
-                                                         twins, bulk_ok);
+                          void* rel_disp, void* rel_dist, int bulk_ok) {
     switch (ctx.plan_tuning.fill_chunk) {
         case 32:
-            return launch_expand_shape<T, D, FEAT, false, 32>(ctx, q, t, inv_r, senders, receivers, rel_disp,
-                                                              rel_dist, nullptr, bulk_ok);
+            return launch_expand_shape<T, D, FEAT, 32>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
+                                                       bulk_ok);
+        case 64:
+            return launch_expand_shape<T, D, FEAT, 64>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
+                                                       bulk_ok);
         case 128:
-            return launch_expand_shape<T, D, FEAT, false, 128>(ctx, q, t, inv_r, senders, receivers, rel_disp,
-                                                               rel_dist, nullptr, bulk_ok);
-        default:
-            return launch_expand_shape<T, D, FEAT, false, 64>(ctx, q, t, inv_r, senders, receivers, rel_disp,
-                                                              rel_dist, nullptr, bulk_ok);
+            return launch_expand_shape<T, D, FEAT, 128>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
+                                                        bulk_ok);
+        default:  // direct stores
+            k_expand_direct<T, D><<<div_up(q.n, 32 * kDirectWarps), kDirectWarps * 32, 0, ctx.stream>>>(
+                q.n, q.iperm.as<int32_t>(), q.spts.as<SPt<T, D>>(), t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
+                ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint16_t>(), inv_r, senders, receivers, (T*)rel_disp,
+                (T*)rel_dist, t.batch());
+            return cudaGetLastError();
     }
 }
 
 template <class T, int D>
 int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_t* senders, int32_t* receivers,
-               void* rel_disp, void* rel_dist, int32_t* twins = nullptr) {
+               void* rel_disp, void* rel_dist) {
     const T r = (T)t.radius;
     const T r2 = r * r;
     const T inv_r = T(1) / r;  // inv(r), src/cpu/edges_cpu.jl:185
@@ -1006,12 +1163,11 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
     if (ctx.rec_cap) {
         const bool feat = rel_disp != nullptr;
         auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
-        const int bulk_ok = aligned(senders) && (!feat || (aligned(receivers) && aligned(rel_disp) && aligned(rel_dist))) &&
-                            (!twins || aligned(twins));
+        const int bulk_ok = aligned(senders) && (!feat || (aligned(receivers) && aligned(rel_disp) && aligned(rel_dist)));
         cudaError_t err = feat ? launch_expand<T, D, true>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
-                                                           twins, bulk_ok)
+                                                           bulk_ok)
                                : launch_expand<T, D, false>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
-                                                            nullptr, bulk_ok);
+                                                            bulk_ok);
         if (err != cudaSuccess) return cuda_status(ctx, err, "edge fill launch");
         ctx.kernel_launches += 1;
     }
@@ -1150,19 +1306,16 @@ int edges_fill_diff(Ctx& ctx, const Tree& t, int32_t* senders, int32_t* receiver
     if (ctx.plan_edges > INT32_MAX)
         return set_error(ctx, ERR_OVERFLOW, "oct_edges_fill_diff: more than 2^31 - 1 edges overflow the Int32 mirrors");
     if (ctx.plan_edges == 0 || t.n == 0 || t.n_nodes == 0) return OK;
-    // From the hit records when every query's records are complete (the
-    // mirror of an edge is read off its target's records); otherwise after
-    // the fill, by scanning the senders' segments.
-    const bool from_records = ctx.rec_cap > 0 && ctx.rec_overflow == 0;
-    int32_t* tw = from_records ? mirror : nullptr;
+    // The COO first, then each edge's mirror by a scan of its sender's
+    // segment.
     int st;
     if (t.dtype == 0)
-        st = t.ndims == 3 ? fill_typed<float, 3>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist, tw)
-                          : fill_typed<float, 2>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist, tw);
+        st = t.ndims == 3 ? fill_typed<float, 3>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist)
+                          : fill_typed<float, 2>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist);
     else
-        st = t.ndims == 3 ? fill_typed<double, 3>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist, tw)
-                          : fill_typed<double, 2>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist, tw);
-    if (st != OK || from_records) return st;
+        st = t.ndims == 3 ? fill_typed<double, 3>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist)
+                          : fill_typed<double, 2>(ctx, t, t, true, senders, receivers, rel_disp, rel_dist);
+    if (st != OK) return st;
     return edges_mirror_scan(ctx, senders, receivers, ctx.plan_edges, t.n, ctx.offsets.as<int64_t>(), mirror);
 }
 

@@ -29,7 +29,7 @@ struct Ctx;
 struct Tuning {
     int max_seg = 16;     // leaves sharing one staged chunk of the traversal (1..16)
     int multi_pop = 4;    // internal nodes expanded together by the traversal (1..4)
-    int fill_chunk = 64;  // edges per bulk-copy chunk of the fill (32, 64 or 128)
+    int fill_chunk = 0;   // the fill's stores: 0 direct, else bulk copies of chunks of 32, 64 or 128 edges
     int group_cap = 32;   // query points per traversal group, set at the build (8..32)
     int sub_boxes = 1;    // boxes a group's queries are split into for the target test (1, 2 or 4)
     int prefetch = 0;     // 1: the traversal prefetches the next chunk's points / children into L1
@@ -192,6 +192,7 @@ struct Ctx {
     // Adjoint scratch (diff.cu).
     DevBuf dkeys[2], dvals[2], dhist, dsort_tmp, droff, dsoff;
     DevBuf dredge;       // edges ordered by receiver (adjoint of a COO not grouped by receiver)
+    DevBuf dterm;        // per-edge cotangent term of the searching self-pair adjoint (4 values)
     DevBuf dseg;         // per-point {first, end} edge of the self-pair adjoint
     DevBuf tstats;       // traversal statistics (oct_edges_traversal_stats)
     // Options (oct_ctx_set_option): the polling rounds of a bounded device

@@ -34,11 +34,11 @@ SHAPES = [
     ("group_cap", 9, (16, 24, 32)),
     ("max_seg", 6, (1, 4, 8, 16)),
     ("multi_pop", 7, (1, 2, 4)),
-    ("fill_chunk", 8, (32, 64, 128)),
+    ("fill_chunk", 8, (0, 32, 64, 128)),
     ("sub_boxes", 10, (1, 2, 4)),
     ("prefetch", 11, (0, 1)),
 ]
-DEFAULTS = {"group_cap": 32, "max_seg": 16, "multi_pop": 4, "fill_chunk": 64, "sub_boxes": 1, "prefetch": 0}
+DEFAULTS = {"group_cap": 32, "max_seg": 16, "multi_pop": 4, "fill_chunk": 0, "sub_boxes": 1, "prefetch": 0}
 
 
 def _package():
@@ -90,8 +90,14 @@ class Runner:
     def force(self, shapes):
         for name, opt, _ in SHAPES:
             v = shapes.get(name)
-            # 0 hands a shape back to the table; prefetch is forced as 1 (off) / 2 (on)
-            v = 0 if v is None else (v + 1 if name == "prefetch" else v)
+            # 0 hands a shape back to the table; prefetch is forced as 1 (off) /
+            # 2 (on), direct fill stores (fill_chunk 0) as 1
+            if v is None:
+                v = 0
+            elif name == "prefetch":
+                v = v + 1
+            elif name == "fill_chunk" and v == 0:
+                v = 1
             self.ctx.check(self.ctx.lib.oct_ctx_set_option(self.ctx.handle, opt, int(v)), name)
 
     def step(self):

@@ -372,10 +372,10 @@ def _fill_diff(ob, tns, sid):
 
 
 @pytest.mark.parametrize("d,dtype", [(3, np.float32), (2, np.float32), (3, np.float64)])
-def test_mirror_indices_from_records_and_from_the_scan(ob, d, dtype):
-    """Every edge's mirror: senders[mirror[k]] = receivers[k] and back; the
-    records path and the segment-scan path (records forced to overflow) give
-    the same indices, and the same COO as build_edges."""
+def test_mirror_indices_of_the_differentiable_fill(ob, d, dtype):
+    """Every edge's mirror: senders[mirror[k]] = receivers[k] and back, the
+    mirror of the mirror is the edge; the same COO as build_edges, also when
+    the hit records overflow and the walking fill writes part of it."""
     x = uniform(30000, d, 8300 + d, dtype=dtype)
     r = dtype(0.05 if d == 3 else 0.01)
     tns, sid, c = setup(ob, x, r)

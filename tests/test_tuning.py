@@ -34,13 +34,13 @@ def test_nearest_row_of_the_same_kind(ob, tmp_path):
     assert select(ob, str(p), 2, 0, 4_000_000, 387.0) == (0, [4, 1, 128, 16, 4, 0], 2)
     assert select(ob, str(p), 3, 1, 5_000, 0.5) == (0, [1, 1, 64, 8, 1, 0], 3)
     # no row of that kind: the built-in defaults
-    assert select(ob, str(p), 2, 1, 1000, 10) == (0, [16, 4, 64, 32, 1, 0], -1)
+    assert select(ob, str(p), 2, 1, 1000, 10) == (0, [16, 4, 0, 32, 1, 0], -1)
     # neighbors not known yet (before a first count): keyed as ~15 per point
     assert select(ob, str(p), 3, 0, 100_000, -1) == (0, [8, 2, 32, 24, 2, 1], 0)
 
 
 def test_no_table_and_bad_tables(ob, tmp_path):
-    assert select(ob, "", 3, 0, 100_000, 25) == (0, [16, 4, 64, 32, 1, 0], -1)
+    assert select(ob, "", 3, 0, 100_000, 25) == (0, [16, 4, 0, 32, 1, 0], -1)
     for bad in ("3 0 16 4 8 2 32\n", "3 0 16 4 8 2 48 24\n", "3 0 16 4 8 9 32 24\n", "4 0 16 4 8 2 32 24\n",
                 "3 0 16 4 8 2 32 24 3\n", "3 0 16 4 8 2 32 24 2 9\n",
                 "3 0 16 4 8 2 32 24 2 0 5\n"):
@@ -59,4 +59,4 @@ def test_packaged_table_parses_and_covers_the_benchmark_configurations(ob):
     for ndims, n, nbrs in ((3, 100_000, 25.6), (3, 1_000_000, 28.3), (2, 4_000_000, 387.0), (3, 2_000_000, 14.3)):
         st, shapes, row = select(ob, path, ndims, 0, n, nbrs)
         assert st == 0 and row >= 0, (ndims, n)
-        assert shapes[2] in (32, 64, 128) and 8 <= shapes[3] <= 32
+        assert shapes[2] in (0, 32, 64, 128) and 8 <= shapes[3] <= 32
