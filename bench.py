@@ -38,7 +38,7 @@ JITTER = 0.1 * H
 SIGMA = 0.005 * H
 METRIC = "edges/s build+query+COO @1M pts; batched & fwd+bwd vs plain, exact edges"
 WORKLOAD = "sph_lattice_timestep_1M"
-# DRAM bytes per edge of the fill launch (k_expand), from an ncu capture of
+# DRAM bytes per edge of the fill launch (k_expand_direct), from an ncu capture of
 # the same kernel on the 70^3-point lattice (same density, radius and leaf
 # structure): dram__bytes_read.sum + dram__bytes_write.sum = 56.0 + 173.9 MB
 # for 9,623,512 edges.  The traffic is per edge, so it scales to the
@@ -365,7 +365,7 @@ def run_ours(args, rank, world, local):
                     "h2d_bytes_per_step": N * 12, "d2h_bytes_per_step": int(24 * e2e_edges / K),
                     "ms_per_step": e2e_ms_max / K},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_src, "kernel": "fill (k_expand)",
+                         "frac": achieved / peak, "peak_source": peak_src, "kernel": "fill (k_expand_direct)",
                          "traffic": (args.fill_traffic if args.fill_traffic is not None
                                      else FILL_DRAM_BYTES_PER_EDGE * e_per_step),
                          "traffic_source": "ncu dram bytes/edge of the fill kernel on the 343k-point "
@@ -526,6 +526,7 @@ def secondary_configs(ob, torch, dev):
     state = {}
 
     def fwd_bwd():
+        state.clear()  # the previous step's COO and gradient go back to the allocator first
         c = xd.detach().clone().requires_grad_(True)
         ob.update_point_set_(tns, sid, c.detach())
         ob.run_(tns)
@@ -535,6 +536,7 @@ def secondary_configs(ob, torch, dev):
         state["grad"], state["e"] = c.grad, e
         return e.senders.numel()
 
+    fwd_bwd()
     fwd_bwd()
     ms_d, e_d = _timed(torch, stream, fwd_bwd, 3)
     g = state["grad"].t().cpu().numpy().astype(np.float64)
@@ -579,7 +581,7 @@ def cpu_baseline(args, budget_s=None):
     import oracle
     budget_s = budget_s if budget_s is not None else args.cpu_budget
     nthreads = oracle.max_threads()
-    snaps = snapshots_np(PER, 4, 999)
+    snaps = snapshots_np(PER, 40, 999)  # more steps than the budget takes
     edges, secs, steps = 0, 0.0, 0
     for x in snaps[1:]:
         t0 = time.perf_counter()
