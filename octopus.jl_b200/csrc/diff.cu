@@ -205,143 +205,144 @@ __global__ void k_check_coo(const int32_t* __restrict__ snd, const int32_t* __re
     if (bad) atomicOr(status, bad);
 }
 
-// Warp layout of the self-pair adjoint: one warp takes kTwinPoints points in
-// the order `order` (the tree's Morton permutation, 1-based; null for
-// 0..n-1) and their segments' edges one per lane.  With a spatial order the
-// mirror edges read by the warps in flight lie in the segments of nearby
-// points, so they stay in L2 while the segments of all points in flight fit: a
-// few points per warp keep that working set small while the lanes still have
-// an edge each.  The order changes only which warp handles a point, never a
-// point's sum.  Each edge also checks the COO (receiver of its segment, sender
-// range, a mirror present); a failed check sets a status bit and the caller
-// takes the sorted path.
+// Layout of the self-pair adjoint: one group of kTwinLanes lanes per point,
+// the points taken in the order `order` (the tree's Morton permutation,
+// 1-based; null for 0..n-1).  With a spatial order the segments the warps in
+// flight read belong to nearby points, so they stay in L2.  Lane s of a group
+// takes the edges s, s + 8, s + 16, ... of its point's segment and adds their
+// contributions in that order in double precision; the group's eight partial
+// sums are then added in a fixed pairwise tree (xor shuffles; every lane ends
+// with the same bits).  The shape of the sum depends on the segment alone, so
+// the gradient is bit-reproducible whatever the order and the launch shape.
+// Each edge also checks the COO (receiver of its segment, sender range, a
+// mirror present); a failed check sets a status bit and the caller takes the
+// sorted path.
 constexpr int kTwinWarps = 4;
-constexpr int kTwinPoints = 4;  // points per warp (a power of two, at most 32)
+constexpr int kTwinLanes = 8;                    // lanes per point
+constexpr int kTwinGroups = 32 / kTwinLanes;     // points per warp
+
+// The point of this lane's group and its segment [k0, k0 + ne); p = -1 when
+// the group has no point.  Flags a bad order entry or an ungrouped COO.
+__device__ __forceinline__ void twin_point(int64_t n, int64_t m, const int32_t* __restrict__ order,
+                                           const int2* __restrict__ seg, int64_t sl, int& p, int& k0, int& ne,
+                                           int& bad) {
+    p = -1;
+    k0 = 0;
+    ne = 0;
+    if (sl >= n) return;
+    const int64_t pp = order ? (int64_t)order[sl] - 1 : sl;
+    if (pp < 0 || pp >= n) {
+        bad |= kAdjBadOrder;
+        return;
+    }
+    p = (int)pp;
+    const int2 sg = seg[p];
+    k0 = sg.x;
+    ne = sg.y - sg.x;
+    if (ne < 0 || (p == 0 && k0 != 0) || (p == n - 1 && sg.y != m)) {
+        bad |= kAdjUngrouped;
+        ne = 0;
+    }
+}
+
+// Sum of the group's lanes in a fixed pairwise tree, in every lane.
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+    for (int o = kTwinLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Index of the entry equal to `key` in snd[lo, hi) (one thread's scan of a
+// segment, in aligned blocks of four entries: one 16-byte load per block when
+// `vec`, the sender array being 16-byte aligned), -1 when absent.  Entries
+// outside [lo, hi) in the first and last block are masked off.  (The adjoint
+// kernel keeps its own form of the scan: measured faster there, slower here.)
+__device__ __forceinline__ int32_t find_mirror(const int32_t* __restrict__ snd, int32_t m, bool vec, int32_t lo,
+                                               int32_t hi, int32_t key) {
+    // unsigned: indices below 2^31, so qa + 4 cannot wrap
+    const uint32_t ulo = (uint32_t)lo, uhi = (uint32_t)hi, um = (uint32_t)m;
+    for (uint32_t qa = ulo & ~3u; qa < uhi; qa += 4) {
+        int32_t c[4];
+        if (vec && qa + 4 <= um) {
+            const int4 v = *reinterpret_cast<const int4*>(snd + qa);
+            c[0] = v.x;
+            c[1] = v.y;
+            c[2] = v.z;
+            c[3] = v.w;
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) c[u] = qa + u < um ? snd[qa + u] : 0;
+        }
+        unsigned mm = (c[0] == key ? 1u : 0u) | (c[1] == key ? 2u : 0u) | (c[2] == key ? 4u : 0u) |
+                      (c[3] == key ? 8u : 0u);
+        if (qa < ulo) mm &= 0xfu << (ulo - qa);
+        if (qa + 4 > uhi) mm &= 0xfu >> (qa + 4 - uhi);
+        if (mm) return (int32_t)(qa + __ffs(mm) - 1);
+    }
+    return -1;
+}
 
 // Pass 2 of the searching adjoint: each edge's mirror found by scanning its
-// sender's segment, term(k) - term(mirror) summed per point.  Measured on
-// B200 at 2M points, these two passes (1.19 ms) beat one pass that searches
-// and reads the mirror's cotangents itself (1.63 ms): the term records
-// stream in one coalesced pass before the searching pass reads them.
-// One warp takes kTwinPoints points in the order `order` (the tree's Morton
-// permutation, 1-based; null for 0..n-1) and their segments' edges one per
-// lane.  With a spatial order the twins read by the warps in flight lie in
-// the segments of nearby points, so they stay in L2 while the segments of
-// all points in flight fit: a few points per warp keep that working set
-// small while the lanes still have an edge each.  The order changes only
-// which warp handles a point, never a point's sum.  Each edge also checks
-// the COO (receiver of its segment, sender range, a twin present); a failed
-// check sets a status bit and the caller takes the sorted path.  `vec`: the
-// sender array is 16-byte aligned, so the twin scan reads four entries per
-// load.
-
+// sender's segment, term(k) - term(mirror) summed per point.  The term
+// records stream in one coalesced pass (k_edge_terms) before this pass reads
+// them.  `vec`: the sender array is 16-byte aligned, so the scan reads four
+// entries per load.
 template <class T>
 __global__ void __launch_bounds__(kTwinWarps * 32) k_adjoint_twins(
     int64_t n, int64_t m, const int32_t* __restrict__ order, const int2* __restrict__ seg,
     const int32_t* __restrict__ snd, const int32_t* __restrict__ rcv, const Term4<T>* __restrict__ term, int ndims,
     bool vec, T* __restrict__ grad, int* __restrict__ status) {
-    __shared__ double snet[kTwinWarps][3][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t s0 = ((int64_t)blockIdx.x * kTwinWarps + w) * kTwinPoints;
-    if (s0 >= n) return;  // warp-uniform
-    const int64_t sl = s0 + lane;
-    int p = -1, k0 = 0, ne = 0;
-    int bad = 0;
-    if (lane < kTwinPoints && sl < n) {
-        const int64_t pp = order ? (int64_t)order[sl] - 1 : sl;
-        if (pp < 0 || pp >= n) {
-            bad |= kAdjBadOrder;
-        } else {
-            p = (int)pp;
-            const int2 sg = seg[p];
-            k0 = sg.x;
-            ne = sg.y - sg.x;
-            if (ne < 0 || (p == 0 && k0 != 0) || (p == n - 1 && sg.y != m)) {
-                bad |= kAdjUngrouped;
-                ne = 0;
-            }
-        }
-    }
-    int incl = ne;  // edge counts fit int32 (n_edges < 2^31)
-#pragma unroll
-    for (int o = 1; o < kTwinPoints; o <<= 1) {
-        const int a = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += a;
-    }
-    const int excl = incl - ne;
-    const int total = __shfl_sync(0xffffffffu, incl, kTwinPoints - 1);
+    const int lane = threadIdx.x & 31, sub = lane & (kTwinLanes - 1);
+    const int64_t w0 = ((int64_t)blockIdx.x * kTwinWarps + (threadIdx.x >> 5)) * kTwinGroups;
+    if (w0 >= n) return;  // warp-uniform
+    int bad = 0, p, k0, ne;
+    twin_point(n, m, order, seg, w0 + lane / kTwinLanes, p, k0, ne, bad);
     double acc[3] = {0.0, 0.0, 0.0};
-    for (int f0 = 0; f0 < total; f0 += 32) {
-        const int f = f0 + lane;
-        // owner of flat edge f: the first lane whose inclusive end exceeds f
-        int o = 0;
-#pragma unroll
-        for (int st = kTwinPoints / 2; st; st >>= 1) {
-            const int v = __shfl_sync(0xffffffffu, incl, o + st - 1);
-            if (v <= f) o += st;
+    for (int e = sub; e < ne; e += kTwinLanes) {
+        const int32_t k = k0 + e;
+        const int32_t i1 = p + 1;
+        const int32_t j1 = snd[k];
+        if (rcv[k] != i1) bad |= kAdjUngrouped;
+        const Term4<T> tk = term[k];
+        if (j1 < 1 || j1 > n) {
+            bad |= kAdjBadIndex;
+            continue;
         }
-        const int ko = __shfl_sync(0xffffffffu, k0, o);
-        const int eo = __shfl_sync(0xffffffffu, excl, o);
-        const int po = __shfl_sync(0xffffffffu, p, o);
-        double net[3] = {0.0, 0.0, 0.0};
-        if (f < total) {
-            const int32_t k = ko + (f - eo);
-            const int32_t i1 = po + 1;
-            const int32_t j1 = snd[k];
-            if (rcv[k] != i1) bad |= kAdjUngrouped;
-            const Term4<T> tk = term[k];
-            if (j1 < 1 || j1 > n) {
-                bad |= kAdjBadIndex;
-            } else {
-                const int2 sj = seg[j1 - 1];
-                int32_t tw = -1;
-                if (vec) {
-                    // aligned blocks of four entries; the last block of the
-                    // array is read entry by entry
-                    for (int32_t qa = sj.x & ~3; qa < sj.y && tw < 0; qa += 4) {
-                        int32_t c[4];
-                        if ((int64_t)qa + 3 < m) {
-                            const int4 v = *reinterpret_cast<const int4*>(snd + qa);
-                            c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
-                        } else {
-#pragma unroll
-                            for (int u = 0; u < 4; ++u) c[u] = (int64_t)qa + u < m ? snd[qa + u] : 0;
-                        }
-#pragma unroll
-                        for (int u = 3; u >= 0; --u)
-                            if (c[u] == i1 && (int64_t)qa + u >= sj.x && (int64_t)qa + u < sj.y) tw = qa + u;
-                    }
+        const int2 sj = seg[j1 - 1];
+        int32_t tw = -1;
+        if (vec) {
+            // aligned blocks of four entries; the last block of the array is
+            // read entry by entry
+            for (int32_t qa = sj.x & ~3; qa < sj.y && tw < 0; qa += 4) {
+                int32_t c[4];
+                if ((int64_t)qa + 3 < m) {
+                    const int4 v = *reinterpret_cast<const int4*>(snd + qa);
+                    c[0] = v.x;
+                    c[1] = v.y;
+                    c[2] = v.z;
+                    c[3] = v.w;
                 } else {
-                    for (int32_t q = sj.x; q < sj.y && tw < 0; q += 4) {
-                        int32_t c[4];
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) c[u] = (int64_t)q + u < sj.y ? snd[q + u] : 0;
-#pragma unroll
-                        for (int u = 3; u >= 0; --u)
-                            if (c[u] == i1 && (int64_t)q + u < sj.y) tw = q + u;
-                    }
+                    for (int u = 0; u < 4; ++u) c[u] = (int64_t)qa + u < m ? snd[qa + u] : 0;
                 }
-                if (tw < 0) {
-                    bad |= kAdjMissingTwin;
-                } else {
-                    const Term4<T> tt = term[tw];
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) net[d] = (double)tk.v[d] - (double)tt.v[d];
-                }
+                for (int u = 3; u >= 0; --u)
+                    if (c[u] == i1 && (int64_t)qa + u >= sj.x && (int64_t)qa + u < sj.y) tw = qa + u;
             }
+        } else {
+            tw = find_mirror(snd, (int32_t)m, false, sj.x, sj.y, i1);
         }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) snet[w][d][lane] = net[d];
-        __syncwarp();
-        // each lane adds the entries of its own segment, in edge order
-        const int e1 = min(incl, f0 + 32);
-        for (int e = max(excl, f0); e < e1; ++e) {
-#pragma unroll
-            for (int d = 0; d < 3; ++d) acc[d] += snet[w][d][e - f0];
+        if (tw < 0) {
+            bad |= kAdjMissingTwin;
+            continue;
         }
-        __syncwarp();
+        const Term4<T> tt = term[tw];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) acc[d] += (double)tk.v[d] - (double)tt.v[d];
     }
-    if (p >= 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = group_sum(acc[d]);
+    if (p >= 0 && sub == 0) {
 #pragma unroll
         for (int d = 0; d < 3; ++d)
             if (d < ndims) grad[(int64_t)ndims * p + d] = (T)acc[d];
@@ -382,98 +383,45 @@ __global__ void __launch_bounds__(kTwinWarps * 32) k_adjoint_mirror(
     const T* __restrict__ rel_disp, const T* __restrict__ rel_dist, const T* __restrict__ coords,
     const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r, T inv_r, T* __restrict__ grad,
     int* __restrict__ status) {
-    __shared__ double snet[kTwinWarps][3][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t s0 = ((int64_t)blockIdx.x * kTwinWarps + w) * kTwinPoints;
-    if (s0 >= n) return;  // warp-uniform
-    const int64_t sl = s0 + lane;
-    int p = -1, k0 = 0, ne = 0;
-    int bad = 0;
-    if (lane < kTwinPoints && sl < n) {
-        const int64_t pp = order ? (int64_t)order[sl] - 1 : sl;
-        if (pp < 0 || pp >= n) {
-            bad |= kAdjBadOrder;
-        } else {
-            p = (int)pp;
-            const int2 sg = seg[p];
-            k0 = sg.x;
-            ne = sg.y - sg.x;
-            if (ne < 0 || (p == 0 && k0 != 0) || (p == n - 1 && sg.y != m)) {
-                bad |= kAdjUngrouped;
-                ne = 0;
-            }
-        }
-    }
-    int incl = ne;
-#pragma unroll
-    for (int o = 1; o < kTwinPoints; o <<= 1) {
-        const int a = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += a;
-    }
-    const int excl = incl - ne;
-    const int total = __shfl_sync(0xffffffffu, incl, kTwinPoints - 1);
+    const int lane = threadIdx.x & 31, sub = lane & (kTwinLanes - 1);
+    const int64_t w0 = ((int64_t)blockIdx.x * kTwinWarps + (threadIdx.x >> 5)) * kTwinGroups;
+    if (w0 >= n) return;  // warp-uniform
+    int bad = 0, p, k0, ne;
+    twin_point(n, m, order, seg, w0 + lane / kTwinLanes, p, k0, ne, bad);
     double acc[3] = {0.0, 0.0, 0.0};
-    for (int f0 = 0; f0 < total; f0 += 32) {
-        const int f = f0 + lane;
-        int o = 0;
+    for (int e = sub; e < ne; e += kTwinLanes) {
+        const int32_t k = k0 + e;
+        if (rcv[k] != p + 1) bad |= kAdjUngrouped;
+        T rd[D], rn = T(0);
+        if (RECOMPUTE) {
+            const int32_t j = snd[k] - 1;
+            if (j < 0 || j >= n) {
+                bad |= kAdjBadIndex;
+                continue;
+            }
+            T diff[D];
+            const T d2 = dist2<T, D>(coords + (int64_t)D * j, coords + (int64_t)D * p, diff);
 #pragma unroll
-        for (int st = kTwinPoints / 2; st; st >>= 1) {
-            const int v = __shfl_sync(0xffffffffu, incl, o + st - 1);
-            if (v <= f) o += st;
+            for (int d = 0; d < D; ++d) rd[d] = mul_rn(-diff[d], inv_r);
+            rn = mul_rn(sqrt_rn(d2), inv_r);
+        } else {
+#pragma unroll
+            for (int d = 0; d < D; ++d) rd[d] = rel_disp[(int64_t)D * k + d];
+            rn = rel_dist[k];
         }
-        const int ko = __shfl_sync(0xffffffffu, k0, o);
-        const int eo = __shfl_sync(0xffffffffu, excl, o);
-        const int po = __shfl_sync(0xffffffffu, p, o);
-        double net[3] = {0.0, 0.0, 0.0};
-        if (f < total) {
-            const int32_t k = ko + (f - eo);
-            if (rcv[k] != po + 1) bad |= kAdjUngrouped;
-            bool ok = true;
-            int32_t j = -1;
-            if (RECOMPUTE) {
-                j = snd[k] - 1;
-                if (j < 0 || j >= n) {
-                    bad |= kAdjBadIndex;
-                    ok = false;
-                }
-            }
-            const int32_t t = mirror[k];
-            T rd[D], rn = T(0);
-            if (ok && !(t >= 0 && (int64_t)t < m)) {
-                bad |= kAdjMissingTwin;
-                ok = false;
-            }
-            if (RECOMPUTE) {
-                if (j >= 0 && j < n) {
-                    T diff[D];
-                    const T d2 = dist2<T, D>(coords + (int64_t)D * j, coords + (int64_t)D * po, diff);
-#pragma unroll
-                    for (int d = 0; d < D; ++d) rd[d] = mul_rn(-diff[d], inv_r);
-                    rn = mul_rn(sqrt_rn(d2), inv_r);
-                }
-            } else {
-#pragma unroll
-                for (int d = 0; d < D; ++d) rd[d] = rel_disp[(int64_t)D * k + d];
-                rn = rel_dist[k];
-            }
-            if (ok) {
-                const Term4<T> tk = mirror_term<T, D, RECOMPUTE>(rd, rn, d_disp, d_dist, k, r, T(1));
-                const Term4<T> tt = mirror_term<T, D, RECOMPUTE>(rd, rn, d_disp, d_dist, t, r, T(-1));
-#pragma unroll
-                for (int d = 0; d < 3; ++d) net[d] = (double)tk.v[d] - (double)tt.v[d];
-            }
+        const int32_t t = mirror[k];
+        if (!(t >= 0 && (int64_t)t < m)) {
+            bad |= kAdjMissingTwin;
+            continue;
         }
+        const Term4<T> tk = mirror_term<T, D, RECOMPUTE>(rd, rn, d_disp, d_dist, k, r, T(1));
+        const Term4<T> tt = mirror_term<T, D, RECOMPUTE>(rd, rn, d_disp, d_dist, t, r, T(-1));
 #pragma unroll
-        for (int d = 0; d < 3; ++d) snet[w][d][lane] = net[d];
-        __syncwarp();
-        const int e1 = min(incl, f0 + 32);
-        for (int e = max(excl, f0); e < e1; ++e) {
-#pragma unroll
-            for (int d = 0; d < 3; ++d) acc[d] += snet[w][d][e - f0];
-        }
-        __syncwarp();
+        for (int d = 0; d < 3; ++d) acc[d] += (double)tk.v[d] - (double)tt.v[d];
     }
-    if (p >= 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = group_sum(acc[d]);
+    if (p >= 0 && sub == 0) {
 #pragma unroll
         for (int d = 0; d < D; ++d) grad[(int64_t)D * p + d] = (T)acc[d];
     }
@@ -481,21 +429,14 @@ __global__ void __launch_bounds__(kTwinWarps * 32) k_adjoint_mirror(
 }
 
 // Mirror index of every edge of a self-pair COO grouped by receiver, by
-// scanning the sender's segment (off: int64 segment starts) -- for the
-// differentiable fill when the hit records were incomplete.  -1 when absent.
+// scanning the sender's segment (off: int64 segment starts); -1 when absent.
 __global__ void k_mirror_scan(const int32_t* __restrict__ snd, const int32_t* __restrict__ rcv, int64_t m, int64_t n,
                               const int64_t* __restrict__ off, int32_t* __restrict__ mirror) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= m) return;
     const int32_t i1 = rcv[k], j = snd[k] - 1;
-    int32_t t = -1;
-    if (j >= 0 && j < n)
-        for (int64_t q = off[j]; q < off[j + 1]; ++q)
-            if (snd[q] == i1) {
-                t = (int32_t)q;
-                break;
-            }
-    mirror[k] = t;
+    const bool vec = ((uintptr_t)snd & 15) == 0;
+    mirror[k] = (j >= 0 && j < n) ? find_mirror(snd, (int32_t)m, vec, (int32_t)off[j], (int32_t)off[j + 1], i1) : -1;
 }
 
 namespace {
@@ -592,7 +533,7 @@ int twins_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_
                                                                 nullptr, (const T*)d_disp, (const T*)d_dist, r, inv_r,
                                                                 term);
     const bool vec = ((uintptr_t)snd & 15) == 0;
-    k_adjoint_twins<T><<<(unsigned)div_up(n, kTwinPoints * kTwinWarps), 32 * kTwinWarps, 0, s>>>(
+    k_adjoint_twins<T><<<(unsigned)div_up(n, kTwinGroups * kTwinWarps), 32 * kTwinWarps, 0, s>>>(
         n, m, order, ctx.dseg.as<int2>(), snd, rcv, term, D, vec, (T*)grad, status);
     ctx.kernel_launches += 4;
     if ((err = cudaGetLastError())) return cuda_status(ctx, err, "adjoint launch");
@@ -712,7 +653,7 @@ int mirror_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32
     if ((err = cudaMemsetAsync(status, 0, 4, s))) return cuda_status(ctx, err, "status reset");
     k_segment_starts<<<div_up(n + 1, tb), tb, 0, s>>>(rcv, m, n, ctx.droff.as<int64_t>());
     k_seg_pairs<<<div_up(n, tb), tb, 0, s>>>(ctx.droff.as<int64_t>(), n, ctx.dseg.as<int2>());
-    const unsigned blocks = (unsigned)div_up(n, kTwinPoints * kTwinWarps);
+    const unsigned blocks = (unsigned)div_up(n, kTwinGroups * kTwinWarps);
     const bool vec = ((uintptr_t)snd & 15) == 0;
     if (coords)
         k_adjoint_mirror<T, D, true><<<blocks, 32 * kTwinWarps, 0, s>>>(

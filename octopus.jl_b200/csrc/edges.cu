@@ -503,54 +503,63 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     }
 }
 
+// Position (0..31) of the k-th set bit (k from 0) of m; k < popc(m).
+__device__ __forceinline__ int kth_set_bit(unsigned m, int k) {
+    int pos = 0;
+    int c = __popc(m & 0xffffu);
+    if (k >= c) { k -= c; m >>= 16; pos += 16; }
+    c = __popc(m & 0xffu);
+    if (k >= c) { k -= c; m >>= 8; pos += 8; }
+    c = __popc(m & 0xfu);
+    if (k >= c) { k -= c; m >>= 4; pos += 4; }
+    c = __popc(m & 0x3u);
+    if (k >= c) { k -= c; m >>= 2; pos += 2; }
+    c = (int)(m & 1u);
+    if (k >= c) pos += 1;
+    return pos;
+}
+
 // Fill pass from the records with direct stores, in original index order
 // (the default fill; k_expand below writes through bulk copies instead, a
-// tuned alternative): warp v writes the
-// edges of queries 32v .. 32v+31, which the COO stores contiguously, so its
-// stores cover whole sectors.  The warp's edges form one flat list, query
-// ql's first at flat index epre(ql), COO slot kq[ql] + flat index.  Records are expanded into shared memory
-// (lanes over consecutive records, each record's first hit at the running sum
-// of the hit counts before it), then each batch of flat edges is written with
-// lanes on consecutive edges.  Queries of an overflowed group (record count
-// kOverflowMark) are left to the walking fill.
+// tuned alternative).  Warp v owns queries 32v .. 32v+31, one per lane; their
+// records, query after query, form one flat list, and so do their edges, in
+// the same order (a record's hits are consecutive edges of its query).  The
+// warp loads the records 32 at a time (one per lane), scans their hit counts,
+// and writes the batch's edges 32 at a time, one per lane, each lane finding
+// its record and, through it, its query:
+//   * the items of a list (records of a query, edges of a record) that reach
+//     into a 32-wide window of the flat list set one bit each at their first
+//     index in the window (the one running into the window at bit 0), so the
+//     item holding window index l is the (popc of the bits up to l)-th of them
+//     after the first (ballot, reduce-or, popc; no search);
+//   * the edge's target is the k-th set bit of its record's mask, its query's
+//     coordinates, index and radius come from the query's lane by shuffles.
+// Edge f of the flat list goes to COO slot kb[q] + f of its query q (slots
+// relative to the warp's first slot).  Queries of an
+// overflowed group (record count kOverflowMark) are left to the walking fill.
 constexpr int kDirectWarps = 4;
-constexpr int kDirectCap = 512;  // staged positions per warp (at least 32: one record)
 
 template <class T, int D>
-struct DirectSmem {
-    int32_t pos[kDirectCap];
-    uint8_t who[kDirectCap];  // query (lane) of each staged position
-    long long kq[32];    // COO slot of each query's flat edge 0: first slot - epre
-    long long key[32];   // COO slot of each entry of a write batch
-    T qx[D][32];
-    T disp[D * 32];
-    T inv_r[32];
-    int32_t qpos[32];    // sorted position of each query
-    int32_t qi[32];      // 1-based receiver index of each query
-    int32_t base[32];    // index base of each query's point set
-    int32_t rpre[33];    // flat record index where each query starts
-};
-
-template <class T, int D>
-__global__ void __launch_bounds__(kDirectWarps * 32, 8) k_expand_direct(
+__global__ void __launch_bounds__(kDirectWarps * 32, sizeof(T) == 4 ? 10 : 1) k_expand_direct(
     int64_t nq, const int32_t* __restrict__ iperm, const SPt<T, D>* __restrict__ qpts,
     const SPt<T, D>* __restrict__ tpts, const int64_t* __restrict__ offsets, const int2* __restrict__ recs,
     int64_t rec_cap, const uint16_t* __restrict__ rcount, T inv_r, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, Batch bt) {
-    __shared__ DirectSmem<T, D> sm_all[kDirectWarps];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t i0 = ((int64_t)blockIdx.x * kDirectWarps + w) * 32;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t i0 = ((int64_t)blockIdx.x * kDirectWarps + (threadIdx.x >> 5)) * 32;
     if (i0 >= nq) return;  // warp-uniform
-    DirectSmem<T, D>& sm = sm_all[w];
     const int64_t i = i0 + lane;
     const bool valid = i < nq;
+    const int64_t K0 = offsets[i0];  // the warp's first COO slot
     const int32_t qp = valid ? iperm[i] : 0;
     int nr = valid ? rcount[qp] : 0;
-    long long cur = 0;
     int ne = 0;
+    long long krel = 0;
     if (valid && nr != kOverflowMark) {
-        cur = offsets[i];
-        ne = (int)(offsets[i + 1] - cur);
+        const int64_t c0 = offsets[i];
+        ne = (int)(offsets[i + 1] - c0);
+        krel = c0 - K0;
     } else {
         nr = 0;
     }
@@ -558,130 +567,104 @@ __global__ void __launch_bounds__(kDirectWarps * 32, 8) k_expand_direct(
     T r2 = T(0), ir = inv_r;
     int32_t start_node = 0, base = 0;
     cloud_params<T>(bt, qp, r2, ir, start_node, base);
-    int ie = ne, irc = nr;
+    const int32_t qi = q.idx - base + 1;
+    const bool feat = rdisp != nullptr;  // false: neighbor lists (CSR values) only
+    const unsigned le = full >> (31 - lane);  // lanes up to this one
+    // flat record and edge ranges of the queries
+    int rinc = nr, einc = ne;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const int a = __shfl_up_sync(0xffffffffu, ie, o);
-        const int b = __shfl_up_sync(0xffffffffu, irc, o);
+        const int a = __shfl_up_sync(full, rinc, o);
+        const int b = __shfl_up_sync(full, einc, o);
         if (lane >= o) {
-            ie += a;
-            irc += b;
+            rinc += a;
+            einc += b;
         }
     }
-    sm.kq[lane] = cur - (ie - ne);
-#pragma unroll
-    for (int d = 0; d < D; ++d) sm.qx[d][lane] = q.x[d];
-    sm.inv_r[lane] = ir;
-    sm.qpos[lane] = qp;
-    sm.qi[lane] = q.idx - base + 1;
-    sm.base[lane] = base;
-    sm.rpre[lane + 1] = irc;
-    if (lane == 0) sm.rpre[0] = 0;
-    __syncwarp();
-    const int total_r = __shfl_sync(0xffffffffu, irc, 31);
-    const bool feat = rdisp != nullptr;  // false: neighbor lists (CSR values) only
-    int used = 0;      // positions staged (warp-uniform)
-    int ebase = 0;     // flat edge index of pos[0]
-    int qr = 0;        // this lane's query, for records
-
-    // Writes flat edges [ebase, ebase + cnt) from the staged positions: four
-    // entries per lane in flight, rel_displacement through shared memory so
-    // that each store of the warp covers consecutive values.
-    auto write_batch = [&](int cnt) {
-        for (int f0 = 0; f0 < cnt; f0 += 4 * 32) {
-            int qv[4];
-            long long kv[4];
-            SPt<T, D> tp[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int f = f0 + 32 * u + lane;
-                if (f < cnt) {
-                    const int qe = sm.who[f];
-                    qv[u] = qe;
-                    kv[u] = sm.kq[qe] + (ebase + f);
-                    tp[u] = tpts[sm.pos[f]];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int fb = f0 + 32 * u;
-                if (fb >= cnt) break;
-                const int nb = min(32, cnt - fb);
-                if (lane < nb) {
-                    const int q2 = qv[u];
-                    const long long k = kv[u];
-                    senders[k] = tp[u].idx - sm.base[q2] + 1;
-                    if (feat) {
-                        const T iv = sm.inv_r[q2];
-                        T px[D], diff[D];
-#pragma unroll
-                        for (int d = 0; d < D; ++d) px[d] = sm.qx[d][q2];
-                        const T d2 = dist2<T, D>(tp[u].x, px, diff);
-                        receivers[k] = sm.qi[q2];
-                        rdist[k] = mul_rn(sqrt_rn(d2), iv);
-#pragma unroll
-                        for (int d = 0; d < D; ++d) sm.disp[D * lane + d] = mul_rn(-diff[d], iv);
-                        sm.key[lane] = k;
-                    }
-                }
-                if (feat) {
-                    __syncwarp();
-#pragma unroll
-                    for (int c = 0; c < D; ++c) {
-                        const int v = 32 * c + lane;  // value v of the batch: entry v / D, axis v % D
-                        const int ent = v / D;
-                        if (ent < nb) rdisp[D * sm.key[ent] + (v - D * ent)] = sm.disp[v];
-                    }
-                    __syncwarp();
-                }
-            }
-        }
-    };
-
-    for (int r0 = 0; r0 < total_r; r0 += 32) {
-        const int rho = r0 + lane;
+    const int rexc = rinc - nr;
+    const long long kb = krel - (einc - ne);  // slot of flat edge f of this query: kb + f
+    const int R = __shfl_sync(full, rinc, 31);
+    int32_t* snd_w = senders + K0;
+    int32_t* rcv_w = receivers + K0;
+    T* dist_w = rdist + K0;
+    T* disp_w = feat ? rdisp + D * K0 : nullptr;
+    int fdone = 0;  // flat edges of the earlier record batches
+    for (int rb = 0; rb < R; rb += 32) {
+        // record rho = rb + lane and its query
+        // (queries without records set no bit, so the k-th bit belongs to the
+        // k-th query lane that reaches into the window)
+        const bool qin = nr > 0 && rexc < rb + 32 && rinc > rb;
+        const unsigned qm = __ballot_sync(full, qin);
+        const unsigned qs = __reduce_or_sync(full, qin ? 1u << max(rexc - rb, 0) : 0u);
+        const int rq = kth_set_bit(qm, __popc(qs & le) - 1);  // query lane of this lane's record
+        const int32_t rqp = __shfl_sync(full, qp, rq);
+        const int rqx = __shfl_sync(full, rexc, rq);
+        const int rho = rb + lane;
         int2 rec = make_int2(0, 0);
-        if (rho < total_r) {
-            while (sm.rpre[qr + 1] <= rho) ++qr;
-            rec = recs[(int64_t)sm.qpos[qr] * rec_cap + (rho - sm.rpre[qr])];
-        }
-        const int p = __popc((unsigned)rec.y);
-        int incl = p;
+        if (rho < R) rec = recs[(int64_t)rqp * rec_cap + (rho - rqx)];
+        const int c = __popc((unsigned)rec.y);
+        int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int a = __shfl_up_sync(0xffffffffu, incl, o);
+            const int a = __shfl_up_sync(full, incl, o);
             if (lane >= o) incl += a;
         }
-        // Stage the round's records in parts that fit the free positions,
-        // writing the staged edges out whenever the next record does not fit.
-        int lo = 0, base_incl = 0;  // lanes below `lo` are staged (warp-uniform)
-        while (lo < 32) {
-            const bool fits = lane >= lo && incl - base_incl <= kDirectCap - used;
-            const int hi = lo + __popc(__ballot_sync(0xffffffffu, fits));
-            if (hi == lo) {
-                write_batch(used);
-                ebase += used;
-                used = 0;
-                continue;
+        const int excl = incl - c;
+        const int tot = __shfl_sync(full, incl, 31);
+        // two windows per round, both gathers in flight before either is written
+        for (int w0 = 0; w0 < tot; w0 += 64) {
+            int32_t tpos[2];
+            long long slot[2];
+            int eqw[2];
+            bool ok[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int wu = w0 + 32 * u;
+                const bool in = c > 0 && excl < wu + 32 && incl > wu;  // record reaches into the window
+                const int r0 = __ffs(__ballot_sync(full, in)) - 1;  // -1: the window is past the batch
+                const unsigned starts = __reduce_or_sync(full, in ? 1u << max(excl - wu, 0) : 0u);
+                const int ri = max(r0 + __popc(starts & le) - 1, 0);  // this lane's record
+                const int rx = __shfl_sync(full, rec.x, ri);
+                const unsigned ry = __shfl_sync(full, (unsigned)rec.y, ri);
+                const int rex = __shfl_sync(full, excl, ri);
+                const int eq = __shfl_sync(full, rq, ri);  // this lane's query
+                slot[u] = __shfl_sync(full, kb, eq) + (fdone + wu + lane);
+                const int qend = __shfl_sync(full, einc, eq);  // flat end of the query's edges
+                const int e = wu + lane;
+                ok[u] = r0 >= 0 && e < tot && fdone + e < qend;  // the last two always hold when records and counts agree
+                tpos[u] = ok[u] ? rx + kth_set_bit(ry, e - rex) : 0;
+                eqw[u] = eq;
             }
-            if (fits) {
-                int at = used + (incl - p - base_incl);
-                unsigned m = (unsigned)rec.y;
-                while (m) {
-                    const int j = __ffs(m) - 1;
-                    m &= m - 1;
-                    sm.who[at] = (uint8_t)qr;
-                    sm.pos[at++] = rec.x + j;
+            SPt<T, D> t[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+                if (ok[u]) t[u] = tpts[tpos[u]];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int eq = eqw[u];
+                const int32_t bq = __shfl_sync(full, base, eq);
+                if (feat) {
+                    const int32_t qiq = __shfl_sync(full, qi, eq);
+                    const T iv = __shfl_sync(full, ir, eq);
+                    T px[D];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) px[d] = __shfl_sync(full, q.x[d], eq);
+                    if (ok[u]) {
+                        T diff[D];
+                        const T d2 = dist2<T, D>(t[u].x, px, diff);
+                        snd_w[slot[u]] = t[u].idx - bq + 1;
+                        rcv_w[slot[u]] = qiq;
+                        dist_w[slot[u]] = mul_rn(sqrt_rn(d2), iv);
+#pragma unroll
+                        for (int d = 0; d < D; ++d) disp_w[(long long)D * slot[u] + d] = mul_rn(-diff[d], iv);
+                    }
+                } else if (ok[u]) {
+                    snd_w[slot[u]] = t[u].idx - bq + 1;
                 }
             }
-            const int hi_incl = __shfl_sync(0xffffffffu, incl, hi - 1);
-            used += hi_incl - base_incl;
-            base_incl = hi_incl;
-            lo = hi;
-            __syncwarp();
         }
+        fdone += tot;
     }
-    write_batch(used);
 }
 
 // Fill pass from the records, in original index order.  Warp v writes the
@@ -723,20 +706,6 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // Orders this thread's shared-memory writes before later bulk-copy reads.
 __device__ __forceinline__ void fence_smem_to_bulk() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Position (0..31) of the k-th set bit (k from 0) of m; k < popc(m).
-__device__ __forceinline__ int kth_set_bit(unsigned m, int k) {
-    int pos = 0;
-    int c = __popc(m & 0xffffu);
-    if (k >= c) { k -= c; m >>= 16; pos += 16; }
-    c = __popc(m & 0xffu);
-    if (k >= c) { k -= c; m >>= 8; pos += 8; }
-    c = __popc(m & 0xfu);
-    if (k >= c) { k -= c; m >>= 4; pos += 4; }
-    c = __popc(m & 0x3u);
-    if (k >= c) { k -= c; m >>= 2; pos += 2; }
-    if (k >= (int)(m & 1u)) pos += 1;
-    return pos;
-}
 
 // Shared-memory bytes of one warp's ring of `ring` edges.
 template <class T, int D, bool FEAT>
