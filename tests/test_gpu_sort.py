@@ -37,8 +37,9 @@ def test_sort_uniform_matches_oracle(ob, oracle_mod, n):
     assert_tree_equal(tns.trees[sid - 1], oracle_mod.build_tree(x, r))
 
 
-def test_sort_staged_passes_above_6m_keys(ob, oracle_mod):
-    """6.5M keys take the staged radix passes; permutation as the oracle's."""
+def test_sort_of_6_5m_keys_with_ties(ob, oracle_mod):
+    """6.5M keys (3,174 tiles of the point-carrying passes, 5,000 points per
+    tied cell): the permutation is the oracle's."""
     n = 6_500_000
     x = tied_points(n, 5000, 77)
     r = np.float32(0.004)
