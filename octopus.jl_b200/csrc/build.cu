@@ -1103,6 +1103,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, nullptr, n, t.spts.as<SPt<T, D>>(),
                                                                     t.iperm.as<int32_t>(), &hdr->status);
             ctx.kernel_launches += 2;
+            t.iperm_valid = true;
             perm = nullptr;
         } else {
             if ((err = ensure(t.look, onesweep_words(n, passes) * 4)))
@@ -1116,11 +1117,13 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             ep.inv_cs = inv_cs;
             ep.bt = bt;
             PhaseTimer pt_(ctx, PH_SORT);
+            // the inverse permutation is left to its first user (ensure_iperm)
             err = point_sort<T, D, K>(coords, ep, n, passes, t.keys[0].as<K>(), t.keys[1].as<K>(),
                                       t.spts.as<SPt<T, D>>(), t.spts_tmp.as<SPt<T, D>>(), t.vals[0].as<int32_t>(),
-                                      t.iperm.as<int32_t>(), t.look.as<uint32_t>(), &hdr->status, sms, ctx.wait_limit,
+                                      nullptr, t.look.as<uint32_t>(), &hdr->status, sms, ctx.wait_limit,
                                       ctx.withhold_tile, s, &ctx.kernel_launches);
             if (err) return cuda_status(ctx, err, "key sort launch");
+            t.iperm_valid = false;
             perm = t.vals[0].as<int32_t>();
             if (!bt.n_clouds) sorted = 0;
         }
@@ -1140,6 +1143,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
                 k_gather<T, D><<<div_up(n, kThreads), kThreads, 0, s>>>(coords, vp, n, t.spts.as<SPt<T, D>>(),
                                                                     t.iperm.as<int32_t>(), &hdr->status);
                 ctx.kernel_launches += 1;
+                t.iperm_valid = true;
             }
             {
                 PhaseTimer pt_(ctx, PH_REFIT);
@@ -1190,6 +1194,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
                                                              t.mvals2.as<int32_t>(), coords, ok, ov,
                                                              t.spts.as<SPt<T, D>>(), t.iperm.as<int32_t>());
             ctx.kernel_launches += 1;
+            t.iperm_valid = true;
         }
         skeys = ok;
         perm = ov;
@@ -1571,6 +1576,19 @@ int build_tree(Ctx& ctx, Tree& t, const void* coords, int64_t n, double radius) 
                           : build_typed<double, 2>(ctx, t, (const double*)coords, n, radius);
     if (st == OK) t.built = true;
     return st;
+}
+
+int ensure_iperm(Ctx& ctx, const Tree& t) {
+    if (t.iperm_valid || t.n == 0) return OK;
+    if (!t.perm_dev) return set_error(ctx, ERR_STATE, "inverse permutation: the tree has no sorted order");
+    OctHeader* hdr = t.hdr.as<OctHeader>();
+    k_inverse_perm<<<(unsigned)div_up(t.n, kSortThreads), kSortThreads, 0, ctx.stream>>>(
+        t.perm_dev, t.n, t.iperm.as<int32_t>(), &hdr->status);
+    ctx.kernel_launches += 1;
+    const cudaError_t err = cudaGetLastError();
+    if (err) return cuda_status(ctx, err, "inverse permutation launch");
+    t.iperm_valid = true;
+    return OK;
 }
 
 namespace {

@@ -1130,6 +1130,8 @@ int fill_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
     PhaseTimer pt_(ctx, PH_FILL);
     const int64_t ng = q.n_groups;
     if (ctx.rec_cap) {
+        const int st = ensure_iperm(ctx, q);  // the fill visits the queries in original index order
+        if (st != OK) return st;
         const bool feat = rel_disp != nullptr;
         auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
         const int bulk_ok = aligned(senders) && (!feat || (aligned(receivers) && aligned(rel_disp) && aligned(rel_dist)));

@@ -102,6 +102,9 @@ struct Tree {
     DevBuf spts;                 // SPt<T,D>[n] in Morton order
     DevBuf spts_tmp;             // SPt<T,D>[n]: the key sort's intermediate passes
     DevBuf iperm;                // int32 [n]: sorted position of each original point
+    // iperm holds the inverse of the current order (a full sort leaves it to
+    // the first caller that needs it: ensure_iperm)
+    mutable bool iperm_valid = false;
     const int32_t* perm_dev = nullptr;  // original index of each sorted position (null: identity)
     const void* skeys_dev = nullptr;    // sorted keys of the last build (key_bytes wide)
     DevBuf tnode;                // TNode<T,D>[capacity]
@@ -248,6 +251,9 @@ int edges_fill(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int32_
                int32_t* receivers, void* rel_disp, void* rel_dist, int64_t n_edges);
 int edges_fill_diff(Ctx& ctx, const Tree& t, int32_t* senders, int32_t* receivers, void* rel_disp, void* rel_dist,
                     int32_t* mirror, int64_t n_edges);
+// The inverse permutation of a built tree, computed on first use after a
+// full sort (the build itself does not need it).
+int ensure_iperm(Ctx& ctx, const Tree& t);
 int edges_mirror_scan(Ctx& ctx, const int32_t* snd, const int32_t* rcv, int64_t m, int64_t n, const int64_t* off,
                       int32_t* mirror);
 int traversal_stats(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, uint64_t* out, int n_out);

@@ -16,7 +16,8 @@
 //                   order and writes each digit's run contiguously.  The first
 //                   pass encodes from the coordinates; the last writes the
 //                   sorted keys, the sorted points and the permutation;
-//   k_inverse_perm  the inverse permutation.
+//   k_inverse_perm  the inverse permutation (when asked for; the build
+//                   leaves it to the first caller that needs it).
 //
 // Every wait is bounded (spin_limit polling rounds); one that runs out sets
 // DF_TIMEOUT, and every store still stays inside its array.
@@ -280,7 +281,8 @@ cudaError_t launch_point_pass(const T* coords, const EncodeParams<T>& ep, const 
 // on return keys_out holds the sorted keys, spts the sorted points, perm the
 // original index of each sorted position and iperm its inverse.  kt and ptmp
 // are scratch of n keys / points (used when passes > 1); `scratch` holds
-// onesweep_words(n, kOnesweepMaxPasses) words.  Launches 2 + passes kernels.
+// onesweep_words(n, kOnesweepMaxPasses) words.  Launches 1 + passes kernels,
+// plus k_inverse_perm when iperm is not null.
 template <class T, int D, class K>
 cudaError_t point_sort(const T* coords, const EncodeParams<T>& ep, int64_t n, int passes, K* keys_out, K* kt,
                        SPt<T, D>* spts, SPt<T, D>* ptmp, int32_t* perm, int32_t* iperm, uint32_t* scratch, int* status,
@@ -296,7 +298,6 @@ cudaError_t point_sort(const T* coords, const EncodeParams<T>& ep, int64_t n, in
     // last pass lands in (keys_out, spts).
     auto kb = [&](int p) { return ((passes - 1 - p) & 1) == 0 ? keys_out : kt; };
     auto pb = [&](int p) { return ((passes - 1 - p) & 1) == 0 ? spts : ptmp; };
-    *launches += 1;  // the inverse permutation
     if (passes == 1) {
         if ((e = launch_point_pass<T, D, K, true, true>(coords, ep, nullptr, nullptr, keys_out, spts, perm, iperm, n, 0,
                                                         ntiles, scratch, status, spin_limit, withhold, s)))
@@ -315,7 +316,11 @@ cudaError_t point_sort(const T* coords, const EncodeParams<T>& ep, int64_t n, in
                                                          spin_limit, withhold, s)))
             return e;
     }
-    k_inverse_perm<<<(unsigned)((n + kSortThreads - 1) / kSortThreads), kSortThreads, 0, s>>>(perm, n, iperm, status);
+    if (iperm) {
+        k_inverse_perm<<<(unsigned)((n + kSortThreads - 1) / kSortThreads), kSortThreads, 0, s>>>(perm, n, iperm,
+                                                                                                   status);
+        *launches += 1;
+    }
     return cudaGetLastError();
 }
 

@@ -103,6 +103,10 @@ int zsort_apply(Ctx& ctx, const Tree& t, const void* in, void* out, int64_t n, i
     if (n == 0) return OK;
     if (!in || !out || in == out) return set_error(ctx, ERR_ARGUMENT, "apply_zsort: input and output must be distinct");
     // direction 0: gather by perm (sorted -> original); 1: gather by its inverse.
+    if (direction == 1) {
+        const int st = ensure_iperm(ctx, t);
+        if (st != OK) return st;
+    }
     const int32_t* src = direction == 0 ? t.perm_dev : t.iperm.as<int32_t>();
     const uintptr_t a = (uintptr_t)in | (uintptr_t)out | (uintptr_t)row_bytes;
     if (a % 16 == 0) launch<uint4>(in, out, src, n, row_bytes, ctx.stream);
