@@ -165,11 +165,20 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     // reports cloud-local indices.
     int32_t base = 0;
     cloud_params<T>(bt, grp.x, r2, inv_r, start_node, base);
+    // The group's box.  Plain min/max suffice here (the coordinates are finite,
+    // and which zero a tie keeps does not move the box), unlike the build's
+    // bounds, which follow Julia's min/max.
     T qlo[D], qhi[D];
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        qlo[d] = warp_min(q.x[d]);
-        qhi[d] = warp_max(q.x[d]);
+        T lo = q.x[d], hi = q.x[d];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        qlo[d] = lo;
+        qhi[d] = hi;
     }
     if (nbox > 1) {
         // sub-boxes over runs of 16 (nbox 2) or 8 (nbox 4) lanes; a lane
