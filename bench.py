@@ -58,12 +58,12 @@ def phase_bytes(n, e, n_nodes, path, passes=3):
     else:
         # digit counts read the coordinates (12); the first pass reads them
         # again and writes key + point (12 + 20); a middle pass moves key +
-        # point (20 + 20); the last also writes the permutation and its
-        # inverse (20 + 20 + 4 + 4)
+        # point (20 + 20); the last also writes the permutation (20 + 20 + 4)
+        # (its inverse is scattered later, on first use by the fill)
         if passes <= 1:
-            b["sort"] = (12 + 12 + 20 + 8) * n
+            b["sort"] = (12 + 12 + 20 + 4) * n
         else:
-            b["sort"] = (12 + 32 + 40 * (passes - 2) + 48) * n
+            b["sort"] = (12 + 32 + 40 * (passes - 2) + 44) * n
     b["refit"] = 16 * n + 2 * 32 * n_nodes          # sorted points in; node records read and written
     if e:
         b["fill"] = (12 + 4 * 3) * e + 8 * n        # (12 + 4D) E + 8N
