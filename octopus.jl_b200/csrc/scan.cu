@@ -1,5 +1,6 @@
-// Device-wide exclusive scan, reduce-then-scan in three launches.  No kernel
-// waits on another block, so there is nothing to spin on.
+// Device-wide exclusive scan, reduce-then-scan in two launches (three above
+// kInlineTiles tiles).  No kernel waits on another block, so there is nothing
+// to spin on.
 #include "scan.cuh"
 
 namespace oct {
@@ -38,13 +39,27 @@ __global__ void __launch_bounds__(1024) k_scan_tiles(int64_t* __restrict__ tile_
 }
 
 // Final pass: each tile scans its items in order (blocked per thread) and
-// adds the tile offset.
-template <class In, class Out>
+// adds the tile offset.  SUMS: tile_off holds the tiles' sums (not yet
+// scanned) and each block adds up those before its own (at most
+// kInlineTiles of them, a few loads per thread), so no separate launch scans
+// them; the last block also writes the total to *d_total.
+template <class In, class Out, bool SUMS>
 __global__ void __launch_bounds__(kScanThreads) k_scan_final(const In* in, int64_t n,
-                                                             const int64_t* __restrict__ tile_off, Out* out) {
+                                                             const int64_t* __restrict__ tile_off, Out* out,
+                                                             int64_t* __restrict__ d_total) {
     __shared__ int64_t sm[kScanThreads / 32 + 1];
     __shared__ In stage[kScanTile];
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    int64_t toff;
+    if (SUMS) {
+        int64_t part = 0;
+        for (int j = threadIdx.x; j < (int)blockIdx.x; j += kScanThreads) part += tile_off[j];
+        int64_t before;
+        block_exclusive_scan<int64_t>(part, sm, &before);
+        toff = before;
+    } else {
+        toff = tile_off[blockIdx.x];
+    }
     // Coalesced load into shared memory, then each thread owns kScanItems
     // consecutive elements.
 #pragma unroll
@@ -62,14 +77,17 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const In* in, int64
         s += v[it];
     }
     int64_t tot;
-    int64_t run = block_exclusive_scan<int64_t>(s, sm, &tot) + tile_off[blockIdx.x];
+    int64_t run = block_exclusive_scan<int64_t>(s, sm, &tot) + toff;
 #pragma unroll
     for (int it = 0; it < kScanItems; ++it) {
         const int64_t i = base + (int64_t)threadIdx.x * kScanItems + it;
         if (i < n) out[i] = (Out)run;
         run += v[it];
     }
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = (Out)(tile_off[blockIdx.x] + tot);
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+        out[n] = (Out)(toff + tot);
+        if (SUMS && d_total) *d_total = toff + tot;
+    }
 }
 
 // Short inputs in one launch: each thread sums, then writes, its own run of
@@ -111,8 +129,12 @@ int exclusive_scan(const In* in, Out* out, int64_t n, int64_t* d_total, int64_t*
     }
     const int ntiles = div_up(n, kScanTile);
     k_scan_tile_sums<In><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp);
+    if (ntiles <= kInlineTiles) {
+        k_scan_final<In, Out, true><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp, out, d_total);
+        return 2;
+    }
     k_scan_tiles<<<1, 1024, 0, s>>>(tile_tmp, ntiles, d_total);
-    k_scan_final<In, Out><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp, out);
+    k_scan_final<In, Out, false><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp, out, nullptr);
     return 3;
 }
 

@@ -40,7 +40,8 @@ template <class T> __device__ __forceinline__ T block_exclusive_scan(T v, T* sme
     return res;
 }
 
-// Both return the number of kernels launched (1 for n <= kSmallScan, else 3).
+// Both return the number of kernels launched (1 for n <= kSmallScan, 2 up to
+// kInlineTiles tiles, else 3).
 int exclusive_scan_i32_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* d_total,
                            int64_t* tile_tmp, cudaStream_t s);
 // In-place capable int32 scan; `out` holds n + 1 elements.
@@ -48,5 +49,8 @@ int exclusive_scan_i32_i32(const int32_t* in, int32_t* out, int64_t n, int64_t* 
 constexpr int kSmallScanThreads = 1024;
 constexpr int64_t kSmallScan = 32 * kSmallScanThreads;  // one block scans up to this many
 inline int64_t scan_tmp_elems(int64_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
+// Up to this many tiles (8M inputs) each final block adds up the sums of the
+// tiles before it itself.
+constexpr int kInlineTiles = 4096;
 
 }  // namespace oct
