@@ -401,20 +401,26 @@ def _pair_index(tns: TNS, q: int, t: int) -> int:
         raise OctopusError(f"build_edges!: pair ({q}, {t}) not registered; call set_active_search! first") from None
 
 
-def _resize_buffer(buf: EdgeBuffer, T, ndims, n_edges, device):
-    """Size the buffer's arrays to n_edges.  The arrays are views of grow-only
-    backing storage (1.25x slack), so a time-stepping loop whose edge count
-    fluctuates does not reallocate every step; like the reference, the arrays
-    are replaced whenever the edge count changes."""
-    dev = f"cuda:{device}"
+def _reserve_buffer(buf: EdgeBuffer, T, ndims, n_edges, device):
+    """Grow-only backing storage of the buffer's arrays (1.25x slack), so a
+    time-stepping loop whose edge count fluctuates does not reallocate every
+    step."""
     cap = getattr(buf, "_capacity", -1)
     if n_edges > cap:
+        dev = f"cuda:{device}"
         cap = n_edges + n_edges // 4
         buf._capacity = cap
         buf._snd = torch.empty(cap, dtype=torch.int32, device=dev)
         buf._rcv = torch.empty(cap, dtype=torch.int32, device=dev)
         buf._disp = torch.empty((cap, ndims), dtype=T, device=dev)
         buf._dist = torch.empty((cap, 1), dtype=T, device=dev)
+
+
+def _resize_buffer(buf: EdgeBuffer, T, ndims, n_edges, device):
+    """Size the buffer's arrays to n_edges: views of the grow-only backing
+    storage; like the reference, the arrays are replaced whenever the edge
+    count changes."""
+    _reserve_buffer(buf, T, ndims, n_edges, device)
     if buf.senders.numel() != n_edges or buf.senders.data_ptr() != buf._snd.data_ptr():
         buf.senders = buf._snd[:n_edges]
         buf.receivers = buf._rcv[:n_edges]
@@ -458,12 +464,15 @@ def build_edges_(tns: TNS, qid: int, tid: int) -> EdgeBuffer:
     ctx, qtree, ttree, excl, n_edges = got
     if n_edges > 2**31 - 1:
         raise OctopusError(f"build_edges!: {n_edges} edges exceed the Int32 edge count of EdgeBuffer")
-    _resize_buffer(buf, tns.T, tns.ndims, n_edges, tns.device)
+    # The fill goes into the backing storage first (its arrays start there, and
+    # _disp is (capacity, D) row-major = the (D, E) column-major matrix), so the
+    # device is busy while the host makes the sized views.
+    _reserve_buffer(buf, tns.T, tns.ndims, n_edges, tns.device)
     if n_edges > 0:
-        rd = buf.rel_displacement.t()  # (E, D) contiguous view of the (D, E) column-major matrix
-        ctx.check(ctx.lib.oct_edges_fill(ctx.handle, qtree.handle, ttree.handle, excl, _ptr(buf.senders),
-                                         _ptr(buf.receivers), _ptr(rd), _ptr(buf.rel_dist_norm), n_edges),
+        ctx.check(ctx.lib.oct_edges_fill(ctx.handle, qtree.handle, ttree.handle, excl, _ptr(buf._snd),
+                                         _ptr(buf._rcv), _ptr(buf._disp), _ptr(buf._dist), n_edges),
                   "build_edges!")
+    _resize_buffer(buf, tns.T, tns.ndims, n_edges, tns.device)
     buf.materialized = True
     return buf
 
