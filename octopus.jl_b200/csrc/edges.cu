@@ -534,15 +534,16 @@ __device__ __forceinline__ int kth_set_bit(unsigned m, int k) {
 // records, query after query, form one flat list, and so do their edges, in
 // the same order (a record's hits are consecutive edges of its query).  The
 // warp loads the records 32 at a time (one per lane), scans their hit counts,
-// and writes the batch's edges 32 at a time, one per lane, each lane finding
-// its record and, through it, its query:
-//   * the items of a list (records of a query, edges of a record) that reach
-//     into a 32-wide window of the flat list set one bit each at their first
-//     index in the window (the one running into the window at bit 0), so the
-//     item holding window index l is the (popc of the bits up to l)-th of them
-//     after the first (ballot, reduce-or, popc; no search);
-//   * the edge's target is the k-th set bit of its record's mask, its query's
-//     coordinates, index and radius come from the query's lane by shuffles.
+// lists each edge's (record lane, bit) in a per-warp shared-memory table (each
+// record lane writes its hits at its edges' slots), and writes the batch's
+// edges 32 at a time, one per lane:
+//   * a record's query: the queries whose records reach into the 32-record
+//     window set one bit each at their first record in the window (the one
+//     running into the window at bit 0), so the query of record l is the
+//     (popc of the bits up to l)-th of them (ballot, reduce-or, popc; no search);
+//   * an edge's target is its record's leaf position plus the bit from the
+//     table; its query's coordinates, index and radius come from the query's
+//     lane by shuffles.
 // Edge f of the flat list goes to COO slot kb[q] + f of its query q (slots
 // relative to the warp's first slot).  Queries of an
 // overflowed group (record count kOverflowMark) are left to the walking fill.
@@ -556,6 +557,9 @@ __global__ void __launch_bounds__(kDirectWarps * 32, sizeof(T) == 4 ? 10 : 1) k_
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, Batch bt) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    // per warp: (record lane << 5 | bit) of each edge of the current record batch
+    __shared__ uint16_t sedge[kDirectWarps][32 * 32];
+    uint16_t* se = sedge[threadIdx.x >> 5];
     const int64_t i0 = ((int64_t)blockIdx.x * kDirectWarps + (threadIdx.x >> 5)) * 32;
     if (i0 >= nq) return;  // warp-uniform
     const int64_t i = i0 + lane;
@@ -620,6 +624,16 @@ __global__ void __launch_bounds__(kDirectWarps * 32, sizeof(T) == 4 ? 10 : 1) k_
         }
         const int excl = incl - c;
         const int tot = __shfl_sync(full, incl, 31);
+        // each record lane lists its hits at its edges' slots
+        __syncwarp();  // the previous batch's table has been read
+        {
+            unsigned mb = (unsigned)rec.y;
+            for (int k = excl; mb; ++k) {
+                se[k] = (uint16_t)((lane << 5) | (__ffs(mb) - 1));
+                mb &= mb - 1;
+            }
+        }
+        __syncwarp();
         // two windows per round, both gathers in flight before either is written
         for (int w0 = 0; w0 < tot; w0 += 64) {
             int32_t tpos[2];
@@ -629,19 +643,15 @@ __global__ void __launch_bounds__(kDirectWarps * 32, sizeof(T) == 4 ? 10 : 1) k_
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
                 const int wu = w0 + 32 * u;
-                const bool in = c > 0 && excl < wu + 32 && incl > wu;  // record reaches into the window
-                const int r0 = __ffs(__ballot_sync(full, in)) - 1;  // -1: the window is past the batch
-                const unsigned starts = __reduce_or_sync(full, in ? 1u << max(excl - wu, 0) : 0u);
-                const int ri = max(r0 + __popc(starts & le) - 1, 0);  // this lane's record
+                const int e = wu + lane;
+                const int sv = e < tot ? se[e] : 0;
+                const int ri = sv >> 5;  // this lane's record
                 const int rx = __shfl_sync(full, rec.x, ri);
-                const unsigned ry = __shfl_sync(full, (unsigned)rec.y, ri);
-                const int rex = __shfl_sync(full, excl, ri);
                 const int eq = __shfl_sync(full, rq, ri);  // this lane's query
                 slot[u] = __shfl_sync(full, kb, eq) + (fdone + wu + lane);
                 const int qend = __shfl_sync(full, einc, eq);  // flat end of the query's edges
-                const int e = wu + lane;
-                ok[u] = r0 >= 0 && e < tot && fdone + e < qend;  // the last two always hold when records and counts agree
-                tpos[u] = ok[u] ? rx + kth_set_bit(ry, e - rex) : 0;
+                ok[u] = e < tot && fdone + e < qend;  // the second always holds when records and counts agree
+                tpos[u] = ok[u] ? rx + (sv & 31) : 0;
                 eqw[u] = eq;
             }
             SPt<T, D> t[2];
