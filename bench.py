@@ -40,10 +40,10 @@ METRIC = "edges/s build+query+COO @1M pts; batched & fwd+bwd vs plain, exact edg
 WORKLOAD = "sph_lattice_timestep_1M"
 # DRAM bytes per edge of the fill launch (k_expand_direct), from an ncu capture of
 # the same kernel on the 70^3-point lattice (same density, radius and leaf
-# structure): dram__bytes_read.sum + dram__bytes_write.sum = 57.1 + 178.0 MB
+# structure): dram__bytes_read.sum + dram__bytes_write.sum = 57.2 + 178.5 MB
 # for 9,623,512 edges.  The traffic is per edge, so it scales to the
 # 1M-point launch by edge count.
-FILL_DRAM_BYTES_PER_EDGE = 24.4
+FILL_DRAM_BYTES_PER_EDGE = 24.5
 
 
 def phase_bytes(n, e, n_nodes, path, passes=3):
