@@ -39,6 +39,8 @@ constexpr int kThreads = 256;
 template <class T, int D>
 __global__ void __launch_bounds__(kThreads) k_bounds(const T* __restrict__ coords, int64_t n,
                                                      double* __restrict__ partials, OctHeader* hdr) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ T smin[kThreads / 32][D], smax[kThreads / 32][D];
     __shared__ int snan;
     __shared__ bool is_last;
@@ -250,6 +252,8 @@ template <int D, class K>
 __global__ void __launch_bounds__(kThreads) k_mark(const K* __restrict__ skeys, int64_t n,
                                                    uint16_t* __restrict__ lohi, int32_t* __restrict__ blockcnt,
                                                    int nblocks, Batch bt) {
+    pdl_wait();
+    pdl_trigger();
     constexpr int MAXLEV = Dims<D>::bits;
     constexpr int NLEV = MAXLEV + 1;
     __shared__ K sk[kMarkTile + 64];
@@ -309,6 +313,8 @@ __global__ void __launch_bounds__(kThreads) k_emit_ids(int64_t n, const uint16_t
                                                        const int64_t* __restrict__ blockoff, int nblocks,
                                                        int64_t capacity, int32_t* __restrict__ first_child,
                                                        int2* __restrict__ nrange, OctHeader* hdr, Batch bt) {
+    pdl_wait();
+    pdl_trigger();
     constexpr int NLEV = Dims<D>::bits + 1;
     __shared__ int32_t wpre[NLEV][kThreads / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -364,6 +370,8 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
                                                          int32_t* __restrict__ parent, int32_t* __restrict__ arrive,
                                                          int32_t* __restrict__ chain, const int64_t* __restrict__ blockoff,
                                                          int nblocks, const OctHeader* hdr, Batch bt) {
+    pdl_wait();
+    pdl_trigger();
     constexpr int BITS = Dims<D>::bits;
     constexpr int NCH = Dims<D>::nch;
     const int64_t nn = hdr->n_nodes;
@@ -457,6 +465,8 @@ __global__ void __launch_bounds__(kThreads) k_refit(int64_t capacity, int64_t n,
                                                     const int2* __restrict__ nrange, const int32_t* __restrict__ parent,
                                                     int32_t* arrive, const SPt<T, D>* __restrict__ spts,
                                                     const OctHeader* hdr, Batch bt) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t nn = hdr->n_nodes;
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (nn > capacity || id >= nn) return;
@@ -544,6 +554,8 @@ __global__ void __launch_bounds__(kThreads) k_groups(const TNode<T, D>* __restri
                                                      const int32_t* __restrict__ parent, OctHeader* hdr, int gmax,
                                                      const K* __restrict__ skeys, const int2* __restrict__ nrange,
                                                      int32_t* __restrict__ gstart) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t nn = hdr->n_nodes;
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id == 0 && nn <= capacity) {
@@ -811,6 +823,8 @@ __global__ void __launch_bounds__(kThreads) k_resort_mark(const T* __restrict__ 
                                                           const K* __restrict__ keys, T inv_cs, OctHeader* hdr,
                                                           uint8_t* __restrict__ changed, int32_t* __restrict__ blockcnt,
                                                           K* __restrict__ mk, int32_t* __restrict__ mv, int64_t cap) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool c = false;
     K nk = 0;
@@ -852,6 +866,8 @@ __global__ void __launch_bounds__(kThreads) k_resort_mark(const T* __restrict__ 
 template <class K>
 __global__ void __launch_bounds__(kChunk / 2) k_moved_sort(const int64_t* __restrict__ m_ptr, int64_t cap,
                                                            K* __restrict__ mk, int32_t* __restrict__ mv) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ K sk[kChunk];
     __shared__ int32_t sv[kChunk];
     const int64_t m = *m_ptr;
@@ -903,6 +919,8 @@ template <class K>
 __global__ void __launch_bounds__(kThreads) k_moved_rank(const int64_t* __restrict__ m_ptr, int64_t cap,
                                                          const K* __restrict__ ck, const int32_t* __restrict__ cv,
                                                          K* __restrict__ sk, int32_t* __restrict__ sv) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t m = *m_ptr;
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m > cap || m <= kChunk || j >= m) return;  // one chunk is already in order
@@ -949,6 +967,8 @@ __global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, const int6
                                                            const T* __restrict__ coords, K* __restrict__ okeys,
                                                            int32_t* __restrict__ operm, SPt<T, D>* __restrict__ spts,
                                                            int32_t* __restrict__ iperm) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ int wsum[kThreads / 32];
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t m = *m_ptr;
@@ -1008,6 +1028,8 @@ __global__ void __launch_bounds__(kThreads) k_refit_prepare(int64_t nn, int64_t 
                                                             const int2* __restrict__ nrange,
                                                             int32_t* __restrict__ arrive, OctHeader* hdr,
                                                             int64_t n_groups, int32_t dfs_start) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id == 0) {
         hdr->n_nodes = nn;
@@ -1148,10 +1170,10 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             {
                 PhaseTimer pt_(ctx, PH_REFIT);
                 const int nb = div_up(t.n_nodes, kThreads);
-                k_refit_prepare<T, D><<<nb, kThreads, 0, s>>>(t.n_nodes, n, t.tnode.as<TNode<T, D>>(),
+                launch_pdl(k_refit_prepare<T, D>, nb, kThreads, 0, s, t.n_nodes, n, t.tnode.as<TNode<T, D>>(),
                                                                t.nrange.as<int2>(), t.arrive.as<int32_t>(), hdr,
                                                                t.n_groups, t.dfs_start);
-                k_refit<T, D><<<nb, kThreads, 0, s>>>(t.capacity, n, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
+                launch_pdl(k_refit<T, D>, nb, kThreads, 0, s, t.capacity, n, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
                                                        t.parent.as<int32_t>(), t.arrive.as<int32_t>(),
                                                        t.spts.as<SPt<T, D>>(), hdr, bt);
                 ctx.kernel_launches += 2;
@@ -1182,14 +1204,14 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             PhaseTimer pt_(ctx, PH_SORT);
             // Threads per chunk: width / 2 when the count is known, else 256.
             const int tpb = moved == kSpeculate ? 256 : std::max(32, width / 2);
-            k_moved_sort<K><<<(unsigned)nchunks, tpb, 0, s>>>(&hdr->n_moved, mcap, mk, mv);
+            launch_pdl(k_moved_sort<K>, (unsigned)nchunks, tpb, 0, s, &hdr->n_moved, mcap, mk, mv);
             ctx.kernel_launches += 1;
             if (nchunks > 1) {
-                k_moved_rank<K><<<div_up(mmax, kThreads), kThreads, 0, s>>>(&hdr->n_moved, mcap, mk, mv,
+                launch_pdl(k_moved_rank<K>, div_up(mmax, kThreads), kThreads, 0, s, &hdr->n_moved, mcap, mk, mv,
                                                                              t.mkeys2.as<K>(), t.mvals2.as<int32_t>());
                 ctx.kernel_launches += 1;
             }
-            k_resort_merge<T, D, K><<<nb, kThreads, 0, s>>>(n, &hdr->n_moved, mcap, kp, vp, t.rflag.as<uint8_t>(),
+            launch_pdl(k_resort_merge<T, D, K>, nb, kThreads, 0, s, n, &hdr->n_moved, mcap, kp, vp, t.rflag.as<uint8_t>(),
                                                              t.roff.as<int64_t>(), mk, mv, t.mkeys2.as<K>(),
                                                              t.mvals2.as<int32_t>(), coords, ok, ov,
                                                              t.spts.as<SPt<T, D>>(), t.iperm.as<int32_t>());
@@ -1241,13 +1263,13 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             return cuda_status(ctx, err, "cloud root reset");
         {
         PhaseTimer pt_(ctx, PH_TOPOLOGY);
-        k_mark<D, K><<<nblocks, kThreads, 0, s>>>(skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(), nblocks,
+        launch_pdl(k_mark<D, K>, nblocks, kThreads, 0, s, skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(), nblocks,
                                                   bt);
         ctx.kernel_launches += exclusive_scan_i32_i64(t.blockcnt.as<int32_t>(), t.blockoff.as<int64_t>(), nbc,
                                                       &hdr->n_nodes, t.scan_tmp.as<int64_t>(), s);
-        k_emit_ids<D><<<nblocks, kThreads, 0, s>>>(n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks, cap,
+        launch_pdl(k_emit_ids<D>, nblocks, kThreads, 0, s, n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks, cap,
                                                     t.fchild.as<int32_t>(), t.nrange.as<int2>(), hdr, bt);
-        k_emit_nodes<T, D, K><<<div_up(cap, kThreads), kThreads, 0, s>>>(
+        launch_pdl(k_emit_nodes<T, D, K>, div_up(cap, kThreads), kThreads, 0, s,
             skeys, n, cap, t.fchild.as<int32_t>(), t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
             t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.chain.as<int32_t>(), t.blockoff.as<int64_t>(), nblocks,
             hdr, bt);
@@ -1255,14 +1277,14 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         }
         {
         PhaseTimer pt_(ctx, PH_REFIT);
-        k_refit<T, D><<<div_up(cap, kThreads), kThreads, 0, s>>>(cap, n, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
+        launch_pdl(k_refit<T, D>, div_up(cap, kThreads), kThreads, 0, s, cap, n, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
                                                                   t.parent.as<int32_t>(), t.arrive.as<int32_t>(),
                                                                   t.spts.as<SPt<T, D>>(), hdr, bt);
         ctx.kernel_launches += 1;
         }
         {
             PhaseTimer pt_(ctx, PH_GROUPS);
-            k_groups<T, D, K><<<div_up(cap, kThreads), kThreads, 0, s>>>(
+            launch_pdl(k_groups<T, D, K>, div_up(cap, kThreads), kThreads, 0, s,
                 t.tnode.as<TNode<T, D>>(), cap, t.groups.as<int2>(), (int64_t)gcap, t.chain.as<int32_t>(),
                 t.parent.as<int32_t>(), hdr, gmax, skeys, t.nrange.as<int2>(),
                 bt.n_clouds ? nullptr : t.gstart.as<int32_t>());
@@ -1328,7 +1350,7 @@ int resort_mark(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int pre
         return cuda_status(ctx, err, "allocating refit-mode scratch");
     OctHeader* hdr = t.hdr.as<OctHeader>();
     PhaseTimer pt_(ctx, PH_ENCODE);
-    k_resort_mark<T, D, K><<<nb, kThreads, 0, s>>>(coords, n, t.vals[prev].as<int32_t>(), t.keys[prev].as<K>(),
+    launch_pdl(k_resort_mark<T, D, K>, nb, kThreads, 0, s, coords, n, t.vals[prev].as<int32_t>(), t.keys[prev].as<K>(),
                                                     T(1) / radius, hdr, t.rflag.as<uint8_t>(), t.rcnt.as<int32_t>(),
                                                     t.mkeys.as<K>(), t.mvals.as<int32_t>(), cap);
     ctx.kernel_launches += 1 + exclusive_scan_i32_i64(t.rcnt.as<int32_t>(), t.roff.as<int64_t>(), nb, nullptr,
@@ -1382,7 +1404,7 @@ int build_typed(Ctx& ctx, Tree& t, const T* coords, int64_t n, double radius_d) 
     if ((err = ensure(t.partials, (size_t)nb * 8 * 8))) return cuda_status(ctx, err, "allocating partials");
     {
         PhaseTimer pt_(ctx, PH_BOUNDS);
-        k_bounds<T, D><<<nb, kThreads, 0, s>>>(coords, n, t.partials.as<double>(), hdr);
+        launch_pdl(k_bounds<T, D>, nb, kThreads, 0, s, coords, n, t.partials.as<double>(), hdr);
         ctx.kernel_launches += 1;
     }
     // Refit mode with a reusable previous order: re-encode in that order now,

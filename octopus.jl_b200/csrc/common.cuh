@@ -214,6 +214,33 @@ __host__ __device__ __forceinline__ uint64_t compact_by_2(uint64_t x) {
     return x;
 }
 
+// ------------------------------------------- programmatic dependent launch --
+// A kernel launched with launch_pdl may be scheduled while the kernel before
+// it in the stream is still running.  Its first statement is pdl_wait(),
+// which returns once every earlier grid of the stream has completed and its
+// memory is visible, so nothing it reads or writes overlaps the earlier
+// kernel; pdl_trigger() then lets the next kernel be scheduled early in turn.
+// What overlaps is the launch and block scheduling between the kernels.  In
+// a launch without the attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <class... P, class... A>
+__host__ inline cudaError_t launch_pdl(void (*kern)(P...), int64_t grid, int block, size_t smem, cudaStream_t s,
+                                       A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<A&&>(args)...);
+}
+
 // ---------------------------------------------------------- warp helpers --
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;

@@ -126,6 +126,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edges(
     int2* __restrict__ recs, int64_t rec_cap, uint16_t* __restrict__ rcount, uint8_t* __restrict__ gflag, Batch bt,
     unsigned long long* __restrict__ stats, int max_seg, int multi_pop, int nbox, int prefetch,
     const int32_t* __restrict__ gstart) {
+    pdl_wait();
+    pdl_trigger();
     constexpr bool STAGE = PASS == EP_FILL;
     constexpr bool STATS = PASS == EP_STATS;
     long long st_t0 = 0, st_leaf = 0, st_pairs = 0;
@@ -555,6 +557,8 @@ __global__ void __launch_bounds__(kDirectWarps * 32, sizeof(T) == 4 ? 10 : 1) k_
     const SPt<T, D>* __restrict__ tpts, const int64_t* __restrict__ offsets, const int2* __restrict__ recs,
     int64_t rec_cap, const uint16_t* __restrict__ rcount, T inv_r, int32_t* __restrict__ senders,
     int32_t* __restrict__ receivers, T* __restrict__ rdisp, T* __restrict__ rdist, Batch bt) {
+    pdl_wait();
+    pdl_trigger();
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     // per warp: (record lane << 5 | bit) of each edge of the current record batch
@@ -1055,14 +1059,14 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
         PhaseTimer pt_(ctx, PH_COUNT);
         const int64_t ng = q.n_groups;
         if (ctx.rec_cap)
-            k_edges<T, D, EP_RECORD><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
+            launch_pdl(k_edges<T, D, EP_RECORD>, div_up(ng, kEdgeWarps), kEdgeThreads, 0, s,
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
                 nullptr, nullptr, nullptr, nullptr, (int*)(ctx.total.as<int64_t>() + 1), ctx.recs.as<int2>(),
                 ctx.rec_cap, ctx.rcount.as<uint16_t>(), ctx.gflag.as<uint8_t>(), t.batch(), nullptr, tn.max_seg,
                 tn.multi_pop, tn.sub_boxes, tn.prefetch, own_start(q, t));
         else
-            k_edges<T, D, EP_COUNT><<<div_up(ng, kEdgeWarps), kEdgeThreads, 0, s>>>(
+            launch_pdl(k_edges<T, D, EP_COUNT>, div_up(ng, kEdgeWarps), kEdgeThreads, 0, s,
                 q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
                 t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
                 nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr,
@@ -1130,7 +1134,7 @@ cudaError_t launch_expand(Ctx& ctx, const Tree& q, const Tree& t, T inv_r, int32
             return launch_expand_shape<T, D, FEAT, 128>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
                                                         bulk_ok);
         default:  // direct stores
-            k_expand_direct<T, D><<<div_up(q.n, 32 * kDirectWarps), kDirectWarps * 32, 0, ctx.stream>>>(
+            launch_pdl(k_expand_direct<T, D>, div_up(q.n, 32 * kDirectWarps), kDirectWarps * 32, 0, ctx.stream,
                 q.n, q.iperm.as<int32_t>(), q.spts.as<SPt<T, D>>(), t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
                 ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint16_t>(), inv_r, senders, receivers, (T*)rel_disp,
                 (T*)rel_dist, t.batch());

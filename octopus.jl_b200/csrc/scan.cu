@@ -9,6 +9,8 @@ namespace oct {
 template <class In>
 __global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const In* __restrict__ in, int64_t n,
                                                                  int64_t* __restrict__ tile_sums) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ int64_t sm[kScanThreads / 32 + 1];
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
     int64_t s = 0;
@@ -25,6 +27,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const In* __res
 // Exclusive scan of the tile sums by one block, carrying across chunks.
 __global__ void __launch_bounds__(1024) k_scan_tiles(int64_t* __restrict__ tile_sums, int64_t ntiles,
                                                      int64_t* __restrict__ d_total) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ int64_t sm[1024 / 32 + 1];
     int64_t carry = 0;
     for (int64_t base = 0; base < ntiles; base += blockDim.x) {
@@ -47,6 +51,8 @@ template <class In, class Out, bool SUMS>
 __global__ void __launch_bounds__(kScanThreads) k_scan_final(const In* in, int64_t n,
                                                              const int64_t* __restrict__ tile_off, Out* out,
                                                              int64_t* __restrict__ d_total) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ int64_t sm[kScanThreads / 32 + 1];
     __shared__ In stage[kScanTile];
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
@@ -96,6 +102,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const In* in, int64
 template <class In, class Out>
 __global__ void __launch_bounds__(kSmallScanThreads) k_scan_small(const In* in, int64_t n, Out* out,
                                                                   int64_t* __restrict__ d_total) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ int64_t sm[kSmallScanThreads / 32 + 1];
     const int64_t per = (n + kSmallScanThreads - 1) / kSmallScanThreads;
     const int64_t b = (int64_t)threadIdx.x * per;
@@ -124,17 +132,17 @@ int exclusive_scan(const In* in, Out* out, int64_t n, int64_t* d_total, int64_t*
         return 0;
     }
     if (n <= kSmallScan) {
-        k_scan_small<In, Out><<<1, kSmallScanThreads, 0, s>>>(in, n, out, d_total);
+        launch_pdl(k_scan_small<In, Out>, 1, kSmallScanThreads, 0, s, in, n, out, d_total);
         return 1;
     }
     const int ntiles = div_up(n, kScanTile);
-    k_scan_tile_sums<In><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp);
+    launch_pdl(k_scan_tile_sums<In>, ntiles, kScanThreads, 0, s, in, n, tile_tmp);
     if (ntiles <= kInlineTiles) {
-        k_scan_final<In, Out, true><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp, out, d_total);
+        launch_pdl(k_scan_final<In, Out, true>, ntiles, kScanThreads, 0, s, in, n, tile_tmp, out, d_total);
         return 2;
     }
-    k_scan_tiles<<<1, 1024, 0, s>>>(tile_tmp, ntiles, d_total);
-    k_scan_final<In, Out, false><<<ntiles, kScanThreads, 0, s>>>(in, n, tile_tmp, out, nullptr);
+    launch_pdl(k_scan_tiles, 1, 1024, 0, s, tile_tmp, ntiles, d_total);
+    launch_pdl(k_scan_final<In, Out, false>, ntiles, kScanThreads, 0, s, in, n, tile_tmp, out, nullptr);
     return 3;
 }
 
