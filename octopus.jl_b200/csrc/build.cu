@@ -305,14 +305,16 @@ __global__ void __launch_bounds__(kThreads) k_mark(const K* __restrict__ skeys, 
     }
 }
 
-// Node (L, k) -> BFS id.  Writes nrange[id] = {k, L} and tnode[id].a = the
-// id of the first child (the node (L+1, k)), or -1 for a leaf; k_emit_nodes
-// completes each node from these.
+// Node (L, k) -> BFS id.  Writes nrange[id] = {k, L}, first_child[id] = the
+// id of the first child (the node (L+1, k)) or -1 for a leaf, and
+// node_end[id] = one past the node's last position; k_emit_nodes completes
+// each node from these.
 template <int D>
 __global__ void __launch_bounds__(kThreads) k_emit_ids(int64_t n, const uint16_t* __restrict__ lohi,
                                                        const int64_t* __restrict__ blockoff, int nblocks,
                                                        int64_t capacity, int32_t* __restrict__ first_child,
-                                                       int2* __restrict__ nrange, OctHeader* hdr, Batch bt) {
+                                                       int2* __restrict__ nrange, int32_t* __restrict__ node_end,
+                                                       OctHeader* hdr, Batch bt) {
     pdl_wait();
     pdl_trigger();
     constexpr int NLEV = Dims<D>::bits + 1;
@@ -359,10 +361,29 @@ __global__ void __launch_bounds__(kThreads) k_emit_ids(int64_t n, const uint16_t
             prev = id;
         }
     }
+    // Node ends.  A level-L node ends where the level-L key prefix changes,
+    // so the nodes holding position k that end at k + 1 are those of levels
+    // lo(k + 1) .. hi(k) (every level at the end of the array).  The level-L
+    // node holding k is the last one starting at or before k: its id is k's
+    // inclusive rank among the level-L starts, minus one.
+    int nlo = __shfl_down_sync(0xffffffffu, lo, 1);  // lo(k + 1)
+    if (lane == 31 && k + 1 < n) nlo = lohi[k + 1] & 0xff;
+    if (k + 1 >= n) nlo = 0;
+    const bool ends = k < n && nlo <= hi;
+    const int elo = warp_min(ends ? nlo : NLEV), ehi = warp_max(ends ? hi : -1);
+    for (int L = elo; L <= ehi; ++L) {
+        const unsigned b = __ballot_sync(0xffffffffu, lo <= L && L <= hi);
+        if (ends && nlo <= L && L <= hi) {
+            const int32_t id = (int32_t)(blockoff[(int64_t)L * nblocks + blockIdx.x] + wpre[L][w] +
+                                         __popc(b & lanemask_lt()) + (int)((b >> lane) & 1u) - 1);
+            node_end[id] = (int32_t)(k + 1);
+        }
+    }
 }
 
-// Completes node `id`: its last position (end of its level-L key group), its
-// occupied child slots and the children's parent links.
+// Completes node `id`: its last position (from the end k_emit_ids left in
+// `arrive`, which is then reset for the refit), its occupied child slots and
+// the children's parent links.
 template <class T, int D, class K>
 __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ skeys, int64_t n, int64_t capacity,
                                                          const int32_t* __restrict__ first_child_in,
@@ -389,29 +410,7 @@ __global__ void __launch_bounds__(kThreads) k_emit_nodes(const K* __restrict__ s
         s0 = bt.coff[cloud];
         s1 = bt.coff[cloud + 1];
     }
-    int64_t e = s1;
-    if (L > 0) {
-        // Within one cloud, comparing whole keys >> sh compares Morton prefixes.
-        const int sh = D * (BITS - L);
-        const uint64_t pk = (uint64_t)skeys[k] >> sh;
-        if (((uint64_t)skeys[s1 - 1] >> sh) != pk) {
-            // Galloping search for the first position whose level-L prefix differs.
-            int64_t good = k, bad = s1, step = 1;
-            while (true) {
-                const int64_t p = k + step;
-                if (p >= s1) break;
-                if (((uint64_t)skeys[p] >> sh) != pk) { bad = p; break; }
-                good = p;
-                step <<= 1;
-            }
-            int64_t a = good + 1, b = bad;
-            while (a < b) {
-                const int64_t mid = (a + b) >> 1;
-                if (((uint64_t)skeys[mid] >> sh) != pk) b = mid; else a = mid + 1;
-            }
-            e = a;
-        }
-    }
+    const int64_t e = arrive[id];  // the end written by k_emit_ids
     TNode<T, D> nd;
     if (first_child < 0) {
         nd.a = (int32_t)k;
@@ -1268,7 +1267,7 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
         ctx.kernel_launches += exclusive_scan_i32_i64(t.blockcnt.as<int32_t>(), t.blockoff.as<int64_t>(), nbc,
                                                       &hdr->n_nodes, t.scan_tmp.as<int64_t>(), s);
         launch_pdl(k_emit_ids<D>, nblocks, kThreads, 0, s, n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks, cap,
-                                                    t.fchild.as<int32_t>(), t.nrange.as<int2>(), hdr, bt);
+                                                    t.fchild.as<int32_t>(), t.nrange.as<int2>(), t.arrive.as<int32_t>(), hdr, bt);
         launch_pdl(k_emit_nodes<T, D, K>, div_up(cap, kThreads), kThreads, 0, s,
             skeys, n, cap, t.fchild.as<int32_t>(), t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
             t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.chain.as<int32_t>(), t.blockoff.as<int64_t>(), nblocks,

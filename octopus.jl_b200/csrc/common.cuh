@@ -259,6 +259,10 @@ template <class T> __device__ __forceinline__ T warp_max(T v) {
     return v;
 }
 
+// Integers: one redux.sync instead of a shuffle tree.
+__device__ __forceinline__ int warp_min(int v) { return __reduce_min_sync(0xffffffffu, v); }
+__device__ __forceinline__ int warp_max(int v) { return __reduce_max_sync(0xffffffffu, v); }
+
 template <class T> __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
