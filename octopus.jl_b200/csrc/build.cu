@@ -34,6 +34,39 @@ namespace oct {
 constexpr int kThreads = 256;
 
 // ------------------------------------------------------------ 1. bounds --
+// Order key of an IEEE value: its bits with the magnitude bits flipped when
+// the sign is set, so that signed integer order is the value order of every
+// non-NaN value, -0.0 below +0.0 (Julia's min/max); the map is its own inverse.
+template <class T> struct OrdKey;
+template <> struct OrdKey<float> {
+    using I = int32_t;
+    static constexpr I kMag = 0x7fffffff, kExp = 0x7f800000;
+    static constexpr I kMaxKey = 0x7fffffff, kMinKey = (I)0x80000000;
+    __device__ static I bits(float x) { return __float_as_int(x); }
+    __device__ static I key(I b) { return b ^ ((b >> 31) & kMag); }
+    __device__ static float value(I k) { return __int_as_float(key(k)); }
+};
+template <> struct OrdKey<double> {
+    using I = long long;
+    static constexpr I kMag = 0x7fffffffffffffffLL, kExp = 0x7ff0000000000000LL;
+    static constexpr I kMaxKey = 0x7fffffffffffffffLL, kMinKey = (I)0x8000000000000000ULL;
+    __device__ static I bits(double x) { return __double_as_longlong(x); }
+    __device__ static I key(I b) { return b ^ ((b >> 63) & kMag); }
+    __device__ static double value(I k) { return __longlong_as_double(key(k)); }
+};
+__device__ __forceinline__ int32_t ord_warp_min(int32_t v) { return __reduce_min_sync(0xffffffffu, v); }
+__device__ __forceinline__ int32_t ord_warp_max(int32_t v) { return __reduce_max_sync(0xffffffffu, v); }
+__device__ __forceinline__ long long ord_warp_min(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ long long ord_warp_max(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 // Per-axis min/max (Julia min/max order) and a non-finite flag.  The last
 // block to finish folds the per-block partials into the header.
 template <class T, int D>
@@ -46,15 +79,21 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const T* __restrict__ coord
     __shared__ bool is_last;
     if (threadIdx.x == 0) snan = 0;
     __syncthreads();
-    T lo[D], hi[D];
+    // The fold runs on order keys (OrdKey): integer min/max give Julia's
+    // min/max of finite values, and a magnitude at or above the exponent
+    // mask marks a NaN or Inf (whose bounds then do not matter: the build
+    // fails).
+    using I = typename OrdKey<T>::I;
+    I klo[D], khi[D], mag = 0;
 #pragma unroll
-    for (int d = 0; d < D; ++d) { lo[d] = T(INFINITY); hi[d] = T(-INFINITY); }
-    int bad = 0;
+    for (int d = 0; d < D; ++d) { klo[d] = OrdKey<T>::kMaxKey; khi[d] = OrdKey<T>::kMinKey; }
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nthr = (int64_t)gridDim.x * blockDim.x;
     auto take = [&](int d, T x) {
-        if (!isfinite(x)) bad = 1;
-        lo[d] = jl_min(lo[d], x);
-        hi[d] = jl_max(hi[d], x);
+        const I b = OrdKey<T>::bits(x);
+        const I k = OrdKey<T>::key(b);
+        klo[d] = min(klo[d], k);
+        khi[d] = max(khi[d], k);
+        mag = max(mag, b & OrdKey<T>::kMag);
     };
     int64_t done = 0;  // points folded by the vector loop
     if constexpr (std::is_same<T, float>::value && D == 3) {
@@ -87,11 +126,13 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const T* __restrict__ coord
         for (int d = 0; d < D; ++d) take(d, coords[D * i + d]);
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    T lo[D], hi[D];
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        lo[d] = warp_min(lo[d]);
-        hi[d] = warp_max(hi[d]);
+        lo[d] = OrdKey<T>::value(ord_warp_min(klo[d]));
+        hi[d] = OrdKey<T>::value(ord_warp_max(khi[d]));
     }
+    const int bad = mag >= OrdKey<T>::kExp;
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&snan, 1);
     if (lane == 0) {
 #pragma unroll
