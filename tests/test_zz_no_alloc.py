@@ -163,6 +163,40 @@ def test_noalloc_count_total_is_refused_while_capturing(ob):
     assert ne.value == 0
 
 
+def test_noalloc_count_replays_in_a_cuda_graph(ob):
+    """Without the total (n_edges NULL) the call may be captured: the count and
+    its scan (kernels that start early on their predecessor, programmatic
+    dependent launch) replay from a CUDA graph with the regular entry point's
+    counts and offsets."""
+    x = uniform(20000, 3, 71)
+    tns, sid = _tns(ob, x, np.float32(0.05))
+    n = x.shape[0]
+    e = ob.build_edges(tns, sid, sid)
+    want_counts = torch.bincount(e.receivers.long() - 1, minlength=n).to(torch.int32)
+    want_offsets = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    want_offsets[1:] = torch.cumsum(want_counts.long(), 0)
+    _noalloc_count(tns, sid, sid, 1)  # set-up call, outside the capture
+    counts = torch.full((n,), -7, dtype=torch.int32, device="cuda")
+    offsets = torch.full((n + 1,), -7, dtype=torch.int64, device="cuda")
+    ctx = tns._ctx
+    h = tns.trees[sid - 1].handle
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        ctx.bind_stream()
+        st = ctx.lib.oct_edges_count_noalloc(ctx.handle, h, h, 1, C.c_void_p(counts.data_ptr()),
+                                             C.c_void_p(offsets.data_ptr()), None)
+    ctx.bind_stream()
+    ctx.check(st, "oct_edges_count_noalloc (captured)")
+    for _ in range(2):
+        counts.fill_(-7)
+        offsets.fill_(-7)
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(counts, want_counts)
+        assert torch.equal(offsets, want_offsets)
+    del g
+
+
 def test_noalloc_count_at_its_exact_limit(ob):
     """16,777,216 query points: the largest set, every tile of the fixed
     scratch in use."""
