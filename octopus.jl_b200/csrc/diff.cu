@@ -41,6 +41,8 @@ __device__ __forceinline__ void edge_term(int64_t k, const T* __restrict__ rel_d
 
 // off[i] = first edge whose (1-based) key is >= i + 1, for i in [0, n].
 __global__ void k_segment_starts(const int32_t* __restrict__ keys1, int64_t m, int64_t n, int64_t* __restrict__ off) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i > n) return;
     int64_t a = 0, b = m;
@@ -146,6 +148,8 @@ __global__ void k_edge_terms(int64_t m, int64_t n, const int32_t* __restrict__ s
                              const T* __restrict__ rel_disp, const T* __restrict__ rel_dist,
                              const T* __restrict__ coords, const T* __restrict__ d_disp,
                              const T* __restrict__ d_dist, T r, T inv_r, Term4<T>* __restrict__ term) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= m) return;
     T rd[D], rn = T(0);
@@ -182,6 +186,8 @@ __global__ void k_edge_terms(int64_t m, int64_t n, const int32_t* __restrict__ s
 
 // seg[i] = {first, end} of point i's edges, from off[i], off[i + 1].
 __global__ void k_seg_pairs(const int64_t* __restrict__ off, int64_t n, int2* __restrict__ seg) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) seg[i] = make_int2((int32_t)off[i], (int32_t)off[i + 1]);
 }
@@ -292,6 +298,8 @@ __global__ void __launch_bounds__(kTwinWarps * 32) k_adjoint_twins(
     int64_t n, int64_t m, const int32_t* __restrict__ order, const int2* __restrict__ seg,
     const int32_t* __restrict__ snd, const int32_t* __restrict__ rcv, const Term4<T>* __restrict__ term, int ndims,
     bool vec, T* __restrict__ grad, int* __restrict__ status) {
+    pdl_wait();
+    pdl_trigger();
     const int lane = threadIdx.x & 31, sub = lane & (kTwinLanes - 1);
     const int64_t w0 = ((int64_t)blockIdx.x * kTwinWarps + (threadIdx.x >> 5)) * kTwinGroups;
     if (w0 >= n) return;  // warp-uniform
@@ -383,6 +391,8 @@ __global__ void __launch_bounds__(kTwinWarps * 32) k_adjoint_mirror(
     const T* __restrict__ rel_disp, const T* __restrict__ rel_dist, const T* __restrict__ coords,
     const T* __restrict__ d_disp, const T* __restrict__ d_dist, T r, T inv_r, T* __restrict__ grad,
     int* __restrict__ status) {
+    pdl_wait();
+    pdl_trigger();
     const int lane = threadIdx.x & 31, sub = lane & (kTwinLanes - 1);
     const int64_t w0 = ((int64_t)blockIdx.x * kTwinWarps + (threadIdx.x >> 5)) * kTwinGroups;
     if (w0 >= n) return;  // warp-uniform
@@ -522,18 +532,18 @@ int twins_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_
     PhaseTimer pt_(ctx, PH_ADJOINT);
     int* status = adjoint_status(ctx);
     if ((err = cudaMemsetAsync(status, 0, 4, s))) return cuda_status(ctx, err, "status reset");
-    k_segment_starts<<<div_up(n + 1, tb), tb, 0, s>>>(rcv, m, n, ctx.droff.as<int64_t>());
-    k_seg_pairs<<<div_up(n, tb), tb, 0, s>>>(ctx.droff.as<int64_t>(), n, ctx.dseg.as<int2>());
+    launch_pdl(k_segment_starts, div_up(n + 1, tb), tb, 0, s, rcv, m, n, ctx.droff.as<int64_t>());
+    launch_pdl(k_seg_pairs, div_up(n, tb), tb, 0, s, ctx.droff.as<int64_t>(), n, ctx.dseg.as<int2>());
     Term4<T>* term = ctx.dterm.as<Term4<T>>();
     if (coords)
-        k_edge_terms<T, D, true><<<div_up(m, tb), tb, 0, s>>>(m, n, snd, rcv, nullptr, nullptr, (const T*)coords,
+        launch_pdl(k_edge_terms<T, D, true>, div_up(m, tb), tb, 0, s, m, n, snd, rcv, nullptr, nullptr, (const T*)coords,
                                                                (const T*)d_disp, (const T*)d_dist, r, inv_r, term);
     else
-        k_edge_terms<T, D, false><<<div_up(m, tb), tb, 0, s>>>(m, n, snd, rcv, (const T*)rel_disp, (const T*)rel_dist,
+        launch_pdl(k_edge_terms<T, D, false>, div_up(m, tb), tb, 0, s, m, n, snd, rcv, (const T*)rel_disp, (const T*)rel_dist,
                                                                 nullptr, (const T*)d_disp, (const T*)d_dist, r, inv_r,
                                                                 term);
     const bool vec = ((uintptr_t)snd & 15) == 0;
-    k_adjoint_twins<T><<<(unsigned)div_up(n, kTwinGroups * kTwinWarps), 32 * kTwinWarps, 0, s>>>(
+    launch_pdl(k_adjoint_twins<T>, (unsigned)div_up(n, kTwinGroups * kTwinWarps), 32 * kTwinWarps, 0, s,
         n, m, order, ctx.dseg.as<int2>(), snd, rcv, term, D, vec, (T*)grad, status);
     ctx.kernel_launches += 4;
     if ((err = cudaGetLastError())) return cuda_status(ctx, err, "adjoint launch");
@@ -651,16 +661,16 @@ int mirror_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32
     PhaseTimer pt_(ctx, PH_ADJOINT);
     int* status = adjoint_status(ctx);
     if ((err = cudaMemsetAsync(status, 0, 4, s))) return cuda_status(ctx, err, "status reset");
-    k_segment_starts<<<div_up(n + 1, tb), tb, 0, s>>>(rcv, m, n, ctx.droff.as<int64_t>());
-    k_seg_pairs<<<div_up(n, tb), tb, 0, s>>>(ctx.droff.as<int64_t>(), n, ctx.dseg.as<int2>());
+    launch_pdl(k_segment_starts, div_up(n + 1, tb), tb, 0, s, rcv, m, n, ctx.droff.as<int64_t>());
+    launch_pdl(k_seg_pairs, div_up(n, tb), tb, 0, s, ctx.droff.as<int64_t>(), n, ctx.dseg.as<int2>());
     const unsigned blocks = (unsigned)div_up(n, kTwinGroups * kTwinWarps);
     const bool vec = ((uintptr_t)snd & 15) == 0;
     if (coords)
-        k_adjoint_mirror<T, D, true><<<blocks, 32 * kTwinWarps, 0, s>>>(
+        launch_pdl(k_adjoint_mirror<T, D, true>, blocks, 32 * kTwinWarps, 0, s,
             n, m, order, ctx.dseg.as<int2>(), snd, rcv, mirror, nullptr, nullptr, (const T*)coords, (const T*)d_disp,
             (const T*)d_dist, r, inv_r, (T*)grad, status);
     else
-        k_adjoint_mirror<T, D, false><<<blocks, 32 * kTwinWarps, 0, s>>>(
+        launch_pdl(k_adjoint_mirror<T, D, false>, blocks, 32 * kTwinWarps, 0, s,
             n, m, order, ctx.dseg.as<int2>(), snd, rcv, mirror, (const T*)rel_disp, (const T*)rel_dist, nullptr,
             (const T*)d_disp, (const T*)d_dist, r, inv_r, (T*)grad, status);
     ctx.kernel_launches += 3;

@@ -84,6 +84,8 @@ __device__ __forceinline__ SPt<T, D> load_point(const T* __restrict__ coords, in
 template <class T, int D, class K>
 __global__ void __launch_bounds__(kSortThreads) k_point_counts(const T* __restrict__ coords, int64_t n, int passes,
                                                                EncodeParams<T> ep, uint32_t* __restrict__ counts) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ uint32_t c[kOnesweepMaxPasses][256];
     for (int p = 0; p < passes; ++p) c[p][threadIdx.x] = 0;
     __syncthreads();
@@ -123,6 +125,8 @@ __global__ void __launch_bounds__(kSortThreads) k_point_pass(
     K* __restrict__ kout, SPt<T, D>* __restrict__ pout, int32_t* __restrict__ perm, int32_t* __restrict__ iperm,
     int64_t n, int pass, int ntiles, uint32_t* __restrict__ scratch, int* __restrict__ status, int64_t spin_limit,
     int withhold_tile) {
+    pdl_wait();
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char pp_smem[];
     PointPassSmem<T, D, K>& sm = *reinterpret_cast<PointPassSmem<T, D, K>*>(pp_smem);
     const int shift = 8 * pass;
@@ -251,6 +255,8 @@ __global__ void __launch_bounds__(kSortThreads) k_point_pass(
 // wait ran out (DF_TIMEOUT is then set already) and is skipped.
 __global__ void __launch_bounds__(kSortThreads) k_inverse_perm(const int32_t* __restrict__ perm, int64_t n,
                                                                int32_t* __restrict__ iperm, int* __restrict__ status) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int32_t j = perm[k];
@@ -272,7 +278,7 @@ cudaError_t launch_point_pass(const T* coords, const EncodeParams<T>& ep, const 
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    kern<<<ntiles, kSortThreads, smem, s>>>(coords, ep, kin, pin, kout, pout, perm, iperm, n, pass, ntiles, scratch,
+    launch_pdl(kern, ntiles, kSortThreads, smem, s, coords, ep, kin, pin, kout, pout, perm, iperm, n, pass, ntiles, scratch,
                                            status, spin_limit, withhold);
     return cudaGetLastError();
 }
@@ -291,7 +297,7 @@ cudaError_t point_sort(const T* coords, const EncodeParams<T>& ep, int64_t n, in
     cudaError_t e = cudaMemsetAsync(scratch, 0, onesweep_words(n, passes) * 4, s);
     if (e != cudaSuccess) return e;
     const int hblocks = (int)std::min<int64_t>(ntiles, (int64_t)4 * std::max(sms, 1));
-    k_point_counts<T, D, K><<<hblocks, kSortThreads, 0, s>>>(coords, n, passes, ep, scratch);
+    launch_pdl(k_point_counts<T, D, K>, hblocks, kSortThreads, 0, s, coords, n, passes, ep, scratch);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     *launches += 1 + passes;
     // Pass p writes the final buffers when passes - 1 - p is even, so the
@@ -317,7 +323,7 @@ cudaError_t point_sort(const T* coords, const EncodeParams<T>& ep, int64_t n, in
             return e;
     }
     if (iperm) {
-        k_inverse_perm<<<(unsigned)((n + kSortThreads - 1) / kSortThreads), kSortThreads, 0, s>>>(perm, n, iperm,
+        launch_pdl(k_inverse_perm, (unsigned)((n + kSortThreads - 1) / kSortThreads), kSortThreads, 0, s, perm, n, iperm,
                                                                                                    status);
         *launches += 1;
     }
