@@ -1211,11 +1211,10 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
                 PhaseTimer pt_(ctx, PH_REFIT);
                 const int nb = div_up(t.n_nodes, kThreads);
                 launch_pdl(k_refit_prepare<T, D>, nb, kThreads, 0, s, t.n_nodes, n, t.tnode.as<TNode<T, D>>(),
-                                                               t.nrange.as<int2>(), t.arrive.as<int32_t>(), hdr,
-                                                               t.n_groups, t.dfs_start);
-                launch_pdl(k_refit<T, D>, nb, kThreads, 0, s, t.capacity, n, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
-                                                       t.parent.as<int32_t>(), t.arrive.as<int32_t>(),
-                                                       t.spts.as<SPt<T, D>>(), hdr, bt);
+                    t.nrange.as<int2>(), t.arrive.as<int32_t>(), hdr, t.n_groups, t.dfs_start);
+                launch_pdl(k_refit<T, D>, nb, kThreads, 0, s, t.capacity, n, t.tnode.as<TNode<T, D>>(),
+                    t.nrange.as<int2>(), t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.spts.as<SPt<T, D>>(), hdr,
+                    bt);
                 ctx.kernel_launches += 2;
             }
             if ((err = cudaGetLastError())) return cuda_status(ctx, err, "bounds refit");
@@ -1248,13 +1247,12 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             ctx.kernel_launches += 1;
             if (nchunks > 1) {
                 launch_pdl(k_moved_rank<K>, div_up(mmax, kThreads), kThreads, 0, s, &hdr->n_moved, mcap, mk, mv,
-                                                                             t.mkeys2.as<K>(), t.mvals2.as<int32_t>());
+                    t.mkeys2.as<K>(), t.mvals2.as<int32_t>());
                 ctx.kernel_launches += 1;
             }
-            launch_pdl(k_resort_merge<T, D, K>, nb, kThreads, 0, s, n, &hdr->n_moved, mcap, kp, vp, t.rflag.as<uint8_t>(),
-                                                             t.roff.as<int64_t>(), mk, mv, t.mkeys2.as<K>(),
-                                                             t.mvals2.as<int32_t>(), coords, ok, ov,
-                                                             t.spts.as<SPt<T, D>>(), t.iperm.as<int32_t>());
+            launch_pdl(k_resort_merge<T, D, K>, nb, kThreads, 0, s, n, &hdr->n_moved, mcap, kp, vp,
+                t.rflag.as<uint8_t>(), t.roff.as<int64_t>(), mk, mv, t.mkeys2.as<K>(), t.mvals2.as<int32_t>(), coords,
+                ok, ov, t.spts.as<SPt<T, D>>(), t.iperm.as<int32_t>());
             ctx.kernel_launches += 1;
             t.iperm_valid = true;
         }
@@ -1303,31 +1301,28 @@ int run_pipeline(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int64_
             return cuda_status(ctx, err, "cloud root reset");
         {
         PhaseTimer pt_(ctx, PH_TOPOLOGY);
-        launch_pdl(k_mark<D, K>, nblocks, kThreads, 0, s, skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(), nblocks,
-                                                  bt);
+        launch_pdl(k_mark<D, K>, nblocks, kThreads, 0, s, skeys, n, t.lohi.as<uint16_t>(), t.blockcnt.as<int32_t>(),
+            nblocks, bt);
         ctx.kernel_launches += exclusive_scan_i32_i64(t.blockcnt.as<int32_t>(), t.blockoff.as<int64_t>(), nbc,
                                                       &hdr->n_nodes, t.scan_tmp.as<int64_t>(), s);
-        launch_pdl(k_emit_ids<D>, nblocks, kThreads, 0, s, n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks, cap,
-                                                    t.fchild.as<int32_t>(), t.nrange.as<int2>(), t.arrive.as<int32_t>(), hdr, bt);
-        launch_pdl(k_emit_nodes<T, D, K>, div_up(cap, kThreads), kThreads, 0, s,
-            skeys, n, cap, t.fchild.as<int32_t>(), t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
-            t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.chain.as<int32_t>(), t.blockoff.as<int64_t>(), nblocks,
-            hdr, bt);
+        launch_pdl(k_emit_ids<D>, nblocks, kThreads, 0, s, n, t.lohi.as<uint16_t>(), t.blockoff.as<int64_t>(), nblocks,
+            cap, t.fchild.as<int32_t>(), t.nrange.as<int2>(), t.arrive.as<int32_t>(), hdr, bt);
+        launch_pdl(k_emit_nodes<T, D, K>, div_up(cap, kThreads), kThreads, 0, s, skeys, n, cap, t.fchild.as<int32_t>(),
+            t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(), t.parent.as<int32_t>(), t.arrive.as<int32_t>(),
+            t.chain.as<int32_t>(), t.blockoff.as<int64_t>(), nblocks, hdr, bt);
         ctx.kernel_launches += 3;
         }
         {
         PhaseTimer pt_(ctx, PH_REFIT);
-        launch_pdl(k_refit<T, D>, div_up(cap, kThreads), kThreads, 0, s, cap, n, t.tnode.as<TNode<T, D>>(), t.nrange.as<int2>(),
-                                                                  t.parent.as<int32_t>(), t.arrive.as<int32_t>(),
-                                                                  t.spts.as<SPt<T, D>>(), hdr, bt);
+        launch_pdl(k_refit<T, D>, div_up(cap, kThreads), kThreads, 0, s, cap, n, t.tnode.as<TNode<T, D>>(),
+            t.nrange.as<int2>(), t.parent.as<int32_t>(), t.arrive.as<int32_t>(), t.spts.as<SPt<T, D>>(), hdr, bt);
         ctx.kernel_launches += 1;
         }
         {
             PhaseTimer pt_(ctx, PH_GROUPS);
-            launch_pdl(k_groups<T, D, K>, div_up(cap, kThreads), kThreads, 0, s,
-                t.tnode.as<TNode<T, D>>(), cap, t.groups.as<int2>(), (int64_t)gcap, t.chain.as<int32_t>(),
-                t.parent.as<int32_t>(), hdr, gmax, skeys, t.nrange.as<int2>(),
-                bt.n_clouds ? nullptr : t.gstart.as<int32_t>());
+            launch_pdl(k_groups<T, D, K>, div_up(cap, kThreads), kThreads, 0, s, t.tnode.as<TNode<T, D>>(), cap,
+                t.groups.as<int2>(), (int64_t)gcap, t.chain.as<int32_t>(), t.parent.as<int32_t>(), hdr, gmax, skeys,
+                t.nrange.as<int2>(), bt.n_clouds ? nullptr : t.gstart.as<int32_t>());
             ctx.kernel_launches += 1;
             if (bt.n_clouds) {
                 k_cloud_start<T, D><<<div_up(bt.n_clouds, 128), 128, 0, s>>>(t.tnode.as<TNode<T, D>>(), bt, cap, hdr);
@@ -1391,8 +1386,7 @@ int resort_mark(Ctx& ctx, Tree& t, const T* coords, int64_t n, T radius, int pre
     OctHeader* hdr = t.hdr.as<OctHeader>();
     PhaseTimer pt_(ctx, PH_ENCODE);
     launch_pdl(k_resort_mark<T, D, K>, nb, kThreads, 0, s, coords, n, t.vals[prev].as<int32_t>(), t.keys[prev].as<K>(),
-                                                    T(1) / radius, hdr, t.rflag.as<uint8_t>(), t.rcnt.as<int32_t>(),
-                                                    t.mkeys.as<K>(), t.mvals.as<int32_t>(), cap);
+        T(1) / radius, hdr, t.rflag.as<uint8_t>(), t.rcnt.as<int32_t>(), t.mkeys.as<K>(), t.mvals.as<int32_t>(), cap);
     ctx.kernel_launches += 1 + exclusive_scan_i32_i64(t.rcnt.as<int32_t>(), t.roff.as<int64_t>(), nb, nullptr,
                                                       t.scan_tmp.as<int64_t>(), s);
     return OK;

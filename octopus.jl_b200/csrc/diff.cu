@@ -536,15 +536,14 @@ int twins_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32_
     launch_pdl(k_seg_pairs, div_up(n, tb), tb, 0, s, ctx.droff.as<int64_t>(), n, ctx.dseg.as<int2>());
     Term4<T>* term = ctx.dterm.as<Term4<T>>();
     if (coords)
-        launch_pdl(k_edge_terms<T, D, true>, div_up(m, tb), tb, 0, s, m, n, snd, rcv, nullptr, nullptr, (const T*)coords,
-                                                               (const T*)d_disp, (const T*)d_dist, r, inv_r, term);
+        launch_pdl(k_edge_terms<T, D, true>, div_up(m, tb), tb, 0, s, m, n, snd, rcv, nullptr, nullptr,
+            (const T*)coords, (const T*)d_disp, (const T*)d_dist, r, inv_r, term);
     else
-        launch_pdl(k_edge_terms<T, D, false>, div_up(m, tb), tb, 0, s, m, n, snd, rcv, (const T*)rel_disp, (const T*)rel_dist,
-                                                                nullptr, (const T*)d_disp, (const T*)d_dist, r, inv_r,
-                                                                term);
+        launch_pdl(k_edge_terms<T, D, false>, div_up(m, tb), tb, 0, s, m, n, snd, rcv, (const T*)rel_disp,
+            (const T*)rel_dist, nullptr, (const T*)d_disp, (const T*)d_dist, r, inv_r, term);
     const bool vec = ((uintptr_t)snd & 15) == 0;
-    launch_pdl(k_adjoint_twins<T>, (unsigned)div_up(n, kTwinGroups * kTwinWarps), 32 * kTwinWarps, 0, s,
-        n, m, order, ctx.dseg.as<int2>(), snd, rcv, term, D, vec, (T*)grad, status);
+    launch_pdl(k_adjoint_twins<T>, (unsigned)div_up(n, kTwinGroups * kTwinWarps), 32 * kTwinWarps, 0, s, n, m, order,
+        ctx.dseg.as<int2>(), snd, rcv, term, D, vec, (T*)grad, status);
     ctx.kernel_launches += 4;
     if ((err = cudaGetLastError())) return cuda_status(ctx, err, "adjoint launch");
     return read_status(ctx, flags);
@@ -666,13 +665,13 @@ int mirror_typed(Ctx& ctx, int64_t n, int64_t m, const int32_t* snd, const int32
     const unsigned blocks = (unsigned)div_up(n, kTwinGroups * kTwinWarps);
     const bool vec = ((uintptr_t)snd & 15) == 0;
     if (coords)
-        launch_pdl(k_adjoint_mirror<T, D, true>, blocks, 32 * kTwinWarps, 0, s,
-            n, m, order, ctx.dseg.as<int2>(), snd, rcv, mirror, nullptr, nullptr, (const T*)coords, (const T*)d_disp,
-            (const T*)d_dist, r, inv_r, (T*)grad, status);
+        launch_pdl(k_adjoint_mirror<T, D, true>, blocks, 32 * kTwinWarps, 0, s, n, m, order, ctx.dseg.as<int2>(), snd,
+            rcv, mirror, nullptr, nullptr, (const T*)coords, (const T*)d_disp, (const T*)d_dist, r, inv_r, (T*)grad,
+            status);
     else
-        launch_pdl(k_adjoint_mirror<T, D, false>, blocks, 32 * kTwinWarps, 0, s,
-            n, m, order, ctx.dseg.as<int2>(), snd, rcv, mirror, (const T*)rel_disp, (const T*)rel_dist, nullptr,
-            (const T*)d_disp, (const T*)d_dist, r, inv_r, (T*)grad, status);
+        launch_pdl(k_adjoint_mirror<T, D, false>, blocks, 32 * kTwinWarps, 0, s, n, m, order, ctx.dseg.as<int2>(), snd,
+            rcv, mirror, (const T*)rel_disp, (const T*)rel_dist, nullptr, (const T*)d_disp, (const T*)d_dist, r, inv_r,
+            (T*)grad, status);
     ctx.kernel_launches += 3;
     if ((err = cudaGetLastError())) return cuda_status(ctx, err, "adjoint launch");
     return read_status(ctx, flags);

@@ -1062,18 +1062,18 @@ int count_typed(Ctx& ctx, const Tree& q, const Tree& t, bool exclude_self, int64
         PhaseTimer pt_(ctx, PH_COUNT);
         const int64_t ng = q.n_groups;
         if (ctx.rec_cap)
-            launch_pdl(k_edges<T, D, EP_RECORD>, div_up(ng, kEdgeWarps), kEdgeThreads, 0, s,
-                q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
-                t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
-                nullptr, nullptr, nullptr, nullptr, (int*)(ctx.total.as<int64_t>() + 1), ctx.recs.as<int2>(),
-                ctx.rec_cap, ctx.rcount.as<uint16_t>(), ctx.gflag.as<uint8_t>(), t.batch(), nullptr, tn.max_seg,
-                tn.multi_pop, tn.sub_boxes, tn.prefetch, own_start(q, t));
+            launch_pdl(k_edges<T, D, EP_RECORD>, div_up(ng, kEdgeWarps), kEdgeThreads, 0, s, q.spts.as<SPt<T, D>>(),
+                q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start, t.spts.as<SPt<T, D>>(), t.n_nodes, r2,
+                T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr,
+                (int*)(ctx.total.as<int64_t>() + 1), ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint16_t>(),
+                ctx.gflag.as<uint8_t>(), t.batch(), nullptr, tn.max_seg, tn.multi_pop, tn.sub_boxes, tn.prefetch,
+                own_start(q, t));
         else
-            launch_pdl(k_edges<T, D, EP_COUNT>, div_up(ng, kEdgeWarps), kEdgeThreads, 0, s,
-                q.spts.as<SPt<T, D>>(), q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start,
-                t.spts.as<SPt<T, D>>(), t.n_nodes, r2, T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr,
-                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr,
-                tn.max_seg, tn.multi_pop, tn.sub_boxes, tn.prefetch, own_start(q, t));
+            launch_pdl(k_edges<T, D, EP_COUNT>, div_up(ng, kEdgeWarps), kEdgeThreads, 0, s, q.spts.as<SPt<T, D>>(),
+                q.groups.as<int2>(), ng, t.tnode.as<TNode<T, D>>(), t.dfs_start, t.spts.as<SPt<T, D>>(), t.n_nodes, r2,
+                T(0), exclude_self ? 1 : 0, ctx.counts.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr,
+                nullptr, nullptr, 0, nullptr, nullptr, t.batch(), nullptr, tn.max_seg, tn.multi_pop, tn.sub_boxes,
+                tn.prefetch, own_start(q, t));
         ctx.kernel_launches += 1;
     }
     {
@@ -1137,8 +1137,8 @@ cudaError_t launch_expand(Ctx& ctx, const Tree& q, const Tree& t, T inv_r, int32
             return launch_expand_shape<T, D, FEAT, 128>(ctx, q, t, inv_r, senders, receivers, rel_disp, rel_dist,
                                                         bulk_ok);
         default:  // direct stores
-            launch_pdl(k_expand_direct<T, D>, div_up(q.n, 32 * kDirectWarps), kDirectWarps * 32, 0, ctx.stream,
-                q.n, q.iperm.as<int32_t>(), q.spts.as<SPt<T, D>>(), t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
+            launch_pdl(k_expand_direct<T, D>, div_up(q.n, 32 * kDirectWarps), kDirectWarps * 32, 0, ctx.stream, q.n,
+                q.iperm.as<int32_t>(), q.spts.as<SPt<T, D>>(), t.spts.as<SPt<T, D>>(), ctx.offsets.as<int64_t>(),
                 ctx.recs.as<int2>(), ctx.rec_cap, ctx.rcount.as<uint16_t>(), inv_r, senders, receivers, (T*)rel_disp,
                 (T*)rel_dist, t.batch());
             return cudaGetLastError();

@@ -278,8 +278,8 @@ cudaError_t launch_point_pass(const T* coords, const EncodeParams<T>& ep, const 
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    launch_pdl(kern, ntiles, kSortThreads, smem, s, coords, ep, kin, pin, kout, pout, perm, iperm, n, pass, ntiles, scratch,
-                                           status, spin_limit, withhold);
+    launch_pdl(kern, ntiles, kSortThreads, smem, s, coords, ep, kin, pin, kout, pout, perm, iperm, n, pass, ntiles,
+        scratch, status, spin_limit, withhold);
     return cudaGetLastError();
 }
 
@@ -323,8 +323,8 @@ cudaError_t point_sort(const T* coords, const EncodeParams<T>& ep, int64_t n, in
             return e;
     }
     if (iperm) {
-        launch_pdl(k_inverse_perm, (unsigned)((n + kSortThreads - 1) / kSortThreads), kSortThreads, 0, s, perm, n, iperm,
-                                                                                                   status);
+        launch_pdl(k_inverse_perm, (unsigned)((n + kSortThreads - 1) / kSortThreads), kSortThreads, 0, s, perm, n,
+            iperm, status);
         *launches += 1;
     }
     return cudaGetLastError();
