@@ -1010,6 +1010,7 @@ __global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, const int6
     pdl_wait();
     pdl_trigger();
     __shared__ int wsum[kThreads / 32];
+    __shared__ int64_t sbound[2];
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t m = *m_ptr;
     if (m > cap) {
@@ -1026,6 +1027,15 @@ __global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, const int6
         return;
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    // The previous (key, index) order is sorted, so the changed keys below any
+    // entry of this block lie between those below its first entry and those
+    // below the next block's first: two full searches per block, then each
+    // thread searches only that span (usually a few entries).
+    const int64_t b0 = (int64_t)blockIdx.x * blockDim.x;
+    if (threadIdx.x < 2) {
+        const int64_t q = b0 + (threadIdx.x ? (int64_t)blockDim.x : 0);
+        sbound[threadIdx.x] = q < n ? count_below(mk, mv, m, keys[q], perm[q]) : m;
+    }
     const bool in = p < n;
     const bool c = in && changed[p];
     const bool u = in && !c;
@@ -1033,6 +1043,7 @@ __global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, const int6
     const unsigned ubal = __ballot_sync(0xffffffffu, u);
     if (lane == 0) wsum[w] = __popc(cbal);
     __syncthreads();
+    const int64_t blo = sbound[0], bhi = sbound[1];
     int before = __popc(cbal & lanemask_lt());
     for (int j = 0; j < w; ++j) before += wsum[j];
     K key = 0;
@@ -1041,7 +1052,7 @@ __global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, const int6
     if (u) {
         key = keys[p];
         idx = perm[p];
-        s = count_below(mk, mv, m, key, idx);
+        s = blo + count_below(mk + blo, mv + blo, bhi - blo, key, idx);
     }
     // Changed keys below the next unchanged key: from the next unchanged lane
     // of this warp, or found past the warp's end.
@@ -1052,7 +1063,14 @@ __global__ void __launch_bounds__(kThreads) k_resort_merge(int64_t n, const int6
     if (!later) {
         int64_t q = p - lane + 32;
         while (q < n && changed[q]) ++q;
-        sn = q < n ? count_below(mk, mv, m, keys[q], perm[q]) : m;
+        if (q >= n)
+            sn = m;
+        else if (q < b0 + (int64_t)blockDim.x)
+            sn = blo + count_below(mk + blo, mv + blo, bhi - blo, keys[q], perm[q]);
+        else if (q == b0 + (int64_t)blockDim.x)
+            sn = bhi;
+        else
+            sn = count_below(mk, mv, m, keys[q], perm[q]);
     }
     const int64_t ui = p - (changed_before[blockIdx.x] + before);  // rank among unchanged keys
     put_sorted<T, D, K>(ui + s, key, idx, coords, okeys, operm, spts, iperm);
